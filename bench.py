@@ -1,0 +1,396 @@
+"""Benchmark of the two-phase time step (cell-steps/s) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form fp64|fp32c]
+                    [--impl capaz|reference] [--grid NX NY NZ]
+
+Workload: the 256x256x128 two-phase problem with gravity on z (reference axes
+NX=256, NY=128 vertical, NZ=256; 8,388,608 cells), lognormal permeability
+(sigma 1, correlation length 8 cells, seeded FFT field), porosity tied to it,
+the workload fluids and boundary setup (capaz_b200/configs.py).  A step is
+one time step of the whole grid.  With N GPUs every rank steps its own
+replica of the grid (weak scaling; the step needs no data-path collective).
+
+One JSON line on rank 0:
+  value   cell-steps/s over exactly K steps, state resident in HBM, CUDA
+          events on the launching stream, max over ranks, summed over ranks;
+  e2e     the same metric through the C ABI with host buffers: pinned-host
+          upload of the state (P_w, S_n, m, K), K steps each followed by a
+          device->host read of that step's diagnostics (mass balance, max
+          residual), then download of (P_w, S_n), all inside the timed region;
+  roofline  algorithmic HBM bytes of the dominant kernel per launch divided
+          by its average launch time (CUDA events), against the measured copy
+          bandwidth; `traffic` from the committed ncu summary when present;
+  cpu_baseline  the OpenMP oracle (all host threads) on a bounded sample.
+`--impl reference` times the reference's own CPU step (oracle/_ref) instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+# Algorithmic HBM bytes per cell-step of the fused step kernels: read the
+# state and the media, write the state, with perfect halo reuse.
+ALGO_BYTES = {
+    ("fp64", True): 48,   # P_w, S_n, m, K read (32) + P_w, S_n written (16)
+    ("fp64", False): 40,  # uniform K
+    ("fp32c", True): 24,  # the same fields at 4 bytes
+    ("fp32c", False): 20,
+}
+PUBLISHED_1GPU = 44.9e6  # reference's published 1-GPU two-phase step, 250^3, cell-steps/s
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="capaz", choices=["capaz", "reference"])
+    ap.add_argument("--form", default=None, choices=[None, "fp64", "fp32c"])
+    ap.add_argument("--grid", type=int, nargs=3, default=[256, 256, 128],
+                    help="workload grid Nx Ny Nz, gravity on z")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self.proc = None
+        self.t0 = self.t1 = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.perf_counter(), line.strip()))
+
+    def mark(self, begin: bool):
+        if begin:
+            self.t0 = time.perf_counter()
+        else:
+            self.t1 = time.perf_counter()
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for t, line in self.samples:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            rows.append((t, f))
+        inside = [r for r in rows if self.t0 is not None and self.t0 - 0.15 <= r[0] <= (self.t1 or 1e30) + 0.15]
+        use = inside if inside else rows
+        sm = [float(f[1]) for _, f in use if f[1].replace(".", "").isdigit()]
+        mx = [float(f[2]) for _, f in use if f[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, f in use for i in range(4) if f[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples_in_region": len(inside), "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws, local=0):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier(device_ids=[local])
+
+
+def reduce_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def load_traffic(kernel: str, workload: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        e = d.get(kernel, {}).get(workload)
+        return None if e is None else e
+    except Exception:
+        return None
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline_port(w, nsteps: int = 2) -> dict:
+    """The OpenMP oracle on the workload's full grid for a few steps."""
+    from oracle import oracle as O
+    p = w.params
+    st = O.init(p, w.m)
+    state = {"P_w": st["P_w"], "S_n": st["S_n"]}
+    O.step(p, state, 1, w.m, w.K)  # page in, thread pool up
+    t0 = time.perf_counter()
+    O.step(p, state, nsteps, w.m, w.K)
+    dt = time.perf_counter() - t0
+    return {"value": p.ncell * nsteps / dt, "unit": "cell-steps/s", "cores": O.max_threads(), "kind": "port",
+            "sample": f"{nsteps} steps of the full {p.nx}x{p.ny}x{p.nz} grid (FP64, bit-identical to the "
+                      f"reference CPU step), {dt:.1f} s"}
+
+
+def reference_sample_grid(total_steps: int, budget_s: float = 90.0, rate: float = 6.0e5):
+    """A slab of the workload grid small enough that total_steps reference
+    steps take about budget_s on one core."""
+    cells = max(3 * 16 * 16, min(256 * 128 * 8, int(rate * budget_s / max(total_steps, 1))))
+    nx = 64 if cells >= 64 * 16 * 3 else 16
+    ny = min(128, max(3, int(round(cells / (nx * 16)))))
+    nz = max(3, int(round(cells / (nx * ny))))
+    return nx, ny, nz
+
+
+def run_reference(args) -> None:
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    from capaz_b200.configs import two_phase_params
+    from oracle import oracle as O
+    K, W = args.steps, args.warmup
+    Nx, Ny, Nz = args.grid
+    line = {"impl": "reference", "metric": "cell-steps/s", "unit": "cell-steps/s", "higher_is_better": True,
+            "n_gpus": args.gpus, "steps": K, "warmup": W, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic"}
+    if not O.ref_available(2):
+        line["unavailable"] = "reference CPU binaries (oracle/_ref) were not built"
+        print(json.dumps(line), flush=True)
+        return
+    nx, ny, nz = reference_sample_grid(K + W)
+    p = two_phase_params(nx, ny, nz, percell_k=False)
+    # The reference model has no top-pressure offset, background saturation
+    # or per-cell K: uniform K = 1e-12 (the field's median) and its own
+    # initial state; the work per cell-step is the same.
+    p.P_top_offset = 0.0
+    p.S_n_background = 0.0
+    p.dt = 1e-3
+    t0 = time.perf_counter()
+    r = O.ref_run(p, K + W)
+    wall = time.perf_counter() - t0
+    secs = r["info"]["seconds"]
+    val = p.ncell * (K + W) / secs
+    line.update({
+        "value": val, "ms_per_step": 1e3 * secs / (K + W),
+        "config": {"workload": f"reference two-phase CPU step on a {nx}x{ny}x{nz} slab of the "
+                               f"{Nx}x{Ny}x{Nz} workload (uniform K)", "grid_ref": [nx, ny, nz]},
+        "cpu_baseline": {"value": val, "unit": "cell-steps/s", "cores": 1, "kind": "reference",
+                         "sample": f"{K + W} steps of a {nx}x{ny}x{nz} grid with the reference's own CPU "
+                                   f"step (single-threaded as written), {secs:.1f} s loop, {wall:.1f} s wall"},
+        "e2e": {"value": val, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    })
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_capaz(args) -> None:
+    import torch
+
+    from capaz_b200 import Simulation, native
+    from capaz_b200.configs import config1
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = local
+    form_name = args.form or "fp64"
+    form = native.FORM_FP64 if form_name == "fp64" else native.FORM_FP32C
+    K, W = args.steps, args.warmup
+    w = config1(form=form, grid=tuple(args.grid))
+    p = w.params
+    ncell = p.ncell
+    percell = w.K is not None
+
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+    sim = Simulation(p, device=dev)
+    sim.set_field("m", w.m)
+    sim.set_field("K", w.K)
+    sim.init_state()
+    sim.sync()
+
+    # ---- device-resident timing ------------------------------------------
+    with torch.cuda.stream(stream):
+        sim.step(W, stream=sh)
+        stream.synchronize()
+        clocks = Clocks(dev)
+        clocks.start()
+        time.sleep(0.3)
+        barrier(ws, local)
+        torch.cuda.synchronize()
+        l0 = sim.launch_count
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        clocks.mark(True)
+        for i in range(K):
+            starts[i].record(stream)
+            sim.step(1, stream=sh)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+        clocks.mark(False)
+        barrier(ws, local)
+        launches = sim.launch_count - l0
+        total_ms = starts[0].elapsed_time(ends[-1])
+        kern_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / K
+        clk = clocks.stop()
+    sim.sync()
+    total_ms = reduce_max(total_ms, ws)
+    value = ncell * K * ws / (total_ms * 1e-3)
+
+    # ---- end to end through the C ABI with host buffers -------------------
+    e2e = None
+    if not args.no_e2e:
+        q = p.copy()
+        q.flags |= native.FLAG_DIAGNOSTICS
+        sim2 = Simulation(q, device=dev)
+        host = {}
+        for name, arr in (("P_w", None), ("S_n", None), ("m", w.m), ("K", w.K)):
+            t = torch.empty(w.m.shape, dtype=torch.float64, pin_memory=True)
+            host[name] = t
+        ref = Simulation(p, device=dev)  # source of the initial state arrays
+        ref.set_field("m", w.m)
+        ref.set_field("K", w.K)
+        ref.init_state()
+        host["P_w"].numpy()[...] = ref.get_field("P_w")
+        host["S_n"].numpy()[...] = ref.get_field("S_n")
+        host["m"].numpy()[...] = w.m
+        host["K"].numpy()[...] = w.K
+        ref.close()
+        out_P = torch.empty(w.m.shape, dtype=torch.float64, pin_memory=True)
+        out_S = torch.empty(w.m.shape, dtype=torch.float64, pin_memory=True)
+        sim2.step(0)
+        torch.cuda.synchronize()
+        barrier(ws, local)
+        t0 = time.perf_counter()
+        for name in ("m", "K", "P_w", "S_n"):
+            sim2.lib.capaz_set_field(sim2.ctx, native.FIELDS[name], host[name].data_ptr(), sh)
+        for i in range(K):
+            sim2.step(1, stream=sh)
+            sim2.diag(stream=sh)
+        native.check(sim2.lib.capaz_get_field(sim2.ctx, native.FIELDS["P_w"], out_P.data_ptr(), sh), sim2.ctx)
+        native.check(sim2.lib.capaz_get_field(sim2.ctx, native.FIELDS["S_n"], out_S.data_ptr(), sh), sim2.ctx)
+        e2e_s = time.perf_counter() - t0
+        barrier(ws, local)
+        e2e_s = reduce_max(e2e_s, ws)
+        es = 8
+        h2d = 4 * ncell * es
+        d2h = 2 * ncell * es
+        e2e = {"value": ncell * K * ws / e2e_s, "unit": "cell-steps/s",
+               "h2d_bytes_per_step": (h2d + K * 0) / K, "d2h_bytes_per_step": (d2h + K * 40) / K,
+               "definition": "pinned-host upload of P_w, S_n, m, K; K steps each with a D2H read of the "
+                             "step's diagnostics (40 B); download of P_w, S_n; wall clock"}
+        sim2.close()
+
+    # ---- roofline ----------------------------------------------------------
+    peak, peak_kind = measured_peaks()
+    abytes = ALGO_BYTES[(form_name, percell)] * ncell
+    achieved = abytes / (kern_ms * 1e-3) / 1e9
+    kname = "step2_fp64_kernel" if form_name == "fp64" else "step2_fp32c_kernel"
+    wl_key = f"{args.grid[0]}x{args.grid[1]}x{args.grid[2]}"
+    traffic = load_traffic(kname, wl_key)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "kernel": kname, "algorithmic_bytes_per_launch": abytes,
+            "kernel_ms": kern_ms, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_port(w)
+        except Exception as e:  # the baseline is informative, never fatal
+            cpu = {"value": None, "unit": "cell-steps/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
+
+    sim.close()
+    if rank == 0:
+        line = {
+            "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": K,
+            "warmup": W, "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": value / PUBLISHED_1GPU,
+            "vs_baseline_source": "reference's published 1-GPU two-phase step, 250^3 grid, 44.9e6 cell-steps/s "
+                                  "(Fermi-era GPU)",
+            "dtype": "f64" if form_name == "fp64" else "f32 storage/stencil + f64 Newton",
+            "data": "synthetic (seeded lognormal K and porosity fields)",
+            "config": {"workload": f"two-phase {args.grid[0]}x{args.grid[1]}x{args.grid[2]} gravity on z, "
+                                   f"lognormal K sigma 1 ell 8, {form_name}",
+                       "grid_ref": [p.nx, p.ny, p.nz], "cells": ncell, "form": form_name, "dt": p.dt,
+                       "newton_iterations": p.newton_iterations,
+                       "parallelism": f"replicas x{ws}",
+                       "l2": "inputs larger than L2: each step reads P_w, S_n, m, K and writes P_w, S_n "
+                             f"({ALGO_BYTES[(form_name, percell)] * ncell / 1e6:.0f} MB)"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_capaz(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,554 @@
+// C ABI of the library (include/capaz_b200.h): contexts, parameters, field
+// transfer, the reference's initial state and the step launcher.
+//
+// Host-side restatements of the reference's setup, with their origins:
+//   capaz_params_from_ini  read_defines          main.cpp:1280-1639
+//   capaz_init_state       data_initialization   two-phase.cpp:113-172,
+//                                                three-phase.cpp:429-500
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "capaz_internal.h"
+#include "capaz_ctx.h"
+
+using namespace capaz;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(capaz_ctx* ctx, int code, const char* fmt, ...) __attribute__((format(printf, 3, 4)));
+int fail(capaz_ctx* ctx, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->last_error = buf;
+  else g_create_error = buf;
+  return code;
+}
+
+int cuda_fail(capaz_ctx* ctx, cudaError_t e, const char* what) {
+  int code = (e == cudaErrorMemoryAllocation) ? CAPAZ_ERR_OUT_OF_MEMORY : CAPAZ_ERR_CUDA;
+  return fail(ctx, code, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CUDA_TRY(ctx, call)                                   \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+bool is_state_field(const capaz_params& p, int f) {
+  if (f == CAPAZ_FIELD_P_W || f == CAPAZ_FIELD_S_N) return true;
+  if (p.phases == 3 && (f == CAPAZ_FIELD_S_W || f == CAPAZ_FIELD_P_N || f == CAPAZ_FIELD_P_G)) return true;
+  return false;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Step constants.
+namespace capaz {
+
+Step2Const make_step2_const(const capaz_params& p) {
+  Step2Const c;
+  memset(&c, 0, sizeof c);
+  c.nx = p.nx;
+  c.ny = p.ny;
+  c.nz = p.nz;
+  c.source = p.source;
+  c.iters = p.newton_iterations;
+  c.sy = p.nx;
+  c.sz = (long long)p.nx * p.ny;
+  c.ncell = c.sz * p.nz;
+  c.tiles_x = (p.nx - 2 + TX - 1) / TX;
+  c.tiles_y = (p.ny - 2 + TY - 1) / TY;
+  if (p.nz == 1) {
+    c.zchunk = 1;
+    c.nzchunks = 1;
+  } else {
+    const int interior = p.nz - 2;
+    const int tiles = c.tiles_x * c.tiles_y;
+    // Enough CTAs to fill 148 SMs several times over; the z-chunk overlap
+    // (two extra planes per chunk) stays small with chunks of >= 8 planes.
+    int chunk = 32;
+    while (chunk > 8 && (long long)tiles * ((interior + chunk - 1) / chunk) < 4 * 148) chunk /= 2;
+    c.zchunk = std::min(chunk, interior);
+    c.nzchunks = (interior + c.zchunk - 1) / c.zchunk;
+  }
+  c.hx = p.hx;
+  c.hy = p.hy;
+  c.hz = p.hz;
+  c.dt = p.dt;
+  c.g = p.g_const;
+  c.P_atm = p.P_atm;
+  c.P_top = p.P_top_offset;
+  c.ro0_w = p.ro0_w;
+  c.ro0_n = p.ro0_n;
+  c.beta_w = p.beta_w;
+  c.beta_n = p.beta_n;
+  c.mu_w = p.mu_w;
+  c.mu_n = p.mu_n;
+  c.S_wr = p.S_wr;
+  c.lambda = p.lambda;
+  c.P_d = p.P_d;
+  c.K0 = p.K0;
+  c.S_n_gr = p.S_n_gr;
+  const double lam = p.lambda;
+  c.e_kw = (2. + 3. * lam) / lam;
+  c.e_kn = (2. + lam) / lam;
+  c.e_pk = -1. / lam;
+  c.e_aaa = ((-1.) / lam) - 1.;
+  // P_d == 0: P_d*pow(S_e, e) is +0 whenever pow is finite and positive,
+  // i.e. for S_e >= 2^(1000/e) with e < 0, and PkS is +0 when
+  // lambda*(1 - S_wr) > 0.  Otherwise the fast path is disabled (0).
+  c.se_fast_min = 0.;
+  if (p.P_d == 0. && lam > 0. && (1. - p.S_wr) > 0. && isfinite(c.e_aaa) && c.e_aaa < 0.)
+    c.se_fast_min = ldexp(1.0, (int)floor(1000. / c.e_aaa) + 1);
+  c.vol = p.hx * p.hy * p.hz;
+  return c;
+}
+
+}  // namespace capaz
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int capaz_abi_version(void) { return CAPAZ_ABI_VERSION; }
+size_t capaz_params_size(void) { return sizeof(capaz_params); }
+size_t capaz_diag_size(void) { return sizeof(capaz_diag); }
+
+int capaz_params_default(capaz_params* p) {
+  if (!p) return CAPAZ_ERR_INVALID_ARGUMENT;
+  memset(p, 0, sizeof *p);
+  // Two-phase/defines.ini values.
+  p->nx = 15;
+  p->ny = 15;
+  p->nz = 1;
+  p->phases = 2;
+  p->form = CAPAZ_FORM_FP64;
+  p->newton_iterations = 10;
+  p->source = 30;
+  p->flags = 0;
+  p->hx = p->hy = p->hz = 5e-2;
+  p->dt = 1e-3;
+  p->beta_w = 4.4e-7;
+  p->beta_n = 1e-6;
+  p->beta_g = 9.2e-6;
+  p->ro0_w = 1000;
+  p->ro0_n = 1460;
+  p->ro0_g = 1.4;
+  p->mu_w = 0.001;
+  p->mu_n = 0.0009;
+  p->mu_g = 1.84e-5;
+  p->g_const = 9.807;
+  p->P_atm = 100000;
+  p->lambda = 2.7;
+  p->S_wr = 0.09;
+  p->S_nr = 0.;
+  p->S_gr = 0.;
+  p->P_d = 755;
+  p->S_n_gr = 0.2;
+  p->S_w_gr = 0.4;
+  p->S_w_init = 0.4;
+  p->S_n_init = 0.3;
+  p->porosity = 0.4;
+  p->K0 = 6.64e-11;
+  p->timeX = 100;
+  p->P_top_offset = 0.;
+  p->S_n_background = 0.;
+  return CAPAZ_OK;
+}
+
+int capaz_params_from_ini(const char* path, capaz_params* p) {
+  if (!path || !p) return CAPAZ_ERR_INVALID_ARGUMENT;
+  FILE* f = fopen(path, "rt");
+  if (!f) return fail(nullptr, CAPAZ_ERR_INI, "cannot open %s", path);
+  char str[250];
+  while (fgets(str, sizeof str, f)) {
+    if (str[0] == '#') continue;
+    const char* eq = strchr(str, '=');
+    if (!eq) continue;
+    std::string name(str, eq - str);
+    // The value runs to the first space (main.cpp:1319); atof/atoi stop at
+    // the line end themselves.
+    std::string value;
+    for (const char* q = eq + 1; *q && *q != ' '; q++) value.push_back(*q);
+    const char* v = value.c_str();
+    double d = atof(v);
+    int n = atoi(v);
+    if (name == "HX") p->hx = d;
+    else if (name == "HY") p->hy = d;
+    else if (name == "HZ") p->hz = d;
+    else if (name == "DT") p->dt = d;
+    else if (name == "BETA_W") p->beta_w = d;
+    else if (name == "BETA_N") p->beta_n = d;
+    else if (name == "BETA_G") p->beta_g = d;
+    else if (name == "RO_W") p->ro0_w = d;
+    else if (name == "RO_N") p->ro0_n = d;
+    else if (name == "RO_G") p->ro0_g = d;
+    else if (name == "MU_W") p->mu_w = d;
+    else if (name == "MU_N") p->mu_n = d;
+    else if (name == "MU_G") p->mu_g = d;
+    else if (name == "G_CONST") p->g_const = d;
+    else if (name == "P_ATM") p->P_atm = d;
+    else if (name == "LAMBDA_0") p->lambda = d;
+    else if (name == "M_0") p->porosity = d;
+    else if (name == "S_WR_0") p->S_wr = d;
+    else if (name == "S_NR_0") p->S_nr = d;
+    else if (name == "S_GR_0") p->S_gr = d;
+    else if (name == "K_0") p->K0 = d;
+    else if (name == "P_D_0") p->P_d = d;
+    else if (name == "S_W_GR") p->S_w_gr = d;
+    else if (name == "S_W_INIT") p->S_w_init = d;
+    else if (name == "S_N_INIT") p->S_n_init = d;
+    else if (name == "S_N_GR") p->S_n_gr = d;
+    else if (name == "SOURCE") p->source = n;
+    else if (name == "ITERATIONS") p->newton_iterations = n;
+    else if (name == "TIMEX") p->timeX = d;
+    else if (name == "NX") p->nx = n;
+    else if (name == "NY") p->ny = n;
+    else if (name == "NZ") p->nz = n;
+    // Extensions (ignored by the reference, which skips unknown keys).
+    else if (name == "P_TOP_OFFSET") p->P_top_offset = d;
+    else if (name == "S_N_BACKGROUND") p->S_n_background = d;
+    else if (name == "PERCELL_K") p->flags = n ? (p->flags | CAPAZ_FLAG_PERCELL_K) : (p->flags & ~CAPAZ_FLAG_PERCELL_K);
+    else if (name == "PHASES") p->phases = n;
+  }
+  fclose(f);
+  return CAPAZ_OK;
+}
+
+int capaz_params_validate(const capaz_params* p) {
+  if (!p) return CAPAZ_ERR_INVALID_ARGUMENT;
+  if (p->phases != 2 && p->phases != 3) return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "phases must be 2 or 3");
+  if (p->form != CAPAZ_FORM_FP64 && p->form != CAPAZ_FORM_FP32C)
+    return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "unknown form %d", p->form);
+  // Grids where every boundary cell's basic coordinate is an interior cell
+  // (cpu.cpp:107-141); elsewhere the reference's result depends on its loop
+  // order.  nx == 1 is the reference's own three-phase column case.
+  const bool nx_ok = p->nx >= 3 || (p->phases == 3 && p->nx == 1);
+  if (!nx_ok || p->ny < 3 || p->nz < 1 || p->nz == 2)
+    return fail(nullptr, CAPAZ_ERR_UNSUPPORTED_GRID, "grid %dx%dx%d unsupported (need nx,ny>=3, nz==1 or >=3)",
+                p->nx, p->ny, p->nz);
+  if ((long long)p->nx * p->ny * p->nz > (1LL << 34))
+    return fail(nullptr, CAPAZ_ERR_UNSUPPORTED_GRID, "grid too large");
+  if (!(p->hx > 0) || !(p->hy > 0) || !(p->hz > 0) || !(p->dt > 0))
+    return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "hx, hy, hz and dt must be > 0");
+  if (p->newton_iterations < 0 || p->newton_iterations > 1000)
+    return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "newton_iterations out of range");
+  if (!(p->mu_w > 0) || !(p->mu_n > 0) || !(p->P_atm > 0) || !(p->lambda != 0))
+    return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "mu, P_atm must be > 0 and lambda != 0");
+  if (!(p->K0 > 0)) return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "K_0 must be > 0");
+  return CAPAZ_OK;
+}
+
+const char* capaz_last_error(const capaz_ctx* ctx) {
+  return ctx ? ctx->last_error.c_str() : g_create_error.c_str();
+}
+
+capaz_ctx* capaz_create(const capaz_params* p, int device, int* status) {
+  int st = capaz_params_validate(p);
+  if (st) {
+    if (status) *status = st;
+    return nullptr;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+    cudaGetLastError();
+    if (status) *status = fail(nullptr, CAPAZ_ERR_NO_DEVICE, "no CUDA device");
+    return nullptr;
+  }
+  if (device < 0 || device >= ndev) {
+    if (status) *status = fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "device %d out of range", device);
+    return nullptr;
+  }
+  capaz_ctx* ctx = new capaz_ctx();
+  ctx->p = *p;
+  ctx->device = device;
+  st = ctx->allocate();
+  if (st) {
+    g_create_error = ctx->last_error;
+    delete ctx;
+    if (status) *status = st;
+    return nullptr;
+  }
+  if (status) *status = CAPAZ_OK;
+  return ctx;
+}
+
+int capaz_destroy(capaz_ctx* ctx) {
+  if (!ctx) return CAPAZ_ERR_INVALID_ARGUMENT;
+  ctx->release();
+  delete ctx;
+  return CAPAZ_OK;
+}
+
+int capaz_get_params(const capaz_ctx* ctx, capaz_params* out) {
+  if (!ctx || !out) return CAPAZ_ERR_INVALID_ARGUMENT;
+  *out = ctx->p;
+  return CAPAZ_OK;
+}
+
+int64_t capaz_launch_count(const capaz_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int capaz_set_dt(capaz_ctx* ctx, double dt) {
+  if (!ctx || !(dt > 0)) return CAPAZ_ERR_INVALID_ARGUMENT;
+  ctx->p.dt = dt;
+  return CAPAZ_OK;
+}
+
+int capaz_set_field(capaz_ctx* ctx, int field, const double* host, void* stream) {
+  if (!ctx || !host) return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->set_field(field, host, false, (cudaStream_t)stream);
+}
+int capaz_set_field_device(capaz_ctx* ctx, int field, const void* dev, void* stream) {
+  if (!ctx || !dev) return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->set_field(field, dev, true, (cudaStream_t)stream);
+}
+int capaz_get_field(capaz_ctx* ctx, int field, double* host, void* stream) {
+  if (!ctx || !host) return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->get_field(field, host, false, (cudaStream_t)stream);
+}
+int capaz_get_field_device(capaz_ctx* ctx, int field, void* dev, void* stream) {
+  if (!ctx || !dev) return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->get_field(field, dev, true, (cudaStream_t)stream);
+}
+int capaz_init_state(capaz_ctx* ctx, void* stream) {
+  if (!ctx) return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->init_state((cudaStream_t)stream);
+}
+int capaz_step(capaz_ctx* ctx, int nsteps, void* stream) {
+  if (!ctx || nsteps < 0) return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->step(nsteps, (cudaStream_t)stream);
+}
+int capaz_read_diag(capaz_ctx* ctx, capaz_diag* out, void* stream) {
+  if (!ctx || !out) return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->read_diag(out, (cudaStream_t)stream);
+}
+int capaz_sync(capaz_ctx* ctx) {
+  if (!ctx) return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->sync();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// capaz_ctx methods.
+int capaz_ctx::fail_cuda(cudaError_t e, const char* what) { return cuda_fail(this, e, what); }
+int capaz_ctx::fail_msg(int code, const char* msg) { return fail(this, code, "%s", msg); }
+
+int capaz_ctx::allocate() {
+  CUDA_TRY(this, cudaSetDevice(device));
+  n = (long long)p.nx * p.ny * p.nz;
+  const size_t es = (p.form == CAPAZ_FORM_FP64) ? sizeof(double) : sizeof(float);
+  const int nstate = (p.phases == 2) ? 2 : 5;  // P_w, S_n[, S_w, P_n, P_g]
+  for (int b = 0; b < 2; b++)
+    for (int s = 0; s < nstate; s++) CUDA_TRY(this, cudaMalloc(&state[b][s], n * es));
+  CUDA_TRY(this, cudaMalloc(&m, n * es));
+  if (p.flags & CAPAZ_FLAG_PERCELL_K) CUDA_TRY(this, cudaMalloc(&K, n * es));
+  CUDA_TRY(this, cudaMalloc(&err_flag, sizeof(unsigned int)));
+  CUDA_TRY(this, cudaMemset(err_flag, 0, sizeof(unsigned int)));
+  CUDA_TRY(this, cudaMalloc(&diag_out, sizeof(double) * DIAG_STRIDE));
+  CUDA_TRY(this, cudaMemset(diag_out, 0, sizeof(double) * DIAG_STRIDE));
+  // Default porosity M_0 and a zero state until the caller sets one.
+  std::vector<double> mh(n, p.porosity);
+  host_m.assign(mh.begin(), mh.end());
+  int st = upload_converted(m, mh.data(), nullptr);
+  if (st) return st;
+  for (int b = 0; b < 2; b++)
+    for (int s = 0; s < nstate; s++) CUDA_TRY(this, cudaMemset(state[b][s], 0, n * es));
+  if (p.flags & CAPAZ_FLAG_PERCELL_K) {
+    std::vector<double> kh(n, p.K0);
+    st = upload_converted(K, kh.data(), nullptr);
+    if (st) return st;
+  }
+  CUDA_TRY(this, cudaDeviceSynchronize());
+  return CAPAZ_OK;
+}
+
+void capaz_ctx::release() {
+  cudaSetDevice(device);
+  for (int b = 0; b < 2; b++)
+    for (int s = 0; s < 5; s++)
+      if (state[b][s]) cudaFree(state[b][s]);
+  if (m) cudaFree(m);
+  if (K) cudaFree(K);
+  if (err_flag) cudaFree(err_flag);
+  if (diag_out) cudaFree(diag_out);
+  if (diag_partials) cudaFree(diag_partials);
+  if (scratch) cudaFree(scratch);
+  if (host_stage) cudaFreeHost(host_stage);
+}
+
+int capaz_ctx::ensure_scratch() {
+  if (!scratch) CUDA_TRY(this, cudaMalloc(&scratch, n * sizeof(double)));
+  return CAPAZ_OK;
+}
+
+int capaz_ctx::upload_converted(void* dst, const double* host, cudaStream_t s) {
+  if (p.form == CAPAZ_FORM_FP64) {
+    CUDA_TRY(this, cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(this, cudaStreamSynchronize(s));
+    return CAPAZ_OK;
+  }
+  std::vector<float> tmp(n);
+  for (long long l = 0; l < n; l++) tmp[l] = (float)host[l];
+  CUDA_TRY(this, cudaMemcpyAsync(dst, tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, s));
+  CUDA_TRY(this, cudaStreamSynchronize(s));
+  return CAPAZ_OK;
+}
+
+int capaz_ctx::set_field(int field, const void* src, bool on_device, cudaStream_t s) {
+  CUDA_TRY(this, cudaSetDevice(device));
+  const size_t es = (p.form == CAPAZ_FORM_FP64) ? sizeof(double) : sizeof(float);
+  void* dst = nullptr;
+  if (field == CAPAZ_FIELD_M) {
+    dst = m;
+  } else if (field == CAPAZ_FIELD_K) {
+    if (!K) return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "K per cell needs CAPAZ_FLAG_PERCELL_K");
+    dst = K;
+  } else if (is_state_field(p, field)) {
+    dst = state[cur][state_slot(field)];
+  } else {
+    return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "field %d cannot be set", field);
+  }
+  if (!on_device) {
+    const double* h = static_cast<const double*>(src);
+    if (field == CAPAZ_FIELD_M || field == CAPAZ_FIELD_K) {
+      for (long long l = 0; l < n; l++)
+        if (!(h[l] > 0) || !isfinite(h[l]))
+          return fail(this, CAPAZ_ERR_BAD_STATE, "%s must be finite and > 0 (cell %lld: %g)",
+                      field == CAPAZ_FIELD_M ? "m" : "K", l, h[l]);
+      if (field == CAPAZ_FIELD_M) host_m.assign(h, h + n);
+    }
+    return upload_converted(dst, h, s);
+  }
+  CUDA_TRY(this, cudaMemcpyAsync(dst, src, n * es, cudaMemcpyDeviceToDevice, s));
+  if (field == CAPAZ_FIELD_M) host_m.clear();  // refreshed from the device when needed
+  return CAPAZ_OK;
+}
+
+int capaz_ctx::check_flag() {
+  unsigned int f = 0;
+  CUDA_TRY(this, cudaMemcpy(&f, err_flag, sizeof f, cudaMemcpyDeviceToHost));
+  if (f) return fail(this, CAPAZ_ERR_NONFINITE, "a step produced a non-finite P or S");
+  return CAPAZ_OK;
+}
+
+int capaz_ctx::get_field(int field, void* dst, bool on_device, cudaStream_t s) {
+  CUDA_TRY(this, cudaSetDevice(device));
+  if (field < 0 || field >= CAPAZ_FIELD_COUNT) return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "bad field %d", field);
+  const size_t es = (p.form == CAPAZ_FORM_FP64) ? sizeof(double) : sizeof(float);
+  const void* src = nullptr;
+  if (field == CAPAZ_FIELD_M) src = m;
+  else if (field == CAPAZ_FIELD_K) {
+    if (!K) return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "no per-cell K");
+    src = K;
+  } else if (is_state_field(p, field)) {
+    src = state[cur][state_slot(field)];
+  } else {
+    int st = derived(field, s);
+    if (st) return st;
+    src = scratch;
+    if (on_device) {
+      CUDA_TRY(this, cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      return CAPAZ_OK;
+    }
+    CUDA_TRY(this, cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(this, cudaStreamSynchronize(s));
+    return check_flag();
+  }
+  if (on_device) {
+    CUDA_TRY(this, cudaMemcpyAsync(dst, src, n * es, cudaMemcpyDeviceToDevice, s));
+    return CAPAZ_OK;
+  }
+  if (es == sizeof(double)) {
+    CUDA_TRY(this, cudaMemcpyAsync(dst, src, n * es, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(this, cudaStreamSynchronize(s));
+  } else {
+    std::vector<float> tmp(n);
+    CUDA_TRY(this, cudaMemcpyAsync(tmp.data(), src, n * es, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(this, cudaStreamSynchronize(s));
+    double* d = static_cast<double*>(dst);
+    for (long long l = 0; l < n; l++) d[l] = tmp[l];
+  }
+  return check_flag();
+}
+
+int capaz_ctx::init_state(cudaStream_t s) {
+  CUDA_TRY(this, cudaSetDevice(device));
+  if (host_m.empty()) {
+    // m was set from device memory: fetch it once.
+    host_m.resize(n);
+    int st = get_field(CAPAZ_FIELD_M, host_m.data(), false, s);
+    if (st) return st;
+  }
+  const long long sy = p.nx;
+  std::vector<double> Pw(n), Sn(n);
+  if (p.phases == 2) {
+    std::vector<double> ro_w(n), ro_n(n);
+    // i, j, k order as two-phase.cpp:116-118: the hydrostatic recurrence
+    // reads the cell above (j - 1), computed in the previous j iteration.
+    for (int i = 0; i < p.nx; i++)
+      for (int j = 0; j < p.ny; j++)
+        for (int k = 0; k < p.nz; k++) {
+          long long l = i + j * sy + (long long)k * sy * p.ny;
+          bool win = (i >= p.nx / 2 - p.source) && (i <= p.nx / 2 + p.source) && (k >= p.nz / 2 - p.source) &&
+                     (k <= p.nz / 2 + p.source);
+          Sn[l] = ((j == 0) && win) ? p.S_n_gr : p.S_n_background;
+          if (j == 0) {
+            Pw[l] = p.P_atm;
+          } else {
+            long long u = l - sy;
+            double ro_g_dy = (ro_n[u] * Sn[u] + ro_w[u] * (1 - Sn[u])) * (host_m[u]) * (p.g_const) * (p.hy);
+            Pw[l] = Pw[u] + ro_g_dy;
+          }
+          ro_w[l] = p.ro0_w * (1. + (p.beta_w) * (Pw[l] - p.P_atm));
+          ro_n[l] = p.ro0_n * (1. + (p.beta_n) * (Pw[l] - p.P_atm));
+        }
+    int st = upload_converted(state[cur][0], Pw.data(), s);
+    if (st) return st;
+    return upload_converted(state[cur][1], Sn.data(), s);
+  }
+  std::vector<double> Sw(n, p.S_w_init), Pn(n, p.P_atm), Pg(n, p.P_atm);
+  std::fill(Pw.begin(), Pw.end(), p.P_atm);
+  std::fill(Sn.begin(), Sn.end(), p.S_n_init);
+  double* src[5] = {Pw.data(), Sn.data(), Sw.data(), Pn.data(), Pg.data()};
+  for (int q = 0; q < 5; q++) {
+    int st = upload_converted(state[cur][q], src[q], s);
+    if (st) return st;
+  }
+  return CAPAZ_OK;
+}
+
+int capaz_ctx::sync() {
+  CUDA_TRY(this, cudaSetDevice(device));
+  CUDA_TRY(this, cudaDeviceSynchronize());
+  return check_flag();
+}
+
+int capaz_ctx::read_diag(capaz_diag* out, cudaStream_t s) {
+  CUDA_TRY(this, cudaSetDevice(device));
+  if (!(p.flags & CAPAZ_FLAG_DIAGNOSTICS))
+    return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "diagnostics need CAPAZ_FLAG_DIAGNOSTICS");
+  double h[DIAG_STRIDE];
+  CUDA_TRY(this, cudaMemcpyAsync(h, diag_out, sizeof h, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(this, cudaStreamSynchronize(s));
+  memset(out, 0, sizeof *out);
+  out->mass[0] = h[0];
+  out->mass[1] = h[1];
+  out->mass[2] = h[2];
+  out->max_residual = h[3];
+  out->nonfinite_cells = h[4];
+  return CAPAZ_OK;
+}

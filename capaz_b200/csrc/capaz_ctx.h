@@ -1,0 +1,63 @@
+// The context behind the opaque capaz_ctx handle of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "capaz_internal.h"
+
+struct capaz_ctx {
+  capaz_params p;
+  int device = 0;
+  long long n = 0;
+  // State ping-pong buffers: state[buffer][slot], slots P_w, S_n, S_w, P_n,
+  // P_g (the last three for three-phase only).  `cur` holds the current
+  // state; after a step the other buffer holds the start-of-step state, from
+  // which derived fields are materialised.
+  void* state[2][5] = {{nullptr}};
+  int cur = 0;
+  long long steps_done = 0;
+  void* m = nullptr;
+  void* K = nullptr;
+  unsigned int* err_flag = nullptr;  // set by kernels on non-finite results
+  double* diag_partials = nullptr;   // per-block diagnostics
+  int diag_blocks = 0;
+  double* diag_out = nullptr;        // reduced diagnostics (DIAG_STRIDE)
+  double* scratch = nullptr;         // one float64 field, derived fields
+  void* host_stage = nullptr;
+  std::vector<double> host_m;        // host copy of m for capaz_init_state
+  long long launches = 0;
+  std::string last_error;
+
+  static int state_slot(int field) {
+    switch (field) {
+      case CAPAZ_FIELD_P_W: return 0;
+      case CAPAZ_FIELD_S_N: return 1;
+      case CAPAZ_FIELD_S_W: return 2;
+      case CAPAZ_FIELD_P_N: return 3;
+      case CAPAZ_FIELD_P_G: return 4;
+      default: return -1;
+    }
+  }
+
+  int allocate();
+  void release();
+  int ensure_scratch();
+  int upload_converted(void* dst, const double* host, cudaStream_t s);
+  int set_field(int field, const void* src, bool on_device, cudaStream_t s);
+  int get_field(int field, void* dst, bool on_device, cudaStream_t s);
+  int derived(int field, cudaStream_t s);
+  int init_state(cudaStream_t s);
+  int step(int nsteps, cudaStream_t s);
+  int read_diag(capaz_diag* out, cudaStream_t s);
+  int check_flag();
+  int sync();
+  int fail_cuda(cudaError_t e, const char* what);
+  int fail_msg(int code, const char* msg);
+};
+
+namespace capaz {
+Step2Const make_step2_const(const capaz_params& p);
+}

@@ -1,0 +1,132 @@
+"""Python host mirror of the C ABI: one `Simulation` per capaz_ctx.
+
+Arrays are numpy float64 of shape (nz, ny, nx) in C order, i.e. the
+reference's index i + j*nx + k*nx*ny (main.cpp:695) with y vertical
+(j = 0 is the top face).  Device-resident variants take raw device pointers
+(e.g. torch tensors' data_ptr()) and a stream handle.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import native
+from .native import FIELDS, Diag, Params, check
+
+
+def default_params(**overrides) -> Params:
+    """The reference's Two-phase/defines.ini values, then `overrides`."""
+    lib = native.load()
+    p = Params()
+    check(lib.capaz_params_default(C.byref(p)))
+    for k, v in overrides.items():
+        setattr(p, "lambda_" if k == "lambda" else k, v)
+    return p
+
+
+def params_from_ini(path: str, base: Params | None = None) -> Params:
+    """Parses a defines.ini the way the reference's read_defines does."""
+    lib = native.load()
+    p = base.copy() if base is not None else default_params()
+    check(lib.capaz_params_from_ini(path.encode(), C.byref(p)))
+    return p
+
+
+def write_ini(p: Params, path: str, extensions: bool = True) -> None:
+    """Writes `p` as a defines.ini the reference reads (KEY=value lines)."""
+    keys = [
+        ("NX", p.nx), ("NY", p.ny), ("NZ", p.nz), ("HX", p.hx), ("HY", p.hy), ("HZ", p.hz),
+        ("DT", p.dt), ("TAU", 1e-7), ("L", 1e-4), ("C_W", 1500), ("C_N", 1000), ("C_G", 330),
+        ("BETA_W", p.beta_w), ("BETA_N", p.beta_n), ("BETA_G", p.beta_g),
+        ("RO_W", p.ro0_w), ("RO_N", p.ro0_n), ("RO_G", p.ro0_g),
+        ("MU_W", p.mu_w), ("MU_N", p.mu_n), ("MU_G", p.mu_g),
+        ("G_CONST", p.g_const), ("P_ATM", p.P_atm), ("LAMBDA_0", p.lambda_), ("LAMBDA_1", p.lambda_),
+        ("M_0", p.porosity), ("M_1", p.porosity), ("S_WR_0", p.S_wr), ("S_WR_1", p.S_wr),
+        ("S_NR_0", p.S_nr), ("S_NR_1", p.S_nr), ("S_GR_0", p.S_gr), ("S_GR_1", p.S_gr),
+        ("K_0", p.K0), ("K_1", p.K0), ("P_D_0", p.P_d), ("P_D_1", p.P_d),
+        ("P_D_NW_0", 0.0), ("P_D_NW_1", 0.0), ("P_D_GN_0", 0.0), ("P_D_GN_1", 0.0),
+        ("S_N_GR", p.S_n_gr), ("S_W_GR", p.S_w_gr), ("S_W_INIT", p.S_w_init), ("S_N_INIT", p.S_n_init),
+        ("SOURCE", p.source), ("ITERATIONS", p.newton_iterations), ("TIMEX", p.timeX),
+        ("SAVE_PLOTS", 1000000), ("PRINT_SCREEN", 1000000),
+        ("Q", 0.0), ("BACKGROUND_Pw", p.P_atm), ("BACKGROUND_Sn", 0.0),
+        ("INJECTION_WELL_Pw", p.P_atm), ("INJECTION_WELL_Sn", 0.0),
+        ("OUTPUT_WELL_Pw", p.P_atm), ("OUTPUT_WELL_Sn", 0.0),
+    ]
+    if extensions:
+        keys += [("P_TOP_OFFSET", p.P_top_offset), ("S_N_BACKGROUND", p.S_n_background),
+                 ("PERCELL_K", 1 if p.flags & native.FLAG_PERCELL_K else 0), ("PHASES", p.phases)]
+    with open(path, "w") as f:
+        f.write("# written by capaz_b200.simulation.write_ini\n")
+        for k, v in keys:
+            f.write(f"{k}={v!r}\n" if isinstance(v, float) else f"{k}={v}\n")
+
+
+class Simulation:
+    """A context of the C ABI (capaz_create ... capaz_destroy)."""
+
+    def __init__(self, params: Params, device: int = 0):
+        self.lib = native.load()
+        st = C.c_int(0)
+        self.params = params.copy()
+        self.ctx = self.lib.capaz_create(C.byref(self.params), device, C.byref(st))
+        if not self.ctx:
+            msg = self.lib.capaz_last_error(None)
+            raise native.CapazError(st.value, msg.decode() if msg else "")
+        self.shape = (params.nz, params.ny, params.nx)
+
+    # -- lifetime --------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self.lib.capaz_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- fields ----------------------------------------------------------
+    def set_field(self, name: str, arr, stream: int = 0) -> None:
+        a = np.ascontiguousarray(np.asarray(arr, dtype=np.float64).reshape(self.shape))
+        check(self.lib.capaz_set_field(self.ctx, FIELDS[name], a.ctypes.data, stream or None), self.ctx)
+
+    def get_field(self, name: str, stream: int = 0) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.float64)
+        check(self.lib.capaz_get_field(self.ctx, FIELDS[name], out.ctypes.data, stream or None), self.ctx)
+        return out
+
+    def set_field_device(self, name: str, dev_ptr: int, stream: int = 0) -> None:
+        check(self.lib.capaz_set_field_device(self.ctx, FIELDS[name], dev_ptr, stream or None), self.ctx)
+
+    def get_field_device(self, name: str, dev_ptr: int, stream: int = 0) -> None:
+        check(self.lib.capaz_get_field_device(self.ctx, FIELDS[name], dev_ptr, stream or None), self.ctx)
+
+    # -- stepping --------------------------------------------------------
+    def init_state(self, stream: int = 0) -> None:
+        check(self.lib.capaz_init_state(self.ctx, stream or None), self.ctx)
+
+    def step(self, nsteps: int = 1, stream: int = 0) -> None:
+        check(self.lib.capaz_step(self.ctx, int(nsteps), stream or None), self.ctx)
+
+    def set_dt(self, dt: float) -> None:
+        check(self.lib.capaz_set_dt(self.ctx, float(dt)), self.ctx)
+
+    def diag(self, stream: int = 0) -> dict:
+        d = Diag()
+        check(self.lib.capaz_read_diag(self.ctx, C.byref(d), stream or None), self.ctx)
+        return {"mass": list(d.mass), "max_residual": d.max_residual, "nonfinite_cells": d.nonfinite_cells}
+
+    def sync(self) -> None:
+        check(self.lib.capaz_sync(self.ctx), self.ctx)
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.lib.capaz_launch_count(self.ctx))

@@ -1,0 +1,207 @@
+/*
+ * capaz_b200.h — C ABI of the Blackwell (sm_100a) implementation of the CAPAZ
+ * multiphase-filtration time step.
+ *
+ * The reference runs one time step as a sequence of stage functions
+ * (main.cpp:93-108, declared in defines.h:186-194): S_calculation,
+ * ro_P_Xi_calculation, u_calculation, roS_calculation, P_S_calculation and
+ * boundary_conditions, each a separate kernel over separately stored arrays
+ * (gpu.cu:243-650).  Here the whole step is one fused sweep over the grid:
+ * a cell's state (P_w, S_n[, S_w]) makes one HBM round trip per step and every
+ * derived quantity (S_w, P_n, rho, Xi, u, roS) lives in registers or shared
+ * memory.  Derived fields are materialised on request from the retained
+ * previous state (capaz_get_field), so nothing the reference stores is lost.
+ *
+ * Conventions shared with the reference:
+ *   - axes follow the reference: x = i, y = j (vertical; j = 0 is the top
+ *     face, gravity acts along +j), z = k (main.cpp:255-267, cpu.cpp:699-705);
+ *   - arrays are structure-of-arrays with index i + j*nx + k*nx*ny
+ *     (main.cpp:695), float64 at the boundary of this ABI;
+ *   - one rank: every cell is active (no_communication.cpp:3-8).
+ *
+ * Every entry point returns a status code (CAPAZ_OK == 0).  Nothing here
+ * calls exit() or throws across the ABI; the reference instead prints and
+ * exits (shared_test.cpp:23-33).  A context is not shared between threads.
+ */
+#ifndef CAPAZ_B200_H
+#define CAPAZ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CAPAZ_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum capaz_status {
+  CAPAZ_OK = 0,
+  CAPAZ_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad field id, bad value   */
+  CAPAZ_ERR_UNSUPPORTED_GRID = 2, /* nx,ny < 3, nz == 2, or too large        */
+  CAPAZ_ERR_CUDA = 3,             /* a CUDA runtime call failed              */
+  CAPAZ_ERR_OUT_OF_MEMORY = 4,
+  CAPAZ_ERR_NO_DEVICE = 5,
+  CAPAZ_ERR_NONFINITE = 6,        /* a step produced NaN/Inf (device flag)   */
+  CAPAZ_ERR_BAD_STATE = 7,        /* input state outside the model's domain  */
+  CAPAZ_ERR_INI = 8,              /* defines.ini could not be read / parsed  */
+  CAPAZ_ERR_UNSUPPORTED = 9       /* valid request this build does not do    */
+};
+
+/* ---- model / numerical form -------------------------------------------- */
+enum capaz_form {
+  /* FP64 storage and arithmetic, the reference's operation order, no FMA
+   * contraction: matches the reference CPU step (cpu.cpp + two-phase.cpp /
+   * three-phase.cpp) to the last bit except where libm and CUDA pow differ. */
+  CAPAZ_FORM_FP64 = 0,
+  /* FP32 storage of P, S, m, K; FP32 stencil with compensated (Kahan)
+   * accumulation of the flux divergence; FP64 delta-form Newton and FP64
+   * mass balance. */
+  CAPAZ_FORM_FP32C = 1
+};
+
+/* Flags (capaz_params.flags). */
+#define CAPAZ_FLAG_PERCELL_K 0x1u /* Xi uses K[cell] instead of K0 (extension) */
+#define CAPAZ_FLAG_DIAGNOSTICS 0x2u /* reduce mass balance + max residual each step */
+
+/*
+ * Physical and numerical parameters: the subset of the reference's `consts`
+ * (defines.h:79-113) that the time step reads, plus the extensions listed at
+ * the end.  Units are SI, as in defines.ini.  Only media 0 is used, as in the
+ * reference (two-phase.cpp:6).
+ */
+typedef struct capaz_params {
+  int32_t nx, ny, nz;        /* NX, NY, NZ                                    */
+  int32_t phases;            /* 2 (TWO_PHASE) or 3 (THREE_PHASE)              */
+  int32_t form;              /* enum capaz_form                               */
+  int32_t newton_iterations; /* ITERATIONS                                    */
+  int32_t source;            /* SOURCE: half-width of the top source window   */
+  uint32_t flags;            /* CAPAZ_FLAG_*                                  */
+  double hx, hy, hz, dt;     /* HX, HY, HZ, DT                                */
+  double beta_w, beta_n, beta_g; /* BETA_W, BETA_N, BETA_G                    */
+  double ro0_w, ro0_n, ro0_g;    /* RO_W, RO_N, RO_G                          */
+  double mu_w, mu_n, mu_g;       /* MU_W, MU_N, MU_G                          */
+  double g_const, P_atm;     /* G_CONST, P_ATM                                */
+  double lambda;             /* LAMBDA_0                                      */
+  double S_wr, S_nr, S_gr;   /* S_WR_0, S_NR_0, S_GR_0                        */
+  double P_d;                /* P_D_0 (two-phase entry pressure)              */
+  double S_n_gr, S_w_gr;     /* S_N_GR, S_W_GR: saturations on the source     */
+  double S_w_init, S_n_init; /* S_W_INIT, S_N_INIT (three-phase initial state) */
+  double porosity;           /* M_0: porosity used by capaz_init_state        */
+  double K0;                 /* K_0: permeability when K is uniform           */
+  double timeX;              /* TIMEX (informational)                         */
+  /* ---- extensions (neutral values reproduce the reference exactly) ---- */
+  double P_top_offset;       /* top-face P_w = P_atm + P_top_offset (0)       */
+  double S_n_background;     /* two-phase initial S_n off the source (0)      */
+  double reserved[8];
+} capaz_params;
+
+/* Field identifiers for capaz_set_field / capaz_get_field. */
+enum capaz_field {
+  /* state (read-write) */
+  CAPAZ_FIELD_P_W = 0,
+  CAPAZ_FIELD_S_N = 1,
+  CAPAZ_FIELD_S_W = 2,  /* state for three-phase; derived (1 - S_n) for two */
+  CAPAZ_FIELD_M = 3,    /* porosity per cell                                */
+  CAPAZ_FIELD_K = 4,    /* permeability per cell (CAPAZ_FLAG_PERCELL_K)     */
+  CAPAZ_FIELD_P_N = 5,  /* derived; three-phase: state on boundary cells    */
+  CAPAZ_FIELD_P_G = 6,  /* derived; three-phase: state on boundary cells    */
+  /* derived at the start of the last step (read-only), as the reference's
+   * arrays hold them after time_step_function returns */
+  CAPAZ_FIELD_S_G = 7,
+  CAPAZ_FIELD_RO_W = 8,
+  CAPAZ_FIELD_RO_N = 9,
+  CAPAZ_FIELD_RO_G = 10,
+  CAPAZ_FIELD_XI_W = 11,
+  CAPAZ_FIELD_XI_N = 12,
+  CAPAZ_FIELD_XI_G = 13,
+  CAPAZ_FIELD_UX_W = 14, CAPAZ_FIELD_UY_W = 15, CAPAZ_FIELD_UZ_W = 16,
+  CAPAZ_FIELD_UX_N = 17, CAPAZ_FIELD_UY_N = 18, CAPAZ_FIELD_UZ_N = 19,
+  CAPAZ_FIELD_UX_G = 20, CAPAZ_FIELD_UY_G = 21, CAPAZ_FIELD_UZ_G = 22,
+  CAPAZ_FIELD_ROS_W = 23,     /* conserved update before Newton (interior)  */
+  CAPAZ_FIELD_ROS_N = 24,
+  CAPAZ_FIELD_ROS_G = 25,
+  CAPAZ_FIELD_ROS_W_OLD = 26, /* rho*S at the start of the step (interior)  */
+  CAPAZ_FIELD_ROS_N_OLD = 27,
+  CAPAZ_FIELD_ROS_G_OLD = 28,
+  CAPAZ_FIELD_COUNT = 29
+};
+
+/* Per-step diagnostics (CAPAZ_FLAG_DIAGNOSTICS), reduced on the device with
+ * warp shuffles over the interior cells after the step:
+ *   mass[p]      = sum over interior cells of m * rho_p(P) * S_p * hx*hy*hz
+ *   max_residual = max over interior cells of the Newton residual at the
+ *                  final iterate, max_p |F_p| / ro0_p (F_p = rho_p(P) S_p -
+ *                  roS_p, the reference's Newton functions) — a saturation-
+ *                  equivalent, dimensionless residual;
+ *   nonfinite_cells = interior cells whose new P or S is NaN/Inf. */
+typedef struct capaz_diag {
+  double mass[3];
+  double max_residual;
+  double nonfinite_cells;
+} capaz_diag;
+
+typedef struct capaz_ctx capaz_ctx;
+
+/* Library / parameters ----------------------------------------------------- */
+int capaz_abi_version(void);
+/* sizeof(capaz_params) and sizeof(capaz_diag) as compiled into the library,
+ * so bindings in other languages can check their struct layouts. */
+size_t capaz_params_size(void);
+size_t capaz_diag_size(void);
+/* Fills the reference's Two-phase/defines.ini defaults for the fields it sets
+ * (used where a defines.ini omits a key) and the neutral extension values. */
+int capaz_params_default(capaz_params* p);
+/* Parses a defines.ini the way read_defines does (main.cpp:1280-1639):
+ * "KEY=value" lines, '#' comment lines, the value ending at the first space.
+ * Keys not in the file keep their value in *p. */
+int capaz_params_from_ini(const char* path, capaz_params* p);
+/* Checks a parameter set; returns CAPAZ_OK or the reason it is rejected. */
+int capaz_params_validate(const capaz_params* p);
+
+/* Context ------------------------------------------------------------------ */
+/* Creates a context on CUDA device `device` and allocates all device memory
+ * the step needs (state ping-pong buffers, m, K, derived-field scratch on
+ * demand).  On failure returns NULL and writes the reason to *status. */
+capaz_ctx* capaz_create(const capaz_params* p, int device, int* status);
+int capaz_destroy(capaz_ctx* ctx);
+int capaz_get_params(const capaz_ctx* ctx, capaz_params* out);
+/* Message for the last error on this context (static storage). */
+const char* capaz_last_error(const capaz_ctx* ctx);
+
+/* Host <-> device (float64 host arrays of nx*ny*nz values).  `stream` is a
+ * cudaStream_t or NULL for the legacy default stream.  set_field validates the
+ * state it receives: m must be > 0 and finite, K > 0 and finite. */
+int capaz_set_field(capaz_ctx* ctx, int field, const double* host, void* stream);
+int capaz_get_field(capaz_ctx* ctx, int field, double* host, void* stream);
+/* Device-resident variants: `dev` is a device pointer of the context's device
+ * holding nx*ny*nz values of the storage type of the form (float64 for
+ * CAPAZ_FORM_FP64, float32 for the state of CAPAZ_FORM_FP32C). */
+int capaz_set_field_device(capaz_ctx* ctx, int field, const void* dev, void* stream);
+int capaz_get_field_device(capaz_ctx* ctx, int field, void* dev, void* stream);
+
+/* The reference's initial state (two-phase.cpp:113-172, three-phase.cpp:
+ * 438-500), computed on the host with the porosity already set in the
+ * context (CAPAZ_FIELD_M; M_0 everywhere if never set) and uploaded. */
+int capaz_init_state(capaz_ctx* ctx, void* stream);
+
+/* Advances `nsteps` time steps on `stream`; t is not used by the scheme
+ * (the reference's roS_calculation ignores it in the NR form).  With
+ * CAPAZ_FLAG_DIAGNOSTICS the diagnostics of the last step are kept on the
+ * device; capaz_read_diag copies them out (synchronising on `stream`). */
+int capaz_step(capaz_ctx* ctx, int nsteps, void* stream);
+int capaz_read_diag(capaz_ctx* ctx, capaz_diag* out, void* stream);
+/* Sets dt for the following steps (a per-step parameter in the reference:
+ * consts.dt); host value, no device traffic beyond the kernel argument. */
+int capaz_set_dt(capaz_ctx* ctx, double dt);
+
+/* Number of kernels the library launched on this context so far. */
+int64_t capaz_launch_count(const capaz_ctx* ctx);
+/* Synchronises the context's device and reports any pending CUDA error. */
+int capaz_sync(capaz_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CAPAZ_B200_H */

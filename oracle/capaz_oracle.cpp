@@ -1,0 +1,710 @@
+// capaz_oracle.cpp — CPU restatement of the reference time step (the oracle).
+//
+// TEST INFRASTRUCTURE.  Only tests/, __graft_entry__.smoke() and bench.py's
+// cpu_baseline leg load this library, and only as the parity reference or the timed
+// CPU baseline.  The product (capaz_b200/) never calls it.
+//
+// What it follows, stage by stage, in the reference's own operation order so
+// that IEEE-754 double arithmetic reproduces the reference bit for bit:
+//   S_calculation          cpu.cpp:28-36, 171-182
+//   ro_P_Xi_calculation    cpu.cpp:3-15, 143-169; two-phase.cpp:4-23;
+//                          three-phase.cpp:11-240
+//   u_calculation          cpu.cpp:17-26, 185-207, 266-314, 346-477
+//   roS_calculation (NR)   cpu.cpp:52-65, 236-314, 619-731
+//   P_S_calculation        cpu.cpp:80-89; two-phase.cpp:25-56;
+//                          three-phase.cpp:286-339 with gauss.cpp:6-92
+//   boundary_conditions    cpu.cpp:91-141; two-phase.cpp:59-111;
+//                          three-phase.cpp:345-427; main.cpp:255-267
+//   data_initialization    two-phase.cpp:113-172; three-phase.cpp:429-500
+// Loops run over cells in parallel (OpenMP): every stage writes only its own
+// cell and reads values of the previous stage, and on grids with nx, ny >= 3
+// and nz == 1 or nz >= 3 each boundary cell reads an interior cell, so the
+// result does not depend on the loop order.
+//
+// Extensions (neutral values reproduce the reference exactly; parity of the
+// non-neutral values is unpinned by the reference):
+//   - per-cell permeability K[cell] in Xi (CAPAZ_FLAG_PERCELL_K), as the
+//     Buckley-Leverett module does (b-l.cpp:65-66);
+//   - top-face pressure P_atm + P_top_offset in Border_P;
+//   - two-phase background initial S_n (S_n_background) off the source window;
+//   - per-cell porosity m at initialisation.
+#include <math.h>
+#include <omp.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "../include/capaz_b200.h"
+
+namespace {
+
+struct Grid {
+  int nx, ny, nz;
+  long sx, sy, sz, n;
+  Grid(const capaz_params* p) : nx(p->nx), ny(p->ny), nz(p->nz) {
+    sx = 1;
+    sy = nx;
+    sz = (long)nx * ny;
+    n = sz * nz;
+  }
+  long at(int i, int j, int k) const { return i + (long)j * sy + (long)k * sz; }
+  // Cells where roS and Newton run (cpu.cpp:621, two-phase.cpp:27).
+  bool interior(int i, int j, int k) const {
+    return (((i != 0) && (i != nx - 1)) || (nx < 2)) && (j != 0) && (j != ny - 1) &&
+           (((k != 0) && (k != nz - 1)) || (nz < 2));
+  }
+  // set_boundary_basic_coordinate, CPU form (cpu.cpp:107-141).
+  long basic(int i, int j, int k) const {
+    int i1 = i, j1 = j, k1 = k;
+    if ((i == 0) && (nx > 2)) i1++;
+    if ((i == nx - 1) && (nx > 2)) i1--;
+    if (j == 0) j1++;
+    if (j == ny - 1) j1--;
+    if ((k == 0) && (nz > 2)) k1++;
+    if ((k == nz - 1) && (nz > 2)) k1--;
+    return at(i1, j1, k1);
+  }
+};
+
+// right_difference / left_difference / central_difference (cpu.cpp:185-314).
+inline double rdiff(const double* a, long l, long s, double h) { return (a[l + s] - a[l]) / h; }
+inline double ldiff(const double* a, long l, long s, double h) { return (a[l] - a[l - s]) / h; }
+inline double cdiff(const double* a, long l, long s, double h) { return (a[l + s] - a[l - s]) / (2. * h); }
+
+// directed_difference (cpu.cpp:236-264): first-order upwind flux difference.
+inline double directed(double x1, double x2, const double* Xi, const double* ro, long l, long s,
+                       double h) {
+  return (((x2 + fabs(x2)) / 2. - (x1 - fabs(x1)) / 2.) * (-1.) * Xi[l] * ro[l] -
+          (x1 + fabs(x1)) / 2. * (-1.) * Xi[l - s] * ro[l - s] +
+          (x2 - fabs(x2)) / 2. * (-1.) * Xi[l + s] * ro[l + s]) /
+         h;
+}
+
+// reverse_matrix: Gauss-Jordan inverse that pivots only when |pivot| < 1e-8
+// (gauss.cpp:6-92).  Returns 0, -1 (singular) or -2 (bad arguments).
+int reverse_matrix(double* a, int n) {
+  if (a == NULL || n < 2) return -2;
+  const double e = 1E-8;
+  const int n1 = n * 2;
+  double matr[2 * 8 * 8];
+  double row[2 * 8];
+  if (n > 8) return -2;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) matr[j + n1 * i] = a[j + n * i];
+  for (int i = 0; i < n; i++)
+    for (int j = n; j < n1; j++) matr[j + n1 * i] = (j == n + i) ? 1 : 0;
+  for (int k = 0; k < n; k++) {
+    double f = matr[k + n1 * k];
+    if (fabs(f) < e) {
+      int det_flag = 0;
+      for (int i = k + 1; i < n; i++) {
+        if (matr[k + n1 * i] > e) {
+          det_flag = 1;
+          for (int j = 0; j < n1; j++) {
+            row[j] = matr[j + n1 * k];
+            matr[j + n1 * k] = matr[j + n1 * i];
+            matr[j + n1 * i] = row[j];
+          }
+          f = matr[k + n1 * k];
+        }
+      }
+      if (det_flag == 0) return -1;
+    }
+    for (int j = 0; j < n1; j++) matr[j + n1 * k] /= f;
+    for (int i = 0; i < n; i++)
+      if (i != k) {
+        double f1 = matr[k + n1 * i];
+        for (int j = 0; j < n1; j++) matr[j + n1 * i] -= (matr[j + n1 * k] * f1);
+      }
+  }
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) a[j + n * i] = matr[j + n + n1 * i];
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Three-phase constitutive relations, CPU form (three-phase.cpp:11-186).  The
+// CPU capillary pressures and their derivatives are identically zero
+// (three-phase.cpp:25,32,39,47,58,80,103,125).
+inline double k_w3(double S_w_e, double A) {
+  double k_w = 0;
+  if (S_w_e >= 1e-3) k_w = pow(S_w_e, 0.5) * pow(1. - pow(1. - pow(S_w_e, A / (A - 1.)), (A - 1.) / A), 2.);
+  return k_w;
+}
+inline double k_g3(double S_g_e, double A) {
+  double k_g = 0;
+  if (S_g_e >= 1e-3) k_g = pow(S_g_e, 0.5) * pow(1. - pow(1. - S_g_e, A / (A - 1.)), 2. * (A - 1.) / A);
+  return k_g;
+}
+inline double k_n3(double S_w_e, double S_n_e, double A) {
+  double k_n = 0;
+  double S_g_e = 1. - S_w_e - S_n_e;
+  if (S_n_e >= 1e-3) {
+    double k_n_w = pow(1. - S_w_e, 0.5) * pow(1. - pow(S_w_e, A / (A - 1.)), 2. * (A - 1.) / A);
+    double k_n_g = pow(S_n_e, 0.5) * pow(1. - pow(1. - pow(S_n_e, A / (A - 1.)), (A - 1.) / A), 2.);
+    k_n = S_n_e * k_n_w * k_n_g / (1 - S_w_e) / (1 - S_g_e);
+  }
+  return k_n;
+}
+
+struct Work {
+  std::vector<double> S_w, S_g, P_n, P_g, ro_w, ro_n, ro_g, Xi_w, Xi_n, Xi_g;
+  std::vector<double> roS_w, roS_n, roS_g, roS_w_old, roS_n_old, roS_g_old;
+  // Three-phase: P_n, P_g as u_calculation sees them (after ro_P_Xi), kept
+  // when keep_u_pressures is set.
+  bool keep_u_pressures = false;
+  std::vector<double> Pn_u, Pg_u;
+};
+
+inline bool in_window(const capaz_params* p, int i, int k) {
+  return (i >= p->nx / 2 - p->source) && (i <= p->nx / 2 + p->source) && (k >= p->nz / 2 - p->source) &&
+         (k <= p->nz / 2 + p->source);
+}
+
+inline double Kc(const capaz_params* p, const double* K, long l) {
+  return ((p->flags & CAPAZ_FLAG_PERCELL_K) && K) ? K[l] : p->K0;
+}
+
+// ---------------------------------------------------------------------------
+// Two-phase step.
+void step2(const capaz_params* p, const Grid& g, double* P_w, double* S_n, const double* m,
+           const double* K, Work& w) {
+  const double lam = p->lambda, S_wr = p->S_wr;
+  const double e_kw = (2. + 3. * lam) / lam, e_kn = (2. + lam) / lam, e_pk = -1. / lam;
+  double *S_w = w.S_w.data(), *P_n = w.P_n.data(), *ro_w = w.ro_w.data(), *ro_n = w.ro_n.data();
+  double *Xi_w = w.Xi_w.data(), *Xi_n = w.Xi_n.data();
+  double *roS_w = w.roS_w.data(), *roS_n = w.roS_n.data();
+  double *roS_w_old = w.roS_w_old.data(), *roS_n_old = w.roS_n_old.data();
+
+  // S_calculation (all cells).
+#pragma omp parallel for schedule(static)
+  for (long l = 0; l < g.n; l++) S_w[l] = 1. - S_n[l];
+
+  // ro_P_Xi_calculation (all cells are active on one rank).
+#pragma omp parallel for schedule(static)
+  for (long l = 0; l < g.n; l++) {
+    double S_e = (1. - S_n[l] - S_wr) / (1. - S_wr);
+    double k_w = pow(S_e, e_kw);
+    double k_n = (1. - S_e) * (1. - S_e) * (1 - pow(S_e, e_kn));
+    double P_k = p->P_d * pow((1. - S_n[l] - S_wr) / (1. - S_wr), e_pk);
+    P_n[l] = P_w[l] + P_k;
+    Xi_w[l] = -1. * Kc(p, K, l) * k_w / p->mu_w;
+    Xi_n[l] = -1. * Kc(p, K, l) * k_n / p->mu_n;
+    ro_w[l] = p->ro0_w * (1. + (p->beta_w) * (P_w[l] - p->P_atm));
+    ro_n[l] = p->ro0_n * (1. + (p->beta_n) * (P_n[l] - p->P_atm));
+  }
+
+  // roS_calculation, NR form (assign_roS_nr).
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        if (!g.interior(i, j, k)) continue;
+        long l = g.at(i, j, k);
+        if (!m[l]) continue;
+        const double q_w = 0., q_n = 0.;  // wells_q (two-phase.cpp:187-192)
+        roS_w[l] = ro_w[l] * (1. - S_n[l]);
+        roS_n[l] = ro_n[l] * S_n[l];
+        double x1, x2, fx_w, fy_w, fz_w, fx_n, fy_n, fz_n;
+        if (g.nz < 2) {
+          fz_w = 0.;
+          fz_n = 0.;
+        } else {
+          x2 = -1. * rdiff(P_w, l, g.sz, p->hz);
+          x1 = -1. * ldiff(P_w, l, g.sz, p->hz);
+          fz_w = directed(x1, x2, Xi_w, ro_w, l, g.sz, p->hz);
+          x2 = -1. * rdiff(P_n, l, g.sz, p->hz);
+          x1 = -1. * ldiff(P_n, l, g.sz, p->hz);
+          fz_n = directed(x1, x2, Xi_n, ro_n, l, g.sz, p->hz);
+        }
+        if (g.nx < 2) {
+          fx_w = 0.;
+          fx_n = 0.;
+        } else {
+          x2 = -1. * rdiff(P_w, l, g.sx, p->hx);
+          x1 = -1. * ldiff(P_w, l, g.sx, p->hx);
+          fx_w = directed(x1, x2, Xi_w, ro_w, l, g.sx, p->hx);
+          x2 = -1. * rdiff(P_n, l, g.sx, p->hx);
+          x1 = -1. * ldiff(P_n, l, g.sx, p->hx);
+          fx_n = directed(x1, x2, Xi_n, ro_n, l, g.sx, p->hx);
+        }
+        x2 = -1. * rdiff(P_w, l, g.sy, p->hy) + p->g_const * (ro_w[l]);
+        x1 = -1. * ldiff(P_w, l, g.sy, p->hy) + p->g_const * (ro_w[l]);
+        fy_w = directed(x1, x2, Xi_w, ro_w, l, g.sy, p->hy);
+        x2 = -1. * rdiff(P_n, l, g.sy, p->hy) + p->g_const * (ro_n[l]);
+        x1 = -1. * ldiff(P_n, l, g.sy, p->hy) + p->g_const * (ro_n[l]);
+        fy_n = directed(x1, x2, Xi_n, ro_n, l, g.sy, p->hy);
+        double A1 = roS_w[l] - (p->dt / m[l]) * (-q_w + fx_w + fy_w + fz_w);
+        double A2 = roS_n[l] - (p->dt / m[l]) * (-q_n + fx_n + fy_n + fz_n);
+        roS_w_old[l] = roS_w[l];
+        roS_n_old[l] = roS_n[l];
+        roS_w[l] = A1;
+        roS_n[l] = A2;
+      }
+
+  // P_S_calculation (Newton, two-phase.cpp:25-56).
+  const double P_d = p->P_d;
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        if (!g.interior(i, j, k)) continue;
+        long l = g.at(i, j, k);
+        double Pw = P_w[l], Sn = S_n[l];
+        for (int it = 1; it <= p->newton_iterations; it++) {
+          double S_e = (1 - Sn - S_wr) / (1 - S_wr);
+          double P_k = P_d * pow(S_e, (-1.) / lam);
+          double AAA = pow(S_e, (((-1.) / lam) - 1.));
+          double F1 = p->ro0_w * (1. + (p->beta_w) * (Pw - p->P_atm)) * (1. - Sn) - roS_w[l];
+          double F2 = p->ro0_n * (1. + (p->beta_n) * (Pw + P_k - p->P_atm)) * Sn - roS_n[l];
+          double PkS = AAA * (P_d) / (lam * (1 - S_wr));
+          double F1P = p->ro0_w * (p->beta_w) * (1 - Sn);
+          double F2P = p->ro0_n * (p->beta_n) * Sn;
+          double F1S = (-1) * (p->ro0_w) * (1 + (p->beta_w) * (Pw - p->P_atm));
+          double F2S = p->ro0_n * (1 + (p->beta_n) * (Pw + P_k - p->P_atm + (Sn * PkS)));
+          double det = F1P * F2S - F1S * F2P;
+          double nPw = Pw - (1 / det) * (F2S * F1 - F1S * F2);
+          double nSn = Sn - (1 / det) * (F1P * F2 - F2P * F1);
+          Pw = nPw;
+          Sn = nSn;
+        }
+        P_w[l] = Pw;
+        S_n[l] = Sn;
+      }
+
+  // boundary_conditions: Border_S then Border_P per boundary cell.
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        bool bnd = (i == 0) || (i == g.nx - 1) || (j == 0) || (j == g.ny - 1) ||
+                   (((k == 0) || (k == g.nz - 1)) && (g.nz >= 2));
+        if (!bnd) continue;
+        long l1 = g.basic(i, j, k);
+        long l = g.at(i, j, k);
+        if ((j != 0) || (p->source <= 0)) S_n[l] = S_n[l1];
+        if ((j == 0) && (p->source > 0)) S_n[l] = in_window(p, i, k) ? p->S_n_gr : S_n[l1];
+        if ((j != 0) && (j != g.ny - 1)) {
+          P_w[l] = P_w[l1];
+        } else if (j == 0) {
+          P_w[l] = p->P_atm + p->P_top_offset;
+        } else {
+          double ro_g_dy = (ro_n[l1] * S_n[l1] + ro_w[l1] * (1 - S_n[l1])) * (m[l1]) * (p->g_const) * (p->hy);
+          P_w[l] = P_w[l1] + ro_g_dy;
+        }
+      }
+}
+
+// ---------------------------------------------------------------------------
+// Three-phase step (CPU physics).
+void step3(const capaz_params* p, const Grid& g, double* P_w, double* S_w, double* S_n, double* P_n,
+           double* P_g, const double* m, const double* K, Work& w) {
+  const double A = p->lambda;
+  const double den = 1. - p->S_wr - p->S_nr - p->S_gr;
+  double *S_g = w.S_g.data(), *ro_w = w.ro_w.data(), *ro_n = w.ro_n.data(), *ro_g = w.ro_g.data();
+  double *Xi_w = w.Xi_w.data(), *Xi_n = w.Xi_n.data(), *Xi_g = w.Xi_g.data();
+  double *roS_w = w.roS_w.data(), *roS_n = w.roS_n.data(), *roS_g = w.roS_g.data();
+  double *roS_w_old = w.roS_w_old.data(), *roS_n_old = w.roS_n_old.data(), *roS_g_old = w.roS_g_old.data();
+
+  // S_calculation (all cells).
+#pragma omp parallel for schedule(static)
+  for (long l = 0; l < g.n; l++) S_g[l] = 1. - S_w[l] - S_n[l];
+
+  // ro_P_Xi_calculation: Xi and rho on all cells, P_n and P_g on interior
+  // cells only (three-phase.cpp:225-235).
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        long l = g.at(i, j, k);
+        double S_w_e = (S_w[l] - p->S_wr) / den;
+        double S_n_e = (S_n[l] - p->S_nr) / den;
+        double S_g_e = 1. - S_w_e - S_n_e;
+        double k_w = k_w3(S_w_e, A), k_g = k_g3(S_g_e, A), k_n = k_n3(S_w_e, S_n_e, A);
+        double Kl = Kc(p, K, l);
+        Xi_w[l] = (-1.) * Kl * k_w / p->mu_w;
+        Xi_n[l] = (-1.) * Kl * k_n / p->mu_n;
+        Xi_g[l] = (-1.) * Kl * k_g / p->mu_g;
+        if (g.interior(i, j, k)) {
+          const double Pk_nw = 0, Pk_gn = 0;
+          P_n[l] = P_w[l] + Pk_nw;
+          P_g[l] = P_w[l] + Pk_nw + Pk_gn;
+        }
+        ro_w[l] = p->ro0_w * (1. + (p->beta_w) * (P_w[l] - p->P_atm));
+        ro_n[l] = p->ro0_n * (1. + (p->beta_n) * (P_n[l] - p->P_atm));
+        ro_g[l] = p->ro0_g * P_g[l] / p->P_atm;
+      }
+  if (w.keep_u_pressures) {
+    w.Pn_u.assign(P_n, P_n + g.n);
+    w.Pg_u.assign(P_g, P_g + g.n);
+  }
+
+  // roS_calculation, NR form.
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        if (!g.interior(i, j, k)) continue;
+        long l = g.at(i, j, k);
+        if (!m[l]) continue;
+        const double q_w = 0., q_n = 0., q_g = 0.;  // wells_q (three-phase.cpp:529-550)
+        roS_w[l] = ro_w[l] * S_w[l];
+        roS_g[l] = ro_g[l] * (1. - S_w[l] - S_n[l]);
+        roS_n[l] = ro_n[l] * S_n[l];
+        double x1, x2, fx_w, fy_w, fz_w, fx_n, fy_n, fz_n, fx_g, fy_g, fz_g;
+        if (g.nz < 2) {
+          fz_w = fz_n = fz_g = 0.;
+        } else {
+          x2 = -1. * rdiff(P_w, l, g.sz, p->hz);
+          x1 = -1. * ldiff(P_w, l, g.sz, p->hz);
+          fz_w = directed(x1, x2, Xi_w, ro_w, l, g.sz, p->hz);
+          x2 = -1. * rdiff(P_n, l, g.sz, p->hz);
+          x1 = -1. * ldiff(P_n, l, g.sz, p->hz);
+          fz_n = directed(x1, x2, Xi_n, ro_n, l, g.sz, p->hz);
+          x2 = -1. * rdiff(P_g, l, g.sz, p->hz);
+          x1 = -1. * ldiff(P_g, l, g.sz, p->hz);
+          fz_g = directed(x1, x2, Xi_g, ro_g, l, g.sz, p->hz);
+        }
+        if (g.nx < 2) {
+          fx_w = fx_n = fx_g = 0.;
+        } else {
+          x2 = -1. * rdiff(P_w, l, g.sx, p->hx);
+          x1 = -1. * ldiff(P_w, l, g.sx, p->hx);
+          fx_w = directed(x1, x2, Xi_w, ro_w, l, g.sx, p->hx);
+          x2 = -1. * rdiff(P_n, l, g.sx, p->hx);
+          x1 = -1. * ldiff(P_n, l, g.sx, p->hx);
+          fx_n = directed(x1, x2, Xi_n, ro_n, l, g.sx, p->hx);
+          x2 = -1. * rdiff(P_g, l, g.sx, p->hx);
+          x1 = -1. * ldiff(P_g, l, g.sx, p->hx);
+          fx_g = directed(x1, x2, Xi_g, ro_g, l, g.sx, p->hx);
+        }
+        x2 = -1. * rdiff(P_w, l, g.sy, p->hy) + p->g_const * (ro_w[l]);
+        x1 = -1. * ldiff(P_w, l, g.sy, p->hy) + p->g_const * (ro_w[l]);
+        fy_w = directed(x1, x2, Xi_w, ro_w, l, g.sy, p->hy);
+        x2 = -1. * rdiff(P_n, l, g.sy, p->hy) + p->g_const * (ro_n[l]);
+        x1 = -1. * ldiff(P_n, l, g.sy, p->hy) + p->g_const * (ro_n[l]);
+        fy_n = directed(x1, x2, Xi_n, ro_n, l, g.sy, p->hy);
+        double A1 = roS_w[l] - (p->dt / m[l]) * (-q_w + fx_w + fy_w + fz_w);
+        double A2 = roS_n[l] - (p->dt / m[l]) * (-q_n + fx_n + fy_n + fz_n);
+        roS_w_old[l] = roS_w[l];
+        roS_n_old[l] = roS_n[l];
+        roS_w[l] = A1;
+        roS_n[l] = A2;
+        x2 = -1. * rdiff(P_g, l, g.sy, p->hy) + p->g_const * (ro_g[l]);
+        x1 = -1. * ldiff(P_g, l, g.sy, p->hy) + p->g_const * (ro_g[l]);
+        fy_g = directed(x1, x2, Xi_g, ro_g, l, g.sy, p->hy);
+        double A3 = roS_g[l] - (p->dt / m[l]) * (q_g + fx_g + fy_g + fz_g);
+        roS_g_old[l] = roS_g[l];
+        roS_g[l] = A3;
+      }
+
+  // P_S_calculation: 3x3 Newton (three-phase.cpp:286-339).
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        if (!g.interior(i, j, k)) continue;
+        long l = g.at(i, j, k);
+        double Pw = P_w[l], Sw = S_w[l], Sn = S_n[l];
+        for (int it = 1; it <= p->newton_iterations; it++) {
+          const double Pk_nw = 0, Pk_gn = 0, PkSw = 0, PkSn = 0;
+          double Sg = 1. - Sw - Sn;
+          double F1 = p->ro0_w * (1. + (p->beta_w) * (Pw - p->P_atm)) * Sw - roS_w[l];
+          double F2 = p->ro0_n * (1. + (p->beta_n) * (Pw + Pk_nw - p->P_atm)) * Sn - roS_n[l];
+          double F3 = p->ro0_g * (Pw + Pk_nw + Pk_gn) / p->P_atm * Sg - roS_g[l];
+          double dF[9];
+          dF[0] = p->ro0_w * p->beta_w * Sw;
+          dF[3] = p->ro0_n * p->beta_n * Sn;
+          dF[6] = p->ro0_g * Sg / p->P_atm;
+          dF[1] = p->ro0_w * (1 + p->beta_w * (Pw - p->P_atm));
+          dF[4] = p->ro0_n * (1. + (p->beta_n) * PkSw) * Sn;
+          dF[7] = (-1) * p->ro0_g * (Pw + Pk_nw + Pk_gn - Sg * (PkSn + PkSw)) / p->P_atm;
+          dF[2] = 0;
+          dF[5] = p->ro0_n * (1. + p->beta_n * (Pw + Pk_nw - p->P_atm));
+          dF[8] = (-1) * p->ro0_g * (Pw + Pk_nw + Pk_gn - Sg * PkSn) / p->P_atm;
+          reverse_matrix(dF, 3);
+          double nPw = Pw - (dF[0] * F1 + dF[1] * F2 + dF[2] * F3);
+          double nSw = Sw - (dF[3] * F1 + dF[4] * F2 + dF[5] * F3);
+          double nSn = Sn - (dF[6] * F1 + dF[7] * F2 + dF[8] * F3);
+          Pw = nPw;
+          Sw = nSw;
+          Sn = nSn;
+        }
+        P_w[l] = Pw;
+        S_w[l] = Sw;
+        S_n[l] = Sn;
+      }
+
+  // boundary_conditions (three-phase.cpp:345-427).
+  const double gh = p->g_const * p->hy;
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        bool bnd = (((i == 0) || (i == g.nx - 1)) && (g.nx >= 2)) || (j == 0) || (j == g.ny - 1) ||
+                   (((k == 0) || (k == g.nz - 1)) && (g.nz >= 2));
+        if (!bnd) continue;
+        long l1 = g.basic(i, j, k);
+        long l = g.at(i, j, k);
+        if ((j != 0) || (p->source <= 0)) {
+          S_w[l] = S_w[l1];
+          S_n[l] = S_n[l1];
+        }
+        if ((j == 0) && (p->source > 0)) {
+          S_w[l] = p->S_w_gr;
+          S_n[l] = p->S_n_gr;
+        }
+        const double Pk_nw = 0, Pk_gn = 0;
+        (void)gh;
+        if ((j != 0) && (j != g.ny - 1)) {
+          P_w[l] = P_w[l1];
+          P_n[l] = P_w[l1] + Pk_nw;
+          P_g[l] = P_w[l1] + Pk_nw + Pk_gn;
+        } else if (j == 0) {
+          P_w[l] = (P_w[l1] - (p->ro0_w) * (p->g_const) * (p->hy) * (1. - (p->beta_w) * (p->P_atm))) /
+                   (1. + (p->beta_w) * (p->ro0_w) * (p->g_const) * (p->hy));
+          P_n[l] = (P_w[l1] + Pk_nw - (p->ro0_n) * (p->g_const) * (p->hy) * (1. - (p->beta_n) * (p->P_atm))) /
+                   (1. + (p->beta_n) * (p->ro0_n) * (p->g_const) * (p->hy));
+          P_g[l] = (P_w[l1] + Pk_nw + Pk_gn) / (1. + (p->ro0_g) * (p->g_const) * (p->hy) / (p->P_atm));
+        } else {
+          P_w[l] = (P_w[l1] + (p->ro0_w) * (p->g_const) * (p->hy) * (1. - (p->beta_w) * (p->P_atm))) /
+                   (1. - (p->beta_w) * (p->ro0_w) * (p->g_const) * (p->hy));
+          P_n[l] = (P_w[l1] + Pk_nw + (p->ro0_n) * (p->g_const) * (p->hy) * (1. - (p->beta_n) * (p->P_atm))) /
+                   (1. - (p->beta_n) * (p->ro0_n) * (p->g_const) * (p->hy));
+          P_g[l] = (P_w[l1] + Pk_nw + Pk_gn) / (1. - (p->ro0_g) * (p->g_const) * (p->hy) / (p->P_atm));
+        }
+      }
+}
+
+// u_calculation (cpu.cpp:346-477) for one phase, from the start-of-step arrays.
+void velocities(const capaz_params* p, const Grid& g, const double* P, const double* Xi, const double* ro,
+                double* ux, double* uy, double* uz) {
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        long l = g.at(i, j, k);
+        if (p->nx > 2) {
+          if (i == 0) ux[l] = Xi[l] * rdiff(P, l, g.sx, p->hx);
+          else if (i == g.nx - 1) ux[l] = Xi[l] * ldiff(P, l, g.sx, p->hx);
+          else ux[l] = Xi[l] * cdiff(P, l, g.sx, p->hx);
+        } else {
+          ux[l] = 0.;
+        }
+        if (p->ny > 2) {
+          if (j == 0) uy[l] = Xi[l] * (rdiff(P, l, g.sy, p->hy) - ro[l] * (p->g_const));
+          else if (j == g.ny - 1) uy[l] = Xi[l] * (ldiff(P, l, g.sy, p->hy) - ro[l] * (p->g_const));
+          else uy[l] = Xi[l] * (cdiff(P, l, g.sy, p->hy) - ro[l] * (p->g_const));
+        } else {
+          uy[l] = 0.;
+        }
+        if (p->nz > 2) {
+          if (k == 0) uz[l] = Xi[l] * rdiff(P, l, g.sz, p->hz);
+          else if (k == g.nz - 1) uz[l] = Xi[l] * ldiff(P, l, g.sz, p->hz);
+          else uz[l] = Xi[l] * cdiff(P, l, g.sz, p->hz);
+        } else {
+          uz[l] = 0.;
+        }
+      }
+}
+
+int check_grid(const capaz_params* p) {
+  if (!p) return CAPAZ_ERR_INVALID_ARGUMENT;
+  if (p->phases != 2 && p->phases != 3) return CAPAZ_ERR_INVALID_ARGUMENT;
+  // nx == 1 is the reference's three-phase column case (Three-phase/defines.ini).
+  const bool nx_ok = p->nx >= 3 || (p->phases == 3 && p->nx == 1);
+  if (!nx_ok || p->ny < 3 || p->nz < 1 || p->nz == 2) return CAPAZ_ERR_UNSUPPORTED_GRID;
+  return CAPAZ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Gauss-Jordan inverse of gauss.cpp:6-92 (row-major n x n, in place).
+int oracle_reverse_matrix(double* a, int n) { return reverse_matrix(a, n); }
+
+// data_initialization.  `m` (in/out): if m_in is non-NULL it gives the
+// porosity per cell, else M_0 is written everywhere.  Two-phase writes P_w,
+// S_n; three-phase also S_w, P_n, P_g.
+int oracle_init(const capaz_params* p, const double* m_in, double* m, double* P_w, double* S_w,
+                double* S_n, double* P_n, double* P_g) {
+  int rc = check_grid(p);
+  if (rc) return rc;
+  Grid g(p);
+  if (p->phases == 2) {
+    std::vector<double> ro_w(g.n), ro_n(g.n);
+    for (int i = 0; i < g.nx; i++)
+      for (int j = 0; j < g.ny; j++)
+        for (int k = 0; k < g.nz; k++) {
+          long l = g.at(i, j, k);
+          m[l] = m_in ? m_in[l] : p->porosity;
+          if ((j == 0) && in_window(p, i, k)) S_n[l] = p->S_n_gr;
+          else S_n[l] = p->S_n_background;
+          if (j == 0) {
+            P_w[l] = p->P_atm;
+          } else {
+            long u = l - g.sy;
+            double ro_g_dy = (ro_n[u] * S_n[u] + ro_w[u] * (1 - S_n[u])) * (m[u]) * (p->g_const) * (p->hy);
+            P_w[l] = P_w[u] + ro_g_dy;
+          }
+          ro_w[l] = p->ro0_w * (1. + (p->beta_w) * (P_w[l] - p->P_atm));
+          ro_n[l] = p->ro0_n * (1. + (p->beta_n) * (P_w[l] - p->P_atm));
+        }
+  } else {
+    for (long l = 0; l < g.n; l++) {
+      m[l] = m_in ? m_in[l] : p->porosity;
+      S_w[l] = p->S_w_init;
+      S_n[l] = p->S_n_init;
+      P_w[l] = p->P_atm;
+      P_n[l] = p->P_atm;
+      P_g[l] = p->P_atm;
+    }
+  }
+  return CAPAZ_OK;
+}
+
+// Advances nsteps.  Two-phase: P_w, S_n in/out (S_w, P_n, P_g may be NULL).
+// Three-phase: P_w, S_w, S_n, P_n, P_g in/out.  K may be NULL (uniform K0).
+// `derived`, if non-NULL, is an array of CAPAZ_FIELD_COUNT pointers (entries
+// may be NULL) that receive the derived fields of the LAST step, as the
+// reference's arrays hold them after time_step_function returns.
+// `diag`, if non-NULL, receives the diagnostics of the last step.
+int oracle_step(const capaz_params* p, int nsteps, double* P_w, double* S_w, double* S_n, double* P_n,
+                double* P_g, const double* m, const double* K, double** derived, capaz_diag* diag,
+                int nthreads) {
+  int rc = check_grid(p);
+  if (rc) return rc;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  Grid g(p);
+  Work w;
+  const long n = g.n;
+  w.S_w.assign(n, 0.);
+  w.P_n.assign(n, 0.);
+  w.ro_w.assign(n, 0.);
+  w.ro_n.assign(n, 0.);
+  w.Xi_w.assign(n, 0.);
+  w.Xi_n.assign(n, 0.);
+  w.roS_w.assign(n, 0.);
+  w.roS_n.assign(n, 0.);
+  w.roS_w_old.assign(n, 0.);
+  w.roS_n_old.assign(n, 0.);
+  if (p->phases == 3) {
+    w.S_g.assign(n, 0.);
+    w.ro_g.assign(n, 0.);
+    w.Xi_g.assign(n, 0.);
+    w.roS_g.assign(n, 0.);
+    w.roS_g_old.assign(n, 0.);
+  }
+  // Keep the start-of-step state of the last step for the velocities.
+  std::vector<double> Pw0;
+  for (int s = 0; s < nsteps; s++) {
+    bool last = (s == nsteps - 1);
+    if (last && derived) {
+      Pw0.assign(P_w, P_w + n);
+      w.keep_u_pressures = (p->phases == 3);
+    }
+    if (p->phases == 2) step2(p, g, P_w, S_n, m, K, w);
+    else step3(p, g, P_w, S_w, S_n, P_n, P_g, m, K, w);
+  }
+  if (derived && nsteps > 0) {
+    auto put = [&](int f, const std::vector<double>& v) {
+      if (derived[f] && !v.empty()) memcpy(derived[f], v.data(), sizeof(double) * n);
+    };
+    if (p->phases == 2) {
+      put(CAPAZ_FIELD_S_W, w.S_w);
+      put(CAPAZ_FIELD_P_N, w.P_n);
+    } else {
+      put(CAPAZ_FIELD_S_G, w.S_g);
+      put(CAPAZ_FIELD_RO_G, w.ro_g);
+      put(CAPAZ_FIELD_XI_G, w.Xi_g);
+      put(CAPAZ_FIELD_ROS_G, w.roS_g);
+      put(CAPAZ_FIELD_ROS_G_OLD, w.roS_g_old);
+    }
+    put(CAPAZ_FIELD_RO_W, w.ro_w);
+    put(CAPAZ_FIELD_RO_N, w.ro_n);
+    put(CAPAZ_FIELD_XI_W, w.Xi_w);
+    put(CAPAZ_FIELD_XI_N, w.Xi_n);
+    put(CAPAZ_FIELD_ROS_W, w.roS_w);
+    put(CAPAZ_FIELD_ROS_N, w.roS_n);
+    put(CAPAZ_FIELD_ROS_W_OLD, w.roS_w_old);
+    put(CAPAZ_FIELD_ROS_N_OLD, w.roS_n_old);
+    // Velocities from the start-of-step pressures (P_n for two-phase is the
+    // start-of-step value held in w.P_n).
+    std::vector<double> tx(n), ty(n), tz(n);
+    auto vel = [&](const double* P, const std::vector<double>& Xi, const std::vector<double>& ro, int fx) {
+      velocities(p, g, P, Xi.data(), ro.data(), tx.data(), ty.data(), tz.data());
+      put(fx, tx);
+      put(fx + 1, ty);
+      put(fx + 2, tz);
+    };
+    vel(Pw0.data(), w.Xi_w, w.ro_w, CAPAZ_FIELD_UX_W);
+    if (p->phases == 2) {
+      vel(w.P_n.data(), w.Xi_n, w.ro_n, CAPAZ_FIELD_UX_N);
+    } else {
+      vel(w.Pn_u.data(), w.Xi_n, w.ro_n, CAPAZ_FIELD_UX_N);
+      vel(w.Pg_u.data(), w.Xi_g, w.ro_g, CAPAZ_FIELD_UX_G);
+    }
+  }
+  if (diag) {
+    // Diagnostics of the final state, summed per k-plane then over planes in
+    // order (deterministic for any thread count).
+    memset(diag, 0, sizeof *diag);
+    const double V = p->hx * p->hy * p->hz;
+    std::vector<double> pm(3 * (size_t)g.nz, 0.), pr(g.nz, 0.), pnf(g.nz, 0.);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < g.nz; k++) {
+      double s0 = 0, s1 = 0, s2 = 0, r = 0, nf = 0;
+      for (int j = 0; j < g.ny; j++)
+        for (int i = 0; i < g.nx; i++) {
+          if (!g.interior(i, j, k)) continue;
+          long l = g.at(i, j, k);
+          double Pw = P_w[l], Sn = S_n[l];
+          double rw = p->ro0_w * (1. + (p->beta_w) * (Pw - p->P_atm));
+          if (p->phases == 2) {
+            double S_e = (1 - Sn - p->S_wr) / (1 - p->S_wr);
+            double Pk = (p->P_d != 0.) ? p->P_d * pow(S_e, (-1.) / p->lambda) : 0.;
+            double rn = p->ro0_n * (1. + (p->beta_n) * (Pw + Pk - p->P_atm));
+            double F1 = rw * (1. - Sn) - w.roS_w[l];
+            double F2 = rn * Sn - w.roS_n[l];
+            s0 += m[l] * rw * (1. - Sn) * V;
+            s1 += m[l] * rn * Sn * V;
+            double rr = fmax(fabs(F1) / p->ro0_w, fabs(F2) / p->ro0_n);
+            if (!(rr <= r)) r = rr;
+            if (!isfinite(Pw) || !isfinite(Sn)) nf += 1;
+          } else {
+            double Sw = S_w[l], Sg = 1. - Sw - Sn;
+            double rn = p->ro0_n * (1. + (p->beta_n) * (Pw - p->P_atm));
+            double rg = p->ro0_g * Pw / p->P_atm;
+            double F1 = rw * Sw - w.roS_w[l];
+            double F2 = rn * Sn - w.roS_n[l];
+            double F3 = rg * Sg - w.roS_g[l];
+            s0 += m[l] * rw * Sw * V;
+            s1 += m[l] * rn * Sn * V;
+            s2 += m[l] * rg * Sg * V;
+            double rr = fmax(fmax(fabs(F1) / p->ro0_w, fabs(F2) / p->ro0_n), fabs(F3) / p->ro0_g);
+            if (!(rr <= r)) r = rr;
+            if (!isfinite(Pw) || !isfinite(Sn) || !isfinite(Sw)) nf += 1;
+          }
+        }
+      pm[3 * k] = s0;
+      pm[3 * k + 1] = s1;
+      pm[3 * k + 2] = s2;
+      pr[k] = r;
+      pnf[k] = nf;
+    }
+    for (int k = 0; k < g.nz; k++) {
+      diag->mass[0] += pm[3 * k];
+      diag->mass[1] += pm[3 * k + 1];
+      diag->mass[2] += pm[3 * k + 2];
+      if (!(pr[k] <= diag->max_residual)) diag->max_residual = pr[k];
+      diag->nonfinite_cells += pnf[k];
+    }
+  }
+  return CAPAZ_OK;
+}
+
+int oracle_max_threads(void) { return omp_get_max_threads(); }
+
+}  // extern "C"

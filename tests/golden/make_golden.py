@@ -1,0 +1,106 @@
+"""Generates tests/golden/*.npz from the reference's own CPU implementation.
+
+    python tests/golden/make_golden.py
+
+Each fixture holds the parameter set, the input state (or none: the
+reference's data_initialization), and the reference's outputs after N steps:
+the state and, where asked, every other per-cell array the reference keeps
+(S_w, P_n, rho, Xi, u, roS, roS_old ...).  The reference binaries come from
+oracle/Makefile (compiled from the reference sources, which must be present
+where the fixtures are generated); the fixtures need nothing at test time.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from capaz_b200.simulation import default_params  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+
+def cfg_fluids(**kw):
+    """Config-0 fluids in the reference model (lambda 2, S_wr 0.1, no P_d)."""
+    base = dict(hx=1.0, hy=1.0, hz=1.0, mu_w=1e-3, mu_n=5e-3, ro0_w=1000.0, ro0_n=850.0, beta_w=1e-9,
+                beta_n=1e-9, lambda_=2.0, S_wr=0.1, P_d=0.0, g_const=9.81, P_atm=1e5, K0=1e-12,
+                porosity=0.3, newton_iterations=10)
+    base.update(kw)
+    return default_params(**base)
+
+
+def random_state2(p, rng, s_mean=0.5):
+    m = np.clip(0.3 + 0.03 * rng.standard_normal((p.nz, p.ny, p.nx)), 0.15, 0.45)
+    st = O.init(p, m)
+    S = np.clip(s_mean + 0.2 * rng.standard_normal(st["S_n"].shape), 0.05, 0.85)
+    return {"P_w": st["P_w"], "S_n": S}, m
+
+
+def save(name, p, nsteps, state, m, with_derived):
+    r = O.ref_run(p, nsteps, state, m if state is not None else None, derived=with_derived)
+    out = {"params": np.array(json.dumps(p.as_dict())), "nsteps": np.array(nsteps)}
+    if state is not None:
+        for k, v in state.items():
+            out["in_" + k] = v
+        out["in_m"] = m
+    for k in ("P_w", "S_w", "S_n", "P_n", "P_g"):
+        if k in r:
+            out["out_" + k] = r[k]
+    if with_derived:
+        for k, v in r["derived"].items():
+            out["der_" + k] = v
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **out)
+    print(f"{path}: {os.path.getsize(path)} bytes, ref {r['info']}")
+
+
+def main():
+    if not (O.ref_available(2) and O.ref_available(3)):
+        raise SystemExit("build the reference binaries first: make -C oracle ref")
+    rng = np.random.default_rng(20261203)
+
+    # The reference's own Two-phase/defines.ini values, its own initial state.
+    save("g2_default_15x15x1", default_params(), 100, None, None, True)
+    # data_initialization on a 3-D grid with a source window (0 steps).
+    save("g2_init_10x9x7", default_params(nx=10, ny=9, nz=7, source=2), 0, None, None, False)
+    # Random states on 3-D grids, with and without capillary pressure.
+    p = cfg_fluids(nx=12, ny=10, nz=7, dt=0.02, source=2, S_n_gr=0.1)
+    st, m = random_state2(p, rng)
+    save("g2_3d_pd0_12x10x7", p, 30, st, m, True)
+    p = cfg_fluids(nx=12, ny=10, nz=7, dt=0.02, source=1, S_n_gr=0.3, P_d=755.0, lambda_=2.7)
+    st, m = random_state2(p, rng)
+    save("g2_3d_pd_12x10x7", p, 30, st, m, True)
+    # Planar grid (NZ = 1), the reference's default geometry, odd sizes.
+    p = cfg_fluids(nx=17, ny=13, nz=1, dt=0.02, source=3, S_n_gr=0.1)
+    st, m = random_state2(p, rng)
+    save("g2_planar_17x13x1", p, 40, st, m, True)
+    # Smallest 3-D grid (every interior cell touches the boundary).
+    p = cfg_fluids(nx=3, ny=3, nz=3, dt=0.02, source=0)
+    st, m = random_state2(p, rng)
+    save("g2_min_3x3x3", p, 10, st, m, True)
+
+    # Three-phase: the reference's Three-phase/defines.ini column case.
+    p3 = default_params(phases=3, nx=1, ny=15, nz=1, newton_iterations=7, lambda_=3.25, S_wr=0.0,
+                        ro0_n=850.0, ro0_g=1.4, mu_n=1e-3, mu_g=1.84e-5, beta_g=9.2e-6, S_w_gr=0.4,
+                        S_n_gr=0.3, S_w_init=0.4, S_n_init=0.3, source=0, porosity=0.4, K0=6.64e-11,
+                        timeX=1000.0)
+    save("g3_column_1x15x1", p3, 200, None, None, True)
+    p3 = default_params(phases=3, nx=9, ny=8, nz=6, newton_iterations=7, lambda_=2.0, S_wr=0.1, S_nr=0.05,
+                        S_gr=0.02, ro0_w=1000.0, ro0_n=850.0, ro0_g=1.2, mu_w=1e-3, mu_n=3e-3, mu_g=1.8e-5,
+                        beta_w=1e-9, beta_n=1e-9, beta_g=9.2e-6, S_w_gr=0.25, S_n_gr=0.7, S_w_init=0.2,
+                        S_n_init=0.3, source=1, porosity=0.3, K0=1e-12, hx=1.0, hy=1.0, hz=1.0, dt=0.01,
+                        g_const=9.81)
+    m = np.clip(0.3 + 0.03 * rng.standard_normal((p3.nz, p3.ny, p3.nx)), 0.15, 0.45)
+    st = O.init(p3, m)
+    st["S_w"] = np.clip(0.3 + 0.1 * rng.standard_normal(st["S_w"].shape), 0.12, 0.6)
+    st["S_n"] = np.clip(0.3 + 0.1 * rng.standard_normal(st["S_n"].shape), 0.07, 0.35)
+    state = {k: st[k] for k in ("P_w", "S_w", "S_n", "P_n", "P_g")}
+    save("g3_3d_9x8x6", p3, 30, state, m, True)
+
+
+if __name__ == "__main__":
+    main()
