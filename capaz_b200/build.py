@@ -79,8 +79,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         dlib = os.path.join(LIB, "libcapaz_dropin_2ph.so")
         dh = [os.path.join(INCLUDE, "capaz_refabi.h"), os.path.join(INCLUDE, "capaz_b200.h")]
         if force or _newer(dlib, [dsrc, lib] + dh):
-            _run([CXX, "-O2", "-fPIC", "-shared", "-std=c++17", "-I" + INCLUDE, dsrc, "-o", dlib,
-                  "-L" + LIB, "-lcapaz_b200", "-Wl,-rpath,$ORIGIN"], verbose)
+            cuda = os.path.dirname(os.path.dirname(NVCC))
+            _run([CXX, "-O2", "-fPIC", "-shared", "-std=c++17", "-I" + INCLUDE, "-I" + os.path.join(cuda, "include"),
+                  dsrc, "-o", dlib, "-L" + LIB, "-lcapaz_b200", "-L" + os.path.join(cuda, "lib64"),
+                  "-lcudart_static", "-ldl", "-lrt", "-lpthread", "-Wl,-rpath,$ORIGIN"], verbose)
         out["libcapaz_dropin_2ph"] = dlib
     return out
 

@@ -118,6 +118,43 @@ Step2Const make_step2_const(const capaz_params& p) {
   return c;
 }
 
+// data_initialization (two-phase.cpp:113-172; the GPU build's copy in
+// two-phase.cu:6-65 is identical) and three-phase.cpp:438-500, on host
+// arrays, m given.  Loop order i, j, k as the reference: the hydrostatic
+// recurrence reads the cell above (j - 1), computed in the previous j pass.
+void reference_init_host(const capaz_params& p, const double* m, double* Pw, double* Sw, double* Sn, double* Pn,
+                         double* Pg) {
+  const long long sy = p.nx, sz = (long long)p.nx * p.ny, n = sz * p.nz;
+  if (p.phases == 2) {
+    std::vector<double> ro_w(n), ro_n(n);
+    for (int i = 0; i < p.nx; i++)
+      for (int j = 0; j < p.ny; j++)
+        for (int k = 0; k < p.nz; k++) {
+          long long l = i + j * sy + (long long)k * sz;
+          bool win = (i >= p.nx / 2 - p.source) && (i <= p.nx / 2 + p.source) && (k >= p.nz / 2 - p.source) &&
+                     (k <= p.nz / 2 + p.source);
+          Sn[l] = ((j == 0) && win) ? p.S_n_gr : p.S_n_background;
+          if (j == 0) {
+            Pw[l] = p.P_atm;
+          } else {
+            long long u = l - sy;
+            double ro_g_dy = (ro_n[u] * Sn[u] + ro_w[u] * (1 - Sn[u])) * (m[u]) * (p.g_const) * (p.hy);
+            Pw[l] = Pw[u] + ro_g_dy;
+          }
+          ro_w[l] = p.ro0_w * (1. + (p.beta_w) * (Pw[l] - p.P_atm));
+          ro_n[l] = p.ro0_n * (1. + (p.beta_n) * (Pw[l] - p.P_atm));
+        }
+    return;
+  }
+  for (long long l = 0; l < n; l++) {
+    Sw[l] = p.S_w_init;
+    Sn[l] = p.S_n_init;
+    Pw[l] = p.P_atm;
+    Pn[l] = p.P_atm;
+    Pg[l] = p.P_atm;
+  }
+}
+
 }  // namespace capaz
 
 // ---------------------------------------------------------------------------
@@ -323,6 +360,25 @@ int capaz_get_field_device(capaz_ctx* ctx, int field, void* dev, void* stream) {
   if (!ctx || !dev) return CAPAZ_ERR_INVALID_ARGUMENT;
   return ctx->get_field(field, dev, true, (cudaStream_t)stream);
 }
+int capaz_get_derived(capaz_ctx* ctx, int field, int state_sel, void* dst, int dst_on_device, void* stream) {
+  if (!ctx || !dst || (state_sel != CAPAZ_STATE_STEP_START && state_sel != CAPAZ_STATE_CURRENT))
+    return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->get_derived(field, state_sel == CAPAZ_STATE_CURRENT, dst, dst_on_device != 0, (cudaStream_t)stream);
+}
+
+int capaz_reference_init(const capaz_params* p, double* m, int m_given, double* P_w, double* S_w, double* S_n,
+                         double* P_n, double* P_g) {
+  if (!p || !m || !P_w || !S_n) return CAPAZ_ERR_INVALID_ARGUMENT;
+  if (p->phases == 3 && (!S_w || !P_n || !P_g)) return CAPAZ_ERR_INVALID_ARGUMENT;
+  int st = capaz_params_validate(p);
+  if (st) return st;
+  const long long n = (long long)p->nx * p->ny * p->nz;
+  if (!m_given)
+    for (long long l = 0; l < n; l++) m[l] = p->porosity;
+  reference_init_host(*p, m, P_w, S_w, S_n, P_n, P_g);
+  return CAPAZ_OK;
+}
+
 int capaz_init_state(capaz_ctx* ctx, void* stream) {
   if (!ctx) return CAPAZ_ERR_INVALID_ARGUMENT;
   return ctx->init_state((cudaStream_t)stream);
@@ -493,42 +549,36 @@ int capaz_ctx::init_state(cudaStream_t s) {
     int st = get_field(CAPAZ_FIELD_M, host_m.data(), false, s);
     if (st) return st;
   }
-  const long long sy = p.nx;
-  std::vector<double> Pw(n), Sn(n);
-  if (p.phases == 2) {
-    std::vector<double> ro_w(n), ro_n(n);
-    // i, j, k order as two-phase.cpp:116-118: the hydrostatic recurrence
-    // reads the cell above (j - 1), computed in the previous j iteration.
-    for (int i = 0; i < p.nx; i++)
-      for (int j = 0; j < p.ny; j++)
-        for (int k = 0; k < p.nz; k++) {
-          long long l = i + j * sy + (long long)k * sy * p.ny;
-          bool win = (i >= p.nx / 2 - p.source) && (i <= p.nx / 2 + p.source) && (k >= p.nz / 2 - p.source) &&
-                     (k <= p.nz / 2 + p.source);
-          Sn[l] = ((j == 0) && win) ? p.S_n_gr : p.S_n_background;
-          if (j == 0) {
-            Pw[l] = p.P_atm;
-          } else {
-            long long u = l - sy;
-            double ro_g_dy = (ro_n[u] * Sn[u] + ro_w[u] * (1 - Sn[u])) * (host_m[u]) * (p.g_const) * (p.hy);
-            Pw[l] = Pw[u] + ro_g_dy;
-          }
-          ro_w[l] = p.ro0_w * (1. + (p.beta_w) * (Pw[l] - p.P_atm));
-          ro_n[l] = p.ro0_n * (1. + (p.beta_n) * (Pw[l] - p.P_atm));
-        }
-    int st = upload_converted(state[cur][0], Pw.data(), s);
-    if (st) return st;
-    return upload_converted(state[cur][1], Sn.data(), s);
+  std::vector<double> Pw(n), Sn(n), Sw, Pn, Pg;
+  if (p.phases == 3) {
+    Sw.resize(n);
+    Pn.resize(n);
+    Pg.resize(n);
   }
-  std::vector<double> Sw(n, p.S_w_init), Pn(n, p.P_atm), Pg(n, p.P_atm);
-  std::fill(Pw.begin(), Pw.end(), p.P_atm);
-  std::fill(Sn.begin(), Sn.end(), p.S_n_init);
+  reference_init_host(p, host_m.data(), Pw.data(), Sw.data(), Sn.data(), Pn.data(), Pg.data());
   double* src[5] = {Pw.data(), Sn.data(), Sw.data(), Pn.data(), Pg.data()};
-  for (int q = 0; q < 5; q++) {
+  const int nstate = p.phases == 2 ? 2 : 5;
+  for (int q = 0; q < nstate; q++) {
     int st = upload_converted(state[cur][q], src[q], s);
     if (st) return st;
   }
   return CAPAZ_OK;
+}
+
+int capaz_ctx::get_derived(int field, bool from_current, void* dst, bool on_device, cudaStream_t s) {
+  CUDA_TRY(this, cudaSetDevice(device));
+  if (field < 0 || field >= CAPAZ_FIELD_COUNT) return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "bad field %d", field);
+  if (field == CAPAZ_FIELD_M || field == CAPAZ_FIELD_K || is_state_field(p, field))
+    return get_field(field, dst, on_device, s);
+  int st = derived(field, s, from_current);
+  if (st) return st;
+  if (on_device) {
+    CUDA_TRY(this, cudaMemcpyAsync(dst, scratch, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    return CAPAZ_OK;
+  }
+  CUDA_TRY(this, cudaMemcpyAsync(dst, scratch, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(this, cudaStreamSynchronize(s));
+  return check_flag();
 }
 
 int capaz_ctx::sync() {

@@ -48,8 +48,12 @@ struct capaz_ctx {
   int upload_converted(void* dst, const double* host, cudaStream_t s);
   int set_field(int field, const void* src, bool on_device, cudaStream_t s);
   int get_field(int field, void* dst, bool on_device, cudaStream_t s);
-  int derived(int field, cudaStream_t s);
+  // Materialises derived `field` into scratch from the start-of-step state
+  // (from_current == false; the current state before any step) or from the
+  // current state.
+  int derived(int field, cudaStream_t s, bool from_current = false);
   int init_state(cudaStream_t s);
+  int get_derived(int field, bool from_current, void* dst, bool on_device, cudaStream_t s);
   int step(int nsteps, cudaStream_t s);
   int read_diag(capaz_diag* out, cudaStream_t s);
   int check_flag();
@@ -60,4 +64,6 @@ struct capaz_ctx {
 
 namespace capaz {
 Step2Const make_step2_const(const capaz_params& p);
+void reference_init_host(const capaz_params& p, const double* m, double* Pw, double* Sw, double* Sn, double* Pn,
+                         double* Pg);
 }

@@ -40,11 +40,11 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
   return fail_msg(CAPAZ_ERR_UNSUPPORTED, "this phase/form combination is not built yet");
 }
 
-int capaz_ctx::derived(int field, cudaStream_t s) {
+int capaz_ctx::derived(int field, cudaStream_t s, bool from_current) {
   int st = ensure_scratch();
   if (st) return st;
   // Start-of-step state of the last step (the current state before any step).
-  const int src = steps_done > 0 ? (cur ^ 1) : cur;
+  const int src = (steps_done > 0 && !from_current) ? (cur ^ 1) : cur;
   if (p.phases == 2 && p.form == CAPAZ_FORM_FP64) {
     const Step2Const c = make_step2_const(p);
     const bool percell = (p.flags & CAPAZ_FLAG_PERCELL_K) != 0;

@@ -97,6 +97,8 @@ PROTOTYPES = {
     "capaz_set_field_device": (C.c_int, [_VP, C.c_int, _VP, _VP]),
     "capaz_get_field_device": (C.c_int, [_VP, C.c_int, _VP, _VP]),
     "capaz_init_state": (C.c_int, [_VP, _VP]),
+    "capaz_reference_init": (C.c_int, [C.POINTER(Params), _VP, C.c_int, _VP, _VP, _VP, _VP, _VP]),
+    "capaz_get_derived": (C.c_int, [_VP, C.c_int, C.c_int, _VP, C.c_int, _VP]),
     "capaz_step": (C.c_int, [_VP, C.c_int, _VP]),
     "capaz_read_diag": (C.c_int, [_VP, C.POINTER(Diag), _VP]),
     "capaz_set_dt": (C.c_int, [_VP, C.c_double]),

@@ -175,6 +175,13 @@ const char* capaz_last_error(const capaz_ctx* ctx);
  * state it receives: m must be > 0 and finite, K > 0 and finite. */
 int capaz_set_field(capaz_ctx* ctx, int field, const double* host, void* stream);
 int capaz_get_field(capaz_ctx* ctx, int field, double* host, void* stream);
+/* Derived fields of an explicitly chosen state: CAPAZ_STATE_STEP_START is
+ * the state at the start of the last step (what capaz_get_field uses after
+ * a step), CAPAZ_STATE_CURRENT the current state (what the reference's
+ * arrays hold between its stage calls, before the Newton stage runs).
+ * `dst` is host memory unless dst_on_device is non-zero. */
+enum capaz_state_sel { CAPAZ_STATE_STEP_START = 0, CAPAZ_STATE_CURRENT = 1 };
+int capaz_get_derived(capaz_ctx* ctx, int field, int state_sel, void* dst, int dst_on_device, void* stream);
 /* Device-resident variants: `dev` is a device pointer of the context's device
  * holding nx*ny*nz values of the storage type of the form (float64 for
  * CAPAZ_FORM_FP64, float32 for the state of CAPAZ_FORM_FP32C). */
@@ -185,6 +192,12 @@ int capaz_get_field_device(capaz_ctx* ctx, int field, void* dev, void* stream);
  * 438-500), computed on the host with the porosity already set in the
  * context (CAPAZ_FIELD_M; M_0 everywhere if never set) and uploaded. */
 int capaz_init_state(capaz_ctx* ctx, void* stream);
+/* The same initial state on host arrays of nx*ny*nz values, no device
+ * involved.  m: in/out — if m_given is 0 it is filled with M_0, else read.
+ * Two-phase writes P_w, S_n (S_w, P_n, P_g may be NULL); three-phase writes
+ * P_w, S_w, S_n, P_n, P_g. */
+int capaz_reference_init(const capaz_params* p, double* m, int m_given, double* P_w, double* S_w,
+                         double* S_n, double* P_n, double* P_g);
 
 /* Advances `nsteps` time steps on `stream`; t is not used by the scheme
  * (the reference's roS_calculation ignores it in the NR form).  With
