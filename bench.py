@@ -11,12 +11,16 @@ one time step of the whole grid.  With N GPUs every rank steps its own
 replica of the grid (weak scaling; the step needs no data-path collective).
 
 One JSON line on rank 0:
-  value   cell-steps/s over exactly K steps, state resident in HBM, CUDA
+  value   cell-steps/s of the precision form (FP32 storage and stencil,
+          FP64 Newton) over exactly K steps, state resident in HBM, CUDA
           events on the launching stream, max over ranks, summed over ranks;
+          the plain FP64 path is timed the same way (`forms`), and both forms
+          are run for the workload's 1000 steps from the same initial state to
+          report the precision form's error against FP64 (`precision`);
   e2e     the same metric through the C ABI with host buffers: pinned-host
-          upload of the state (P_w, S_n, m, K), K steps each followed by a
-          device->host read of that step's diagnostics (mass balance, max
-          residual), then download of (P_w, S_n), all inside the timed region;
+          float64 upload of the state (P_w, S_n, m, K), K steps each followed
+          by a device->host read of that step's diagnostics (mass balance,
+          Newton residual), then download of (P_w, S_n), all timed;
   roofline  algorithmic HBM bytes of the dominant kernel per launch divided
           by its average launch time (CUDA events), against the measured copy
           bandwidth; `traffic` from the committed ncu summary when present;
@@ -63,6 +67,7 @@ def parse():
                     help="workload grid Nx Ny Nz, gravity on z")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-precision", action="store_true")
     return ap.parse_args()
 
 
@@ -244,6 +249,76 @@ def run_reference(args) -> None:
 
 
 # ---------------------------------------------------------------------------
+def time_form(sim, K, W, stream, ws, local, clocks=None):
+    """W untimed steps, then exactly K steps each bracketed by CUDA events on
+    the launching stream; barrier + synchronize on both sides."""
+    import torch
+    sh = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        sim.step(W, stream=sh)
+        stream.synchronize()
+        barrier(ws, local)
+        torch.cuda.synchronize()
+        l0 = sim.launch_count
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        if clocks:
+            clocks.mark(True)
+        for i in range(K):
+            starts[i].record(stream)
+            sim.step(1, stream=sh)
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.mark(False)
+        barrier(ws, local)
+        launches = sim.launch_count - l0
+        total_ms = starts[0].elapsed_time(ends[-1])
+        kern_ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)) / K
+    sim.sync()
+    return {"total_ms": reduce_max(total_ms, ws), "kern_ms": kern_ms, "launches": launches}
+
+
+def make_sim(w, form, dev, diag=False):
+    from capaz_b200 import Simulation, native
+    p = w.params.copy()
+    p.form = form
+    if diag:
+        p.flags |= native.FLAG_DIAGNOSTICS
+    sim = Simulation(p, device=dev)
+    sim.set_field("m", w.m)
+    if w.K is not None:
+        sim.set_field("K", w.K)
+    sim.init_state()
+    sim.sync()
+    return sim
+
+
+def precision_check(w, dev, steps):
+    """Both forms from the same initial state for `steps` steps: per-field
+    max-abs and relative-L2 error of the precision form against FP64."""
+    from capaz_b200 import native
+    out = {}
+    init = None
+    for name, form in (("fp64", native.FORM_FP64), ("fp32c", native.FORM_FP32C)):
+        sim = make_sim(w, form, dev, diag=True)
+        if init is None:
+            init = {"P_w": sim.get_field("P_w"), "S_n": sim.get_field("S_n")}
+        sim.step(steps)
+        out[name] = {"P_w": sim.get_field("P_w"), "S_n": sim.get_field("S_n"), "diag": sim.diag()}
+        sim.close()
+    r = {"steps": steps, "against": "FP64 path (matches the reference CPU step to 1e-12)"}
+    for f in ("S_n", "P_w"):
+        a, b = out["fp32c"][f], out["fp64"][f]
+        r[f] = {"max_abs": float(np.abs(a - b).max()),
+                "rel_l2": float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel())),
+                "max_change_over_run": float(np.abs(b - init[f]).max())}
+    ds = [float(out["fp32c"]["diag"]["mass"][i] / out["fp64"]["diag"]["mass"][i] - 1.0) for i in range(2)]
+    r["mass_rel_diff"] = ds
+    r["newton_residual_fp32c"] = out["fp32c"]["diag"]["max_residual"]
+    return r
+
+
 def run_capaz(args) -> None:
     import torch
 
@@ -253,77 +328,61 @@ def run_capaz(args) -> None:
     ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
     dev = local
-    form_name = args.form or "fp64"
-    form = native.FORM_FP64 if form_name == "fp64" else native.FORM_FP32C
+    forms = [args.form] if args.form else ["fp32c", "fp64"]
+    head = forms[0]
+    form_id = {"fp64": native.FORM_FP64, "fp32c": native.FORM_FP32C}
     K, W = args.steps, args.warmup
-    w = config1(form=form, grid=tuple(args.grid))
+    w = config1(form=native.FORM_FP64, grid=tuple(args.grid))
     p = w.params
     ncell = p.ncell
     percell = w.K is not None
-
     stream = torch.cuda.Stream(device=dev)
     sh = stream.cuda_stream
-    sim = Simulation(p, device=dev)
-    sim.set_field("m", w.m)
-    sim.set_field("K", w.K)
-    sim.init_state()
-    sim.sync()
 
-    # ---- device-resident timing ------------------------------------------
-    with torch.cuda.stream(stream):
-        sim.step(W, stream=sh)
-        stream.synchronize()
-        clocks = Clocks(dev)
-        clocks.start()
-        time.sleep(0.3)
-        barrier(ws, local)
-        torch.cuda.synchronize()
-        l0 = sim.launch_count
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
-        clocks.mark(True)
-        for i in range(K):
-            starts[i].record(stream)
-            sim.step(1, stream=sh)
-            ends[i].record(stream)
-        torch.cuda.synchronize()
-        clocks.mark(False)
-        barrier(ws, local)
-        launches = sim.launch_count - l0
-        total_ms = starts[0].elapsed_time(ends[-1])
-        kern_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / K
-        clk = clocks.stop()
-    sim.sync()
-    total_ms = reduce_max(total_ms, ws)
-    value = ncell * K * ws / (total_ms * 1e-3)
+    # ---- device-resident timing of each form --------------------------------
+    timing = {}
+    clk = None
+    for f in forms:
+        sim = make_sim(w, form_id[f], dev)
+        clocks = None
+        if f == head:
+            clocks = Clocks(dev)
+            clocks.start()
+            time.sleep(0.3)
+        timing[f] = time_form(sim, K, W, stream, ws, local, clocks)
+        if clocks:
+            clk = clocks.stop()
+        sim.close()
+    t = timing[head]
+    value = ncell * K * ws / (t["total_ms"] * 1e-3)
 
-    # ---- end to end through the C ABI with host buffers -------------------
+    # ---- precision of the precision form (1000 steps of the workload) -------
+    prec = None
+    if not args.no_precision and "fp32c" in forms and "fp64" in forms:
+        prec = precision_check(w, dev, w.steps)
+
+    # ---- end to end through the C ABI with host buffers ---------------------
     e2e = None
     if not args.no_e2e:
         q = p.copy()
+        q.form = form_id[head]
         q.flags |= native.FLAG_DIAGNOSTICS
-        sim2 = Simulation(q, device=dev)
-        host = {}
-        for name, arr in (("P_w", None), ("S_n", None), ("m", w.m), ("K", w.K)):
-            t = torch.empty(w.m.shape, dtype=torch.float64, pin_memory=True)
-            host[name] = t
-        ref = Simulation(p, device=dev)  # source of the initial state arrays
-        ref.set_field("m", w.m)
-        ref.set_field("K", w.K)
-        ref.init_state()
-        host["P_w"].numpy()[...] = ref.get_field("P_w")
-        host["S_n"].numpy()[...] = ref.get_field("S_n")
+        init = make_sim(w, native.FORM_FP64, dev)
+        host = {k: torch.empty(w.m.shape, dtype=torch.float64, pin_memory=True) for k in ("P_w", "S_n", "m", "K")}
+        host["P_w"].numpy()[...] = init.get_field("P_w")
+        host["S_n"].numpy()[...] = init.get_field("S_n")
         host["m"].numpy()[...] = w.m
         host["K"].numpy()[...] = w.K
-        ref.close()
+        init.close()
         out_P = torch.empty(w.m.shape, dtype=torch.float64, pin_memory=True)
         out_S = torch.empty(w.m.shape, dtype=torch.float64, pin_memory=True)
+        sim2 = Simulation(q, device=dev)
         sim2.step(0)
         torch.cuda.synchronize()
         barrier(ws, local)
         t0 = time.perf_counter()
         for name in ("m", "K", "P_w", "S_n"):
-            sim2.lib.capaz_set_field(sim2.ctx, native.FIELDS[name], host[name].data_ptr(), sh)
+            native.check(sim2.lib.capaz_set_field(sim2.ctx, native.FIELDS[name], host[name].data_ptr(), sh), sim2.ctx)
         for i in range(K):
             sim2.step(1, stream=sh)
             sim2.diag(stream=sh)
@@ -332,25 +391,26 @@ def run_capaz(args) -> None:
         e2e_s = time.perf_counter() - t0
         barrier(ws, local)
         e2e_s = reduce_max(e2e_s, ws)
-        es = 8
-        h2d = 4 * ncell * es
-        d2h = 2 * ncell * es
+        h2d = 4 * ncell * 8
+        d2h = 2 * ncell * 8 + K * 40
         e2e = {"value": ncell * K * ws / e2e_s, "unit": "cell-steps/s",
-               "h2d_bytes_per_step": (h2d + K * 0) / K, "d2h_bytes_per_step": (d2h + K * 40) / K,
-               "definition": "pinned-host upload of P_w, S_n, m, K; K steps each with a D2H read of the "
-                             "step's diagnostics (40 B); download of P_w, S_n; wall clock"}
+               "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+               "definition": "float64 pinned-host upload of P_w, S_n, m, K; K steps each followed by a "
+                             "device-to-host read of that step's diagnostics (mass balance, Newton residual, "
+                             "40 B); float64 download of P_w, S_n; wall clock around all of it"}
         sim2.close()
 
-    # ---- roofline ----------------------------------------------------------
+    # ---- roofline of the headline kernel -------------------------------------
     peak, peak_kind = measured_peaks()
-    abytes = ALGO_BYTES[(form_name, percell)] * ncell
-    achieved = abytes / (kern_ms * 1e-3) / 1e9
-    kname = "step2_fp64_kernel" if form_name == "fp64" else "step2_fp32c_kernel"
+    abytes = ALGO_BYTES[(head, percell)] * ncell
+    achieved = abytes / (t["kern_ms"] * 1e-3) / 1e9
+    kname = "step2_fp64_kernel" if head == "fp64" else "step2_fp32c_kernel"
     wl_key = f"{args.grid[0]}x{args.grid[1]}x{args.grid[2]}"
-    traffic = load_traffic(kname, wl_key)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "kernel": kname, "algorithmic_bytes_per_launch": abytes,
-            "kernel_ms": kern_ms, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+            "traffic": load_traffic(kname, wl_key), "kernel": kname,
+            "algorithmic_bytes_per_launch": abytes,
+            "algorithmic_bytes_per_cell": ALGO_BYTES[(head, percell)],
+            "kernel_ms": t["kern_ms"], "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -359,24 +419,32 @@ def run_capaz(args) -> None:
         except Exception as e:  # the baseline is informative, never fatal
             cpu = {"value": None, "unit": "cell-steps/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
 
-    sim.close()
     if rank == 0:
+        forms_out = {}
+        for f, tt in timing.items():
+            ab = ALGO_BYTES[(f, percell)] * ncell
+            forms_out[f] = {"value": ncell * K * ws / (tt["total_ms"] * 1e-3), "ms_per_step": tt["total_ms"] / K,
+                            "kernel_ms": tt["kern_ms"], "hbm_frac": ab / (tt["kern_ms"] * 1e-3) / 1e9 / peak,
+                            "launches": tt["launches"]}
         line = {
             "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": K,
-            "warmup": W, "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak",
+            "warmup": W, "ms_per_step": t["total_ms"] / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": value / PUBLISHED_1GPU,
             "vs_baseline_source": "reference's published 1-GPU two-phase step, 250^3 grid, 44.9e6 cell-steps/s "
                                   "(Fermi-era GPU)",
-            "dtype": "f64" if form_name == "fp64" else "f32 storage/stencil + f64 Newton",
+            "dtype": "f64" if head == "fp64" else "f32 storage+stencil (compensated), f64 Newton",
             "data": "synthetic (seeded lognormal K and porosity fields)",
             "config": {"workload": f"two-phase {args.grid[0]}x{args.grid[1]}x{args.grid[2]} gravity on z, "
-                                   f"lognormal K sigma 1 ell 8, {form_name}",
-                       "grid_ref": [p.nx, p.ny, p.nz], "cells": ncell, "form": form_name, "dt": p.dt,
-                       "newton_iterations": p.newton_iterations,
+                                   f"lognormal K sigma 1 ell 8, form {head}",
+                       "grid_ref": [p.nx, p.ny, p.nz], "cells": ncell, "form": head, "dt": p.dt,
                        "parallelism": f"replicas x{ws}",
                        "l2": "inputs larger than L2: each step reads P_w, S_n, m, K and writes P_w, S_n "
-                             f"({ALGO_BYTES[(form_name, percell)] * ncell / 1e6:.0f} MB)"},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+                             f"({ALGO_BYTES[(head, percell)] * ncell / 1e6:.0f} MB of the {126} MB L2)"},
+            "forms": forms_out,
+            "speedup_fp32c_vs_fp64": (forms_out["fp32c"]["value"] / forms_out["fp64"]["value"]
+                                      if "fp32c" in forms_out and "fp64" in forms_out else None),
+            "precision": prec,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": t["launches"],
         }
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -32,6 +32,10 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" 
 # (source, extra flags).  Order is the link order.
 CUDA_SOURCES = [
     ("step2_fp64.cu", ["-fmad=false"]),
+    ("step2_fp32c.cu", []),
+    ("step2_fp32c_tma.cu", []),
+    ("step3_fp64.cu", ["-fmad=false"]),
+    ("fields.cu", []),
     ("capaz_api.cu", []),
     ("capaz_run.cu", []),
 ]

@@ -118,6 +118,114 @@ Step2Const make_step2_const(const capaz_params& p) {
   return c;
 }
 
+Step2FConst make_step2f_const(const capaz_params& p, double S_ref) {
+  const Step2Const d = make_step2_const(p);
+  Step2FConst c;
+  memset(&c, 0, sizeof c);
+  c.nx = d.nx;
+  c.ny = d.ny;
+  c.nz = d.nz;
+  c.source = d.source;
+  c.iters = 2;  // delta-form Newton: the system is bilinear and starts within one step's change
+  c.tiles_x = d.tiles_x;
+  c.tiles_y = d.tiles_y;
+  c.zchunk = d.zchunk;
+  c.nzchunks = d.nzchunks;
+  c.sy = d.sy;
+  c.sz = d.sz;
+  const double ekw = d.e_kw, ekn = d.e_kn;
+  c.intpow = (ekw == floor(ekw) && ekn == floor(ekn) && ekw >= 0 && ekn >= 0 && ekw <= 16 && ekn <= 16) ? 1 : 0;
+  c.n_kw = (int)ekw;
+  c.n_kn = (int)ekn;
+  c.S_ref = S_ref;
+  c.S_ref_f = (float)S_ref;
+  c.one_m_swr_f = (float)(1. - p.S_wr);
+  c.inv_one_m_swr_f = (float)(1. / (1. - p.S_wr));
+  c.e_kw_f = (float)ekw;
+  c.e_kn_f = (float)ekn;
+  c.e_pk_f = (float)d.e_pk;
+  c.P_d_f = (float)p.P_d;
+  c.ro0_w_f = (float)p.ro0_w;
+  c.ro0_n_f = (float)p.ro0_n;
+  c.beta_w_f = (float)p.beta_w;
+  c.beta_n_f = (float)p.beta_n;
+  c.inv_mu_w_f = (float)(1. / p.mu_w);
+  c.inv_mu_n_f = (float)(1. / p.mu_n);
+  c.K0_f = (float)p.K0;
+  c.g_f = (float)p.g_const;
+  c.inv_hx_f = (float)(1. / p.hx);
+  c.inv_hy_f = (float)(1. / p.hy);
+  c.inv_hz_f = (float)(1. / p.hz);
+  c.dt = p.dt;
+  c.P_atm = p.P_atm;
+  c.P_top = p.P_top_offset;
+  c.P_d = p.P_d;
+  c.S_wr = p.S_wr;
+  c.e_pk = d.e_pk;
+  c.ro0_w = p.ro0_w;
+  c.ro0_n = p.ro0_n;
+  c.beta_w = p.beta_w;
+  c.beta_n = p.beta_n;
+  c.g = p.g_const;
+  c.hy = p.hy;
+  c.S_n_gr = p.S_n_gr;
+  c.vol = d.vol;
+  return c;
+}
+
+Step3Const make_step3_const(const capaz_params& p) {
+  Step3Const c;
+  memset(&c, 0, sizeof c);
+  c.nx = p.nx;
+  c.ny = p.ny;
+  c.nz = p.nz;
+  c.source = p.source;
+  c.iters = p.newton_iterations;
+  c.source_window = (p.flags & CAPAZ_FLAG_SOURCE_WINDOW) ? 1 : 0;
+  // Interior x range: [1, nx-2], or the single column of an nx == 1 grid.
+  c.i_lo = p.nx == 1 ? 0 : 1;
+  c.i_hi = p.nx == 1 ? 0 : p.nx - 2;
+  c.sy = p.nx;
+  c.sz = (long long)p.nx * p.ny;
+  c.ncell = c.sz * p.nz;
+  c.tiles_x = (c.i_hi - c.i_lo + 1 + TX - 1) / TX;
+  c.tiles_y = (p.ny - 2 + TY - 1) / TY;
+  if (p.nz == 1) {
+    c.zchunk = 1;
+    c.nzchunks = 1;
+  } else {
+    const int interior = p.nz - 2;
+    const int tiles = c.tiles_x * c.tiles_y;
+    int chunk = 32;
+    while (chunk > 4 && (long long)tiles * ((interior + chunk - 1) / chunk) < 4 * 148) chunk /= 2;
+    c.zchunk = std::min(chunk, interior);
+    c.nzchunks = (interior + c.zchunk - 1) / c.zchunk;
+  }
+  c.hx = p.hx;
+  c.hy = p.hy;
+  c.hz = p.hz;
+  c.dt = p.dt;
+  c.g = p.g_const;
+  c.P_atm = p.P_atm;
+  c.ro0_w = p.ro0_w;
+  c.ro0_n = p.ro0_n;
+  c.ro0_g = p.ro0_g;
+  c.beta_w = p.beta_w;
+  c.beta_n = p.beta_n;
+  c.mu_w = p.mu_w;
+  c.mu_n = p.mu_n;
+  c.mu_g = p.mu_g;
+  c.S_wr = p.S_wr;
+  c.S_nr = p.S_nr;
+  c.S_gr = p.S_gr;
+  c.A = p.lambda;
+  c.K0 = p.K0;
+  c.S_w_gr = p.S_w_gr;
+  c.S_n_gr = p.S_n_gr;
+  c.vol = p.hx * p.hy * p.hz;
+  return c;
+}
+
 // data_initialization (two-phase.cpp:113-172; the GPU build's copy in
 // two-phase.cu:6-65 is identical) and three-phase.cpp:438-500, on host
 // arrays, m given.  Loop order i, j, k as the reference: the hydrostatic
@@ -412,20 +520,37 @@ int capaz_ctx::allocate() {
     for (int s = 0; s < nstate; s++) CUDA_TRY(this, cudaMalloc(&state[b][s], n * es));
   CUDA_TRY(this, cudaMalloc(&m, n * es));
   if (p.flags & CAPAZ_FLAG_PERCELL_K) CUDA_TRY(this, cudaMalloc(&K, n * es));
+  if (p.form == CAPAZ_FORM_FP32C) {
+    CUDA_TRY(this, cudaMalloc(&Pref, sizeof(double) * p.ny));
+    CUDA_TRY(this, cudaMalloc(&PrelF, sizeof(float) * p.ny));
+    CUDA_TRY(this, cudaMalloc(&dPrefF, sizeof(float) * p.ny));
+    std::vector<double> pref0(p.ny, p.P_atm);
+    std::vector<float> z(p.ny, 0.f);
+    CUDA_TRY(this, cudaMemcpy(Pref, pref0.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice));
+    CUDA_TRY(this, cudaMemcpy(PrelF, z.data(), sizeof(float) * p.ny, cudaMemcpyHostToDevice));
+    CUDA_TRY(this, cudaMemcpy(dPrefF, z.data(), sizeof(float) * p.ny, cudaMemcpyHostToDevice));
+  }
+  CUDA_TRY(this, cudaMalloc(&first_bad, sizeof(unsigned long long)));
+  CUDA_TRY(this, cudaMalloc(&sum_parts, sizeof(double) * 1024));
+  CUDA_TRY(this, cudaMalloc(&S_ref_dev, sizeof(double)));
   CUDA_TRY(this, cudaMalloc(&err_flag, sizeof(unsigned int)));
   CUDA_TRY(this, cudaMemset(err_flag, 0, sizeof(unsigned int)));
   CUDA_TRY(this, cudaMalloc(&diag_out, sizeof(double) * DIAG_STRIDE));
   CUDA_TRY(this, cudaMemset(diag_out, 0, sizeof(double) * DIAG_STRIDE));
   // Default porosity M_0 and a zero state until the caller sets one.
-  std::vector<double> mh(n, p.porosity);
-  host_m.assign(mh.begin(), mh.end());
-  int st = upload_converted(m, mh.data(), nullptr);
-  if (st) return st;
   for (int b = 0; b < 2; b++)
     for (int s = 0; s < nstate; s++) CUDA_TRY(this, cudaMemset(state[b][s], 0, n * es));
-  if (p.flags & CAPAZ_FLAG_PERCELL_K) {
-    std::vector<double> kh(n, p.K0);
-    st = upload_converted(K, kh.data(), nullptr);
+  {
+    // Defaults need no validation: the caller's own m and K are checked when
+    // set.  A non-positive M_0 is kept as given until m is set.
+    std::vector<double> mh(n, p.porosity);
+    defaults_unchecked = true;
+    int st = set_field(CAPAZ_FIELD_M, mh.data(), false, nullptr);
+    if (!st && (p.flags & CAPAZ_FLAG_PERCELL_K)) {
+      std::fill(mh.begin(), mh.end(), p.K0);
+      st = set_field(CAPAZ_FIELD_K, mh.data(), false, nullptr);
+    }
+    defaults_unchecked = false;
     if (st) return st;
   }
   CUDA_TRY(this, cudaDeviceSynchronize());
@@ -443,6 +568,18 @@ void capaz_ctx::release() {
   if (diag_out) cudaFree(diag_out);
   if (diag_partials) cudaFree(diag_partials);
   if (scratch) cudaFree(scratch);
+  if (Pref) cudaFree(Pref);
+  if (stage) cudaFree(stage);
+  if (tma_inst) cudaFree(tma_inst);
+  if (tma_items) cudaFree(tma_items);
+  if (tma_counter) cudaFree(tma_counter);
+  if (first_bad) cudaFree(first_bad);
+  if (sum_parts) cudaFree(sum_parts);
+  if (S_ref_dev) cudaFree(S_ref_dev);
+  if (PrelF) cudaFree(PrelF);
+  if (dPrefF) cudaFree(dPrefF);
+  for (int q = 0; q < 4; q++)
+    if (wide[q]) cudaFree(wide[q]);
   if (host_stage) cudaFreeHost(host_stage);
 }
 
@@ -451,22 +588,8 @@ int capaz_ctx::ensure_scratch() {
   return CAPAZ_OK;
 }
 
-int capaz_ctx::upload_converted(void* dst, const double* host, cudaStream_t s) {
-  if (p.form == CAPAZ_FORM_FP64) {
-    CUDA_TRY(this, cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    CUDA_TRY(this, cudaStreamSynchronize(s));
-    return CAPAZ_OK;
-  }
-  std::vector<float> tmp(n);
-  for (long long l = 0; l < n; l++) tmp[l] = (float)host[l];
-  CUDA_TRY(this, cudaMemcpyAsync(dst, tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, s));
-  CUDA_TRY(this, cudaStreamSynchronize(s));
-  return CAPAZ_OK;
-}
-
 int capaz_ctx::set_field(int field, const void* src, bool on_device, cudaStream_t s) {
   CUDA_TRY(this, cudaSetDevice(device));
-  const size_t es = (p.form == CAPAZ_FORM_FP64) ? sizeof(double) : sizeof(float);
   void* dst = nullptr;
   if (field == CAPAZ_FIELD_M) {
     dst = m;
@@ -478,19 +601,46 @@ int capaz_ctx::set_field(int field, const void* src, bool on_device, cudaStream_
   } else {
     return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "field %d cannot be set", field);
   }
+  // Stage the float64 values on the device (from pinned or pageable host
+  // memory, or another device array), check them there, then store them in
+  // the form's layout.
+  const double* d = static_cast<const double*>(src);
   if (!on_device) {
-    const double* h = static_cast<const double*>(src);
-    if (field == CAPAZ_FIELD_M || field == CAPAZ_FIELD_K) {
-      for (long long l = 0; l < n; l++)
-        if (!(h[l] > 0) || !isfinite(h[l]))
-          return fail(this, CAPAZ_ERR_BAD_STATE, "%s must be finite and > 0 (cell %lld: %g)",
-                      field == CAPAZ_FIELD_M ? "m" : "K", l, h[l]);
-      if (field == CAPAZ_FIELD_M) host_m.assign(h, h + n);
-    }
-    return upload_converted(dst, h, s);
+    if (!stage) CUDA_TRY(this, cudaMalloc(&stage, n * sizeof(double)));
+    CUDA_TRY(this, cudaMemcpyAsync(stage, src, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    d = stage;
   }
-  CUDA_TRY(this, cudaMemcpyAsync(dst, src, n * es, cudaMemcpyDeviceToDevice, s));
-  if (field == CAPAZ_FIELD_M) host_m.clear();  // refreshed from the device when needed
+  if ((field == CAPAZ_FIELD_M || field == CAPAZ_FIELD_K) && !defaults_unchecked) {
+    const unsigned long long none = (unsigned long long)n;
+    CUDA_TRY(this, cudaMemcpyAsync(first_bad, &none, sizeof none, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(this, launch_first_invalid(d, n, first_bad, s));
+    launches++;
+    unsigned long long bad = 0;
+    CUDA_TRY(this, cudaMemcpyAsync(&bad, first_bad, sizeof bad, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(this, cudaStreamSynchronize(s));
+    if (bad < (unsigned long long)n) {
+      double v = 0.;
+      CUDA_TRY(this, cudaMemcpy(&v, d + bad, sizeof v, cudaMemcpyDeviceToHost));
+      return fail(this, CAPAZ_ERR_BAD_STATE, "%s must be finite and > 0 (cell %llu: %g)",
+                  field == CAPAZ_FIELD_M ? "m" : "K", bad, v);
+    }
+  }
+  if (p.form == CAPAZ_FORM_FP64) {
+    if (d != dst) CUDA_TRY(this, cudaMemcpyAsync(dst, d, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  } else if (field == CAPAZ_FIELD_P_W) {
+    CUDA_TRY(this, launch_encode_pressure(d, p.nx, p.ny, p.nz, p.P_atm, Pref, PrelF, dPrefF, (float*)dst, s));
+    launches += 3;
+  } else if (field == CAPAZ_FIELD_S_N) {
+    CUDA_TRY(this, launch_encode_saturation(d, n, sum_parts, S_ref_dev, (float*)dst, s));
+    launches += 3;
+    CUDA_TRY(this, cudaMemcpyAsync(&S_ref, S_ref_dev, sizeof(double), cudaMemcpyDeviceToHost, s));
+  } else if (field == CAPAZ_FIELD_M || field == CAPAZ_FIELD_K) {
+    CUDA_TRY(this, launch_narrow(d, n, (float*)dst, s));
+    launches++;
+  } else {
+    return fail(this, CAPAZ_ERR_UNSUPPORTED, "the precision form stores P_w, S_n, m and K");
+  }
+  CUDA_TRY(this, cudaStreamSynchronize(s));
   return CAPAZ_OK;
 }
 
@@ -510,8 +660,26 @@ int capaz_ctx::get_field(int field, void* dst, bool on_device, cudaStream_t s) {
   else if (field == CAPAZ_FIELD_K) {
     if (!K) return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "no per-cell K");
     src = K;
-  } else if (is_state_field(p, field)) {
+  } else if (p.phases == 3 && (field == CAPAZ_FIELD_P_N || field == CAPAZ_FIELD_P_G) && steps_done > 0) {
+    int st = derived(field, s);
+    if (st) return st;
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    CUDA_TRY(this, cudaMemcpyAsync(dst, scratch, n * sizeof(double), kind, s));
+    if (on_device) return CAPAZ_OK;
+    CUDA_TRY(this, cudaStreamSynchronize(s));
+    return check_flag();
+  } else if (is_state_field(p, field) && p.form == CAPAZ_FORM_FP64) {
     src = state[cur][state_slot(field)];
+  } else if (is_state_field(p, field)) {
+    // Precision form: decode the FP32 deviations of the current state.
+    int st = decode_all(cur, s);
+    if (st) return st;
+    src = wide[field == CAPAZ_FIELD_P_W ? 0 : 1];
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    CUDA_TRY(this, cudaMemcpyAsync(dst, src, n * sizeof(double), kind, s));
+    if (on_device) return CAPAZ_OK;
+    CUDA_TRY(this, cudaStreamSynchronize(s));
+    return check_flag();
   } else {
     int st = derived(field, s);
     if (st) return st;
@@ -543,9 +711,8 @@ int capaz_ctx::get_field(int field, void* dst, bool on_device, cudaStream_t s) {
 
 int capaz_ctx::init_state(cudaStream_t s) {
   CUDA_TRY(this, cudaSetDevice(device));
-  if (host_m.empty()) {
-    // m was set from device memory: fetch it once.
-    host_m.resize(n);
+  std::vector<double> host_m(n);
+  {
     int st = get_field(CAPAZ_FIELD_M, host_m.data(), false, s);
     if (st) return st;
   }
@@ -556,10 +723,11 @@ int capaz_ctx::init_state(cudaStream_t s) {
     Pg.resize(n);
   }
   reference_init_host(p, host_m.data(), Pw.data(), Sw.data(), Sn.data(), Pn.data(), Pg.data());
+  const int fields[5] = {CAPAZ_FIELD_P_W, CAPAZ_FIELD_S_N, CAPAZ_FIELD_S_W, CAPAZ_FIELD_P_N, CAPAZ_FIELD_P_G};
   double* src[5] = {Pw.data(), Sn.data(), Sw.data(), Pn.data(), Pg.data()};
   const int nstate = p.phases == 2 ? 2 : 5;
   for (int q = 0; q < nstate; q++) {
-    int st = upload_converted(state[cur][q], src[q], s);
+    int st = set_field(fields[q], src[q], false, s);
     if (st) return st;
   }
   return CAPAZ_OK;
@@ -579,6 +747,20 @@ int capaz_ctx::get_derived(int field, bool from_current, void* dst, bool on_devi
   CUDA_TRY(this, cudaMemcpyAsync(dst, scratch, n * sizeof(double), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(this, cudaStreamSynchronize(s));
   return check_flag();
+}
+
+int capaz_ctx::decode_all(int b, cudaStream_t s) {
+  for (int q = 0; q < 4; q++)
+    if (!wide[q]) CUDA_TRY(this, cudaMalloc(&wide[q], n * sizeof(double)));
+  CUDA_TRY(this, launch_decode2((const float*)state[b][0], (const float*)state[b][1], Pref, S_ref, p.nx, p.ny, n,
+                                wide[0], wide[1], s));
+  CUDA_TRY(this, launch_widen((const float*)m, n, wide[2], s));
+  launches += 2;
+  if (K) {
+    CUDA_TRY(this, launch_widen((const float*)K, n, wide[3], s));
+    launches++;
+  }
+  return CAPAZ_OK;
 }
 
 int capaz_ctx::sync() {

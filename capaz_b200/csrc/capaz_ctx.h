@@ -27,8 +27,27 @@ struct capaz_ctx {
   double* diag_out = nullptr;        // reduced diagnostics (DIAG_STRIDE)
   double* scratch = nullptr;         // one float64 field, derived fields
   void* host_stage = nullptr;
-  std::vector<double> host_m;        // host copy of m for capaz_init_state
+  // Precision form: state stored as FP32 deviations from P_ref(j) and S_ref.
+  double* Pref = nullptr;    // ny
+  float* PrelF = nullptr;    // ny: Pref - P_atm
+  float* dPrefF = nullptr;   // ny: Pref[j+1] - Pref[j]
+  double S_ref = 0.;
+  double* wide[4] = {nullptr, nullptr, nullptr, nullptr};  // FP64 decode scratch
+  // TMA path of the precision form.
+  capaz::InstT* tma_inst = nullptr;  // device descriptor
+  int4* tma_items = nullptr;
+  int tma_nitems = 0;
+  unsigned int* tma_counter = nullptr;
+  double tma_dt = 0., tma_S_ref = 0.;  // values baked into the descriptor
+  int tma_grid = 0;
+  bool tma_ready = false;
+  int tma_prepare();
+  double* stage = nullptr;           // float64 staging of set_field
+  unsigned long long* first_bad = nullptr;  // validation result
+  double* sum_parts = nullptr;       // 1024 partial sums (S_ref)
+  double* S_ref_dev = nullptr;
   long long launches = 0;
+  bool defaults_unchecked = false;   // set while allocate() stores the defaults
   std::string last_error;
 
   static int state_slot(int field) {
@@ -45,7 +64,6 @@ struct capaz_ctx {
   int allocate();
   void release();
   int ensure_scratch();
-  int upload_converted(void* dst, const double* host, cudaStream_t s);
   int set_field(int field, const void* src, bool on_device, cudaStream_t s);
   int get_field(int field, void* dst, bool on_device, cudaStream_t s);
   // Materialises derived `field` into scratch from the start-of-step state
@@ -57,6 +75,8 @@ struct capaz_ctx {
   int step(int nsteps, cudaStream_t s);
   int read_diag(capaz_diag* out, cudaStream_t s);
   int check_flag();
+  // Precision form: FP64 view of (P_w, S_n, m, K) of state buffer b.
+  int decode_all(int b, cudaStream_t s);
   int sync();
   int fail_cuda(cudaError_t e, const char* what);
   int fail_msg(int code, const char* msg);
@@ -64,6 +84,8 @@ struct capaz_ctx {
 
 namespace capaz {
 Step2Const make_step2_const(const capaz_params& p);
+Step2FConst make_step2f_const(const capaz_params& p, double S_ref);
+Step3Const make_step3_const(const capaz_params& p);
 void reference_init_host(const capaz_params& p, const double* m, double* Pw, double* Sw, double* Sn, double* Pn,
                          double* Pg);
 }

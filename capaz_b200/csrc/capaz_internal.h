@@ -1,6 +1,7 @@
 // Internal declarations shared by the kernels and the C-ABI layer.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -35,6 +36,98 @@ struct Step2Const {
   double se_fast_min; // S_e at or above which P_d*pow(S_e, e) == +0 exactly
   double vol;         // hx*hy*hz (diagnostics)
 };
+
+// Constants of the two-phase precision-form step (step2_fp32c.cu).
+struct Step2FConst {
+  int nx, ny, nz;
+  int source, iters;
+  int tiles_x, tiles_y, zchunk, nzchunks;
+  int intpow, n_kw, n_kn;  // relative-permeability exponents are small integers
+  long long sy, sz;
+  float S_ref_f, one_m_swr_f, inv_one_m_swr_f, e_kw_f, e_kn_f, e_pk_f, P_d_f;
+  float ro0_w_f, ro0_n_f, beta_w_f, beta_n_f, inv_mu_w_f, inv_mu_n_f, K0_f, g_f;
+  float inv_hx_f, inv_hy_f, inv_hz_f;
+  double S_ref, dt, P_atm, P_top, P_d, S_wr, e_pk, ro0_w, ro0_n, beta_w, beta_n, g, hy, S_n_gr, vol;
+};
+
+struct Step2FArgs {
+  const float *p_in, *s_in;
+  float *p_out, *s_out;
+  const float *m, *K;  // K == nullptr: uniform K0
+  const double* Pref;  // per-row reference pressure (ny)
+  const float* PrelF;  // Pref - P_atm (ny), FP32
+  const float* dPrefF; // Pref[j+1] - Pref[j] (ny), FP32
+  double* diag;        // per-block partials or nullptr
+  unsigned int* err;
+};
+
+cudaError_t launch_step2_fp32c(const Step2FConst& c, const Step2FArgs& a, cudaStream_t s);
+cudaError_t launch_decode2(const float* p, const float* s, const double* Pref, double S_ref, int nx, int ny,
+                           long long n, double* P, double* S, cudaStream_t st);
+cudaError_t launch_widen(const float* a, long long n, double* out, cudaStream_t st);
+
+// Constants of the three-phase FP64 step (step3_fp64.cu).
+struct Step3Const {
+  int nx, ny, nz, source, iters, source_window;
+  int tiles_x, tiles_y, zchunk, nzchunks, i_lo, i_hi;
+  long long sy, sz, ncell;
+  double hx, hy, hz, dt, g, P_atm;
+  double ro0_w, ro0_n, ro0_g, beta_w, beta_n, mu_w, mu_n, mu_g;
+  double S_wr, S_nr, S_gr, A, K0, S_w_gr, S_n_gr, vol;
+};
+struct Step3Buffers {
+  double *Pw, *Sw, *Sn, *Pn, *Pg;
+};
+cudaError_t launch_step3_fp64(const Step3Const& c, const Step3Buffers& in, const Step3Buffers& out, const double* m,
+                              const double* K, double* diag, unsigned int* err, cudaStream_t s);
+cudaError_t launch_derived3_fp64(const Step3Const& c, int field, const Step3Buffers& st, const double* m,
+                                 const double* K, double* out, cudaStream_t s);
+cudaError_t launch_compose3(const Step3Const& c, const double* Pw_start, const double* bnd_now, double* out,
+                            cudaStream_t s);
+
+// Batched (ensemble) steps: one persistent launch over (instance, tile,
+// z-chunk) work items.  State pointers per ping-pong parity.
+struct Inst64 {
+  Step2Const c;
+  double* Pw[2];
+  double* Sn[2];
+  const double* m;
+  const double* K;
+  unsigned int* err;
+};
+struct InstF {
+  Step2FConst c;
+  Step2FArgs a[2];  // a[parity]: reads buffer parity, writes parity ^ 1
+};
+cudaError_t launch_step2_fp64_batch(const Inst64* insts, const int4* items, int nitems, int parity, bool unik, bool pd0,
+                                    unsigned int* counter, int grid, cudaStream_t s);
+cudaError_t launch_step2_fp32c_batch(const InstF* insts, const int4* items, int nitems, int parity, bool unik,
+                                     bool pd0, bool intpow, unsigned int* counter, int grid, cudaStream_t s);
+int step2_fp64_batch_grid(int device);
+int step2_fp32c_batch_grid(int device);
+
+// TMA-staged precision-form step (step2_fp32c_tma.cu): one descriptor per
+// instance in global memory, tensor maps of the state ping-pong buffers.
+struct alignas(128) InstT {
+  CUtensorMap map_p[2], map_s[2], map_K, map_m;
+  Step2FConst c;
+  Step2FArgs a[2];  // a[parity]: reads buffer parity, writes parity ^ 1
+};
+struct TmaFlags {
+  bool unik, pd0, lam2;
+};
+cudaError_t launch_step2_fp32c_tma(const InstT* insts, const int4* items, int nitems, int parity, const TmaFlags& f,
+                                   unsigned int* counter, double* diag_partials, int grid, cudaStream_t s);
+int step2_fp32c_tma_grid(int device, const TmaFlags& f);
+int encode_field_map(CUtensorMap* map, const float* base, int nx, int ny, int nz);
+
+// Field preparation (fields.cu).
+cudaError_t launch_first_invalid(const double* a, long long n, unsigned long long* first, cudaStream_t s);
+cudaError_t launch_encode_pressure(const double* P, int nx, int ny, int nz, double P_atm, double* Pref, float* PrelF,
+                                   float* dPrefF, float* out, cudaStream_t s);
+cudaError_t launch_encode_saturation(const double* S, long long n, double* part, double* S_ref, float* out,
+                                     cudaStream_t s);
+cudaError_t launch_narrow(const double* a, long long n, float* out, cudaStream_t s);
 
 // Per-block partial diagnostics: mass[3], max residual, non-finite count.
 constexpr int DIAG_STRIDE = 5;

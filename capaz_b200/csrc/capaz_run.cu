@@ -1,4 +1,9 @@
 // Step dispatch and derived-field materialisation for a context.
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
 #include "capaz_ctx.h"
 #include "capaz_internal.h"
 
@@ -37,6 +42,93 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
     }
     return CAPAZ_OK;
   }
+  if (p.phases == 2 && p.form == CAPAZ_FORM_FP32C && p.nx % 4 == 0 && !(p.flags & CAPAZ_FLAG_NO_TMA)) {
+    int st = tma_prepare();
+    if (st) return st;
+    const TmaFlags f{!(p.flags & CAPAZ_FLAG_PERCELL_K), p.P_d == 0., p.lambda == 2.0};
+    if (diag && !diag_partials) {
+      diag_blocks = tma_grid;
+      e = cudaMalloc(&diag_partials, sizeof(double) * DIAG_STRIDE * diag_blocks);
+      if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(diag)");
+    }
+    for (int t = 0; t < nsteps; t++) {
+      const bool last = t == nsteps - 1;
+      e = launch_step2_fp32c_tma(tma_inst, tma_items, tma_nitems, cur, f, tma_counter,
+                                 (diag && last) ? diag_partials : nullptr, tma_grid, s);
+      launches++;
+      if (e != cudaSuccess) return fail_cuda(e, "step2_fp32c_tma launch");
+      cur ^= 1;
+      steps_done++;
+    }
+    if (diag) {
+      e = launch_diag_finalize(diag_partials, tma_grid, diag_out, s);
+      launches++;
+      if (e != cudaSuccess) return fail_cuda(e, "diag finalize launch");
+    }
+    return CAPAZ_OK;
+  }
+  if (p.phases == 2 && p.form == CAPAZ_FORM_FP32C) {
+    const Step2FConst c = make_step2f_const(p, S_ref);
+    if (diag && !diag_partials) {
+      diag_blocks = c.tiles_x * c.tiles_y * c.nzchunks;
+      e = cudaMalloc(&diag_partials, sizeof(double) * DIAG_STRIDE * diag_blocks);
+      if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(diag)");
+    }
+    for (int t = 0; t < nsteps; t++) {
+      const int nxt = cur ^ 1;
+      Step2FArgs a;
+      a.p_in = (const float*)state[cur][0];
+      a.s_in = (const float*)state[cur][1];
+      a.p_out = (float*)state[nxt][0];
+      a.s_out = (float*)state[nxt][1];
+      a.m = (const float*)m;
+      a.K = (p.flags & CAPAZ_FLAG_PERCELL_K) ? (const float*)K : nullptr;
+      a.Pref = Pref;
+      a.PrelF = PrelF;
+      a.dPrefF = dPrefF;
+      a.diag = (diag && t == nsteps - 1) ? diag_partials : nullptr;
+      a.err = err_flag;
+      e = launch_step2_fp32c(c, a, s);
+      launches++;
+      if (e != cudaSuccess) return fail_cuda(e, "step2_fp32c launch");
+      cur = nxt;
+      steps_done++;
+    }
+    if (diag) {
+      e = launch_diag_finalize(diag_partials, diag_blocks, diag_out, s);
+      launches++;
+      if (e != cudaSuccess) return fail_cuda(e, "diag finalize launch");
+    }
+    return CAPAZ_OK;
+  }
+  if (p.phases == 3 && p.form == CAPAZ_FORM_FP64) {
+    const Step3Const c = make_step3_const(p);
+    if (diag && !diag_partials) {
+      diag_blocks = c.tiles_x * c.tiles_y * c.nzchunks;
+      e = cudaMalloc(&diag_partials, sizeof(double) * DIAG_STRIDE * diag_blocks);
+      if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(diag)");
+    }
+    const double* Kp = (p.flags & CAPAZ_FLAG_PERCELL_K) ? (const double*)K : nullptr;
+    for (int t = 0; t < nsteps; t++) {
+      const int nxt = cur ^ 1;
+      Step3Buffers in{(double*)state[cur][0], (double*)state[cur][2], (double*)state[cur][1], (double*)state[cur][3],
+                      (double*)state[cur][4]};
+      Step3Buffers out{(double*)state[nxt][0], (double*)state[nxt][2], (double*)state[nxt][1],
+                       (double*)state[nxt][3], (double*)state[nxt][4]};
+      e = launch_step3_fp64(c, in, out, (const double*)m, Kp, (diag && t == nsteps - 1) ? diag_partials : nullptr,
+                            err_flag, s);
+      launches++;
+      if (e != cudaSuccess) return fail_cuda(e, "step3_fp64 launch");
+      cur = nxt;
+      steps_done++;
+    }
+    if (diag) {
+      e = launch_diag_finalize(diag_partials, diag_blocks, diag_out, s);
+      launches++;
+      if (e != cudaSuccess) return fail_cuda(e, "diag finalize launch");
+    }
+    return CAPAZ_OK;
+  }
   return fail_msg(CAPAZ_ERR_UNSUPPORTED, "this phase/form combination is not built yet");
 }
 
@@ -61,5 +153,111 @@ int capaz_ctx::derived(int field, cudaStream_t s, bool from_current) {
     if (e != cudaSuccess) return fail_cuda(e, "derived launch");
     return CAPAZ_OK;
   }
+  if (p.phases == 2 && p.form == CAPAZ_FORM_FP32C) {
+    // Decode the chosen state to FP64 and evaluate the FP64 derived kernel.
+    st = decode_all(src, s);
+    if (st) return st;
+    const Step2Const c = make_step2_const(p);
+    const bool percell = (p.flags & CAPAZ_FLAG_PERCELL_K) != 0;
+    cudaError_t e = launch_derived2_fp64(c, field, wide[0], wide[1], wide[2], wide[3], percell, scratch, s);
+    launches++;
+    if (e != cudaSuccess) return fail_cuda(e, "derived launch");
+    return CAPAZ_OK;
+  }
+  if (p.phases == 3 && p.form == CAPAZ_FORM_FP64) {
+    const Step3Const c = make_step3_const(p);
+    const double* Kp = (p.flags & CAPAZ_FLAG_PERCELL_K) ? (const double*)K : nullptr;
+    Step3Buffers stb{(double*)state[src][0], (double*)state[src][2], (double*)state[src][1], (double*)state[src][3],
+                     (double*)state[src][4]};
+    if (field == CAPAZ_FIELD_P_N || field == CAPAZ_FIELD_P_G) {
+      // The reference's P_n, P_g arrays after a step: start-of-step P_w on
+      // interior cells, this step's Border_P values on boundary cells.
+      const int slot = field == CAPAZ_FIELD_P_N ? 3 : 4;
+      cudaError_t e = launch_compose3(c, (const double*)state[src][0], (const double*)state[cur][slot], scratch, s);
+      launches++;
+      if (e != cudaSuccess) return fail_cuda(e, "compose launch");
+      return CAPAZ_OK;
+    }
+    if (field == CAPAZ_FIELD_S_W || field == CAPAZ_FIELD_P_W || field == CAPAZ_FIELD_S_N)
+      return fail_msg(CAPAZ_ERR_INVALID_ARGUMENT, "state field");
+    cudaError_t e = launch_derived3_fp64(c, field, stb, (const double*)m, Kp, scratch, s);
+    launches++;
+    if (e != cudaSuccess) return fail_cuda(e, "derived launch");
+    return CAPAZ_OK;
+  }
   return fail_msg(CAPAZ_ERR_UNSUPPORTED, "derived fields for this phase/form are not built yet");
+}
+
+// Builds (or refreshes) the device descriptor of the TMA-staged precision
+// step: tensor maps of both state buffers and of K and m, the step constants
+// (which depend on dt and S_ref) and the work-item list.
+int capaz_ctx::tma_prepare() {
+  if (tma_ready && tma_dt == p.dt && tma_S_ref == S_ref) return CAPAZ_OK;
+  InstT h;
+  memset(&h, 0, sizeof h);
+  h.c = make_step2f_const(p, S_ref);
+  // Shorter z-chunks than the plain kernel: the dynamic schedule balances
+  // the work, and 16-plane chunks give enough items for every SM.
+  if (p.nz > 1) {
+    const int interior = p.nz - 2;
+    h.c.zchunk = std::min(16, interior);
+    h.c.nzchunks = (interior + h.c.zchunk - 1) / h.c.zchunk;
+  }
+  for (int b = 0; b < 2; b++) {
+    if (encode_field_map(&h.map_p[b], (const float*)state[b][0], p.nx, p.ny, p.nz) ||
+        encode_field_map(&h.map_s[b], (const float*)state[b][1], p.nx, p.ny, p.nz))
+      return fail_msg(CAPAZ_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  }
+  if (encode_field_map(&h.map_m, (const float*)m, p.nx, p.ny, p.nz))
+    return fail_msg(CAPAZ_ERR_CUDA, "cuTensorMapEncodeTiled failed (m)");
+  if (K && encode_field_map(&h.map_K, (const float*)K, p.nx, p.ny, p.nz))
+    return fail_msg(CAPAZ_ERR_CUDA, "cuTensorMapEncodeTiled failed (K)");
+  if (!K) h.map_K = h.map_m;  // unused (uniform K)
+  for (int b = 0; b < 2; b++) {
+    Step2FArgs& a = h.a[b];
+    a.p_in = (const float*)state[b][0];
+    a.s_in = (const float*)state[b][1];
+    a.p_out = (float*)state[b ^ 1][0];
+    a.s_out = (float*)state[b ^ 1][1];
+    a.m = (const float*)m;
+    a.K = (const float*)K;
+    a.Pref = Pref;
+    a.PrelF = PrelF;
+    a.dPrefF = dPrefF;
+    a.diag = nullptr;
+    a.err = err_flag;
+  }
+  cudaError_t e;
+  if (tma_ready) {
+    // A step launched earlier may still read the old descriptor.
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return fail_cuda(e, "cudaDeviceSynchronize");
+  }
+  if (!tma_inst) {
+    e = cudaMalloc(&tma_inst, sizeof(InstT));
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(tma)");
+    e = cudaMalloc(&tma_counter, sizeof(unsigned int));
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(tma)");
+  }
+  e = cudaMemcpy(tma_inst, &h, sizeof h, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy(tma descriptor)");
+  if (!tma_items) {
+    // Items ordered z-chunk-major: CTAs that run together work on the same
+    // z range, so the halos of neighbouring tiles meet in L2.
+    const int ntiles = h.c.tiles_x * h.c.tiles_y;
+    std::vector<int4> items;
+    for (int zc = 0; zc < h.c.nzchunks; zc++)
+      for (int t = 0; t < ntiles; t++) items.push_back(make_int4(0, t, zc, 0));
+    tma_nitems = (int)items.size();
+    e = cudaMalloc(&tma_items, sizeof(int4) * items.size());
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(items)");
+    e = cudaMemcpy(tma_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy(items)");
+    const TmaFlags f{!(p.flags & CAPAZ_FLAG_PERCELL_K), p.P_d == 0., p.lambda == 2.0};
+    tma_grid = std::min(tma_nitems, step2_fp32c_tma_grid(device, f));
+  }
+  tma_dt = p.dt;
+  tma_S_ref = S_ref;
+  tma_ready = true;
+  return CAPAZ_OK;
 }

@@ -25,6 +25,8 @@ struct DropIn {
   long long n = 0;
   int device = 0;
   Stage stage = IDLE;
+  long long steps = 0;     // fused steps run
+  bool stepping = false;   // a step's stages have started since device set-up
   // Device arrays handed to the host program, by reference field.
   struct Handle {
     double* dev;
@@ -214,7 +216,11 @@ void load_data_to_host(double* HostArrayPtr, double* DevArrayPtr, consts def) {
   (void)def;
   const size_t bytes = (size_t)g.n * sizeof(double);
   const int f = field_of(DevArrayPtr);
-  if (f >= 0) {
+  const bool state_or_media = (f == CAPAZ_FIELD_P_W || f == CAPAZ_FIELD_S_N || f == CAPAZ_FIELD_M);
+  // Before the first stage call the reference's derived arrays hold what
+  // the allocation left there (the handles are zeroed) or what the host
+  // uploaded; they are computed only once a step has begun.
+  if (f >= 0 && (state_or_media || g.stepping)) {
     // Before the Newton stage of a step has run, the reference's derived
     // arrays describe the current state; otherwise the start of the last step.
     const int sel = (g.stage == IDLE || g.stage == AFTER_P_S) ? CAPAZ_STATE_STEP_START : CAPAZ_STATE_CURRENT;
@@ -240,7 +246,10 @@ void data_initialization(ptr_Arrays H, long int* time_counter, consts def) {
 }
 
 // ---- stages ----------------------------------------------------------------
-void S_calculation(ptr_Arrays, ptr_Arrays, consts) { advance(IDLE, AFTER_S, "S_calculation", __LINE__); }
+void S_calculation(ptr_Arrays, ptr_Arrays, consts) {
+  advance(IDLE, AFTER_S, "S_calculation", __LINE__);
+  g.stepping = true;
+}
 
 void ro_P_Xi_calculation(ptr_Arrays, ptr_Arrays, consts) {
   advance(AFTER_S, AFTER_RO_P_XI, "ro_P_Xi_calculation", __LINE__);
@@ -256,6 +265,7 @@ void roS_calculation(ptr_Arrays, ptr_Arrays, double t, consts) {
 void P_S_calculation(ptr_Arrays, ptr_Arrays, consts) {
   advance(AFTER_ROS, AFTER_P_S, "P_S_calculation", __LINE__);
   check(capaz_step(g.ctx, 1, nullptr), "capaz_step", __LINE__);
+  g.steps++;
 }
 
 void boundary_conditions(ptr_Arrays, ptr_Arrays, consts) {

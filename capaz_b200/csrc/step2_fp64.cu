@@ -159,17 +159,15 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
+// One work item: the TX x TY column tile `tile` over z-chunk `zc`.  Called
+// by every thread of the CTA (it contains barriers).
 template <bool UNIK, bool PD0, bool PLANAR, bool DIAG>
-__global__ void __launch_bounds__(NTHREADS, 2)
-    step2_fp64_kernel(const Step2Const c, const double* __restrict__ Pw_in, const double* __restrict__ Sn_in,
-                      double* __restrict__ Pw_out, double* __restrict__ Sn_out, const double* __restrict__ m,
-                      const double* __restrict__ K, double* __restrict__ diag_partials,
-                      unsigned int* __restrict__ err_flag) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Plane2* ring = reinterpret_cast<Plane2*>(smem_raw);
-
+__device__ __forceinline__ void fp64_tile(const Step2Const& c, const double* __restrict__ Pw_in,
+                                          const double* __restrict__ Sn_in, double* __restrict__ Pw_out,
+                                          double* __restrict__ Sn_out, const double* __restrict__ m,
+                                          const double* __restrict__ K, unsigned int* __restrict__ err_flag,
+                                          int tile, int zc, Plane2* ring, double* diag_slot) {
   const int tid = threadIdx.x + TX * threadIdx.y;
-  const int tile = blockIdx.x;
   const int ti = tile % c.tiles_x, tj = tile / c.tiles_x;
   const int i0 = 1 + ti * TX, j0 = 1 + tj * TY;  // first interior cell of the tile
   const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
@@ -181,7 +179,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     kb = 0;
     ke = 1;
   } else {
-    kb = 1 + blockIdx.y * c.zchunk;
+    kb = 1 + zc * c.zchunk;
     ke = min(kb + c.zchunk, c.nz - 1);
   }
 
@@ -301,13 +299,56 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         t2 = fmax(t2, red[w][2]);
         t3 += red[w][3];
       }
-      double* out = diag_partials + (size_t)DIAG_STRIDE * (blockIdx.x + (size_t)gridDim.x * blockIdx.y);
-      out[0] = t0;
-      out[1] = t1;
-      out[2] = 0.;
-      out[3] = t2;
-      out[4] = t3;
+      diag_slot[0] = t0;
+      diag_slot[1] = t1;
+      diag_slot[2] = 0.;
+      diag_slot[3] = t2;
+      diag_slot[4] = t3;
     }
+    __syncthreads();
+  }
+}
+
+template <bool UNIK, bool PD0, bool PLANAR, bool DIAG>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    step2_fp64_kernel(const Step2Const c, const double* __restrict__ Pw_in, const double* __restrict__ Sn_in,
+                      double* __restrict__ Pw_out, double* __restrict__ Sn_out, const double* __restrict__ m,
+                      const double* __restrict__ K, double* __restrict__ diag_partials,
+                      unsigned int* __restrict__ err_flag) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Plane2* ring = reinterpret_cast<Plane2*>(smem_raw);
+  double* slot = DIAG ? diag_partials + (size_t)DIAG_STRIDE * (blockIdx.x + (size_t)gridDim.x * blockIdx.y) : nullptr;
+  fp64_tile<UNIK, PD0, PLANAR, DIAG>(c, Pw_in, Sn_in, Pw_out, Sn_out, m, K, err_flag, blockIdx.x, blockIdx.y, ring,
+                                     slot);
+}
+
+// Batched persistent kernel: CTAs take (instance, tile, z-chunk) work items
+// from a shared counter until the list is exhausted, so instances of uneven
+// size share one launch.  All instances have the same flags (K per cell,
+// P_d == 0); planar and 3-D instances may be mixed.
+template <bool UNIK, bool PD0>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    step2_fp64_batch_kernel(const Inst64* __restrict__ insts, const int4* __restrict__ items, int nitems, int parity,
+                            unsigned int* __restrict__ counter) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Plane2* ring = reinterpret_cast<Plane2*>(smem_raw);
+  __shared__ int w_sh;
+  for (;;) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) w_sh = (int)atomicAdd(counter, 1u);
+    __syncthreads();
+    const int w = w_sh;
+    __syncthreads();
+    if (w >= nitems) break;
+    const int4 it = items[w];
+    const Inst64& I = insts[it.x];
+    const Step2Const& c = I.c;
+    const int src = parity, dst = parity ^ 1;
+    if (c.nz == 1)
+      fp64_tile<UNIK, PD0, true, false>(c, I.Pw[src], I.Sn[src], I.Pw[dst], I.Sn[dst], I.m, I.K, I.err, it.y, it.z,
+                                        ring, nullptr);
+    else
+      fp64_tile<UNIK, PD0, false, false>(c, I.Pw[src], I.Sn[src], I.Pw[dst], I.Sn[dst], I.m, I.K, I.err, it.y, it.z,
+                                         ring, nullptr);
   }
 }
 
@@ -511,6 +552,36 @@ cudaError_t launch_step2_fp64(const Step2Const& c, const double* Pw_in, const do
             : launch_p<false, false>(planar, diag_on, c, Pw_in, Sn_in, Pw_out, Sn_out, m, K, diag_partials, err_flag, s);
   if (nlaunch) *nlaunch += 1;
   return e;
+}
+
+cudaError_t launch_step2_fp64_batch(const Inst64* insts, const int4* items, int nitems, int parity, bool unik, bool pd0,
+                                    unsigned int* counter, int grid, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), s);
+  if (e != cudaSuccess) return e;
+#define CAPAZ_BATCH64(U, P)                                                                               \
+  do {                                                                                                    \
+    auto kern = step2_fp64_batch_kernel<U, P>;                                                            \
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem2);            \
+    if (e != cudaSuccess) return e;                                                                       \
+    kern<<<grid, dim3(TX, TY), kSmem2, s>>>(insts, items, nitems, parity, counter);                       \
+  } while (0)
+  if (unik) {
+    if (pd0) CAPAZ_BATCH64(true, true);
+    else CAPAZ_BATCH64(true, false);
+  } else {
+    if (pd0) CAPAZ_BATCH64(false, true);
+    else CAPAZ_BATCH64(false, false);
+  }
+#undef CAPAZ_BATCH64
+  return cudaGetLastError();
+}
+
+int step2_fp64_batch_grid(int device) {
+  int sms = 148, per = 2;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp64_batch_kernel<false, true>, NTHREADS, kSmem2);
+  if (per < 1) per = 1;
+  return sms * per;
 }
 
 cudaError_t launch_diag_finalize(const double* partials, int nblocks, double* out, cudaStream_t s) {

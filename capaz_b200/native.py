@@ -30,6 +30,8 @@ FORM_FP32C = 1
 
 FLAG_PERCELL_K = 0x1
 FLAG_DIAGNOSTICS = 0x2
+FLAG_SOURCE_WINDOW = 0x4
+FLAG_NO_TMA = 0x8
 
 FIELDS = {
     "P_w": 0, "S_n": 1, "S_w": 2, "m": 3, "K": 4, "P_n": 5, "P_g": 6, "S_g": 7,

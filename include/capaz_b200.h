@@ -64,6 +64,13 @@ enum capaz_form {
 /* Flags (capaz_params.flags). */
 #define CAPAZ_FLAG_PERCELL_K 0x1u /* Xi uses K[cell] instead of K0 (extension) */
 #define CAPAZ_FLAG_DIAGNOSTICS 0x2u /* reduce mass balance + max residual each step */
+/* Three-phase: the top-face source covers only the SOURCE window around the
+ * face centre (the two-phase rule, two-phase.cpp:71-77) instead of the whole
+ * face (three-phase.cpp:358-362).  Extension. */
+#define CAPAZ_FLAG_SOURCE_WINDOW 0x4u
+/* Precision form: use the plain-load kernel even where the TMA-staged one
+ * applies (nx a multiple of 4).  For comparisons and tests. */
+#define CAPAZ_FLAG_NO_TMA 0x8u
 
 /*
  * Physical and numerical parameters: the subset of the reference's `consts`

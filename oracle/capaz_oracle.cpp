@@ -27,7 +27,9 @@
 //     Buckley-Leverett module does (b-l.cpp:65-66);
 //   - top-face pressure P_atm + P_top_offset in Border_P;
 //   - two-phase background initial S_n (S_n_background) off the source window;
-//   - per-cell porosity m at initialisation.
+//   - per-cell porosity m at initialisation;
+//   - three-phase top source limited to the SOURCE window
+//     (CAPAZ_FLAG_SOURCE_WINDOW), as the two-phase rule is.
 #include <math.h>
 #include <omp.h>
 #include <stdlib.h>
@@ -447,11 +449,14 @@ void step3(const capaz_params* p, const Grid& g, double* P_w, double* S_w, doubl
         if (!bnd) continue;
         long l1 = g.basic(i, j, k);
         long l = g.at(i, j, k);
-        if ((j != 0) || (p->source <= 0)) {
+        // With CAPAZ_FLAG_SOURCE_WINDOW (extension) only the SOURCE window of
+        // the top face is a source; without it, the whole face, as written.
+        const bool src = (j == 0) && (p->source > 0) &&
+                         (!(p->flags & CAPAZ_FLAG_SOURCE_WINDOW) || in_window(p, i, k));
+        if (!src) {
           S_w[l] = S_w[l1];
           S_n[l] = S_n[l1];
-        }
-        if ((j == 0) && (p->source > 0)) {
+        } else {
           S_w[l] = p->S_w_gr;
           S_n[l] = p->S_n_gr;
         }

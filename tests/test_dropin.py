@@ -116,7 +116,7 @@ def test_dropin_rejects_out_of_order_stages(tmp_path):
         '#include "capaz_refabi.h"\n#include <string.h>\n'
         "int main(){ consts d; memset(&d,0,sizeof d); d.locNx=d.Nx=5; d.locNy=d.Ny=5; d.locNz=d.Nz=1;"
         "d.size=d.sizex=d.sizey=d.sizez=1; d.hx=d.hy=d.hz=1; d.dt=1e-3; d.mu_w=d.mu_n=1e-3; d.P_atm=1e5;"
-        "d.lambda[0]=2; d.K[0]=1e-12; d.newton_iterations=1; device_initialization(&d);"
+        "d.lambda[0]=2; d.K[0]=1e-12; d.porosity[0]=0.3; d.newton_iterations=1; device_initialization(&d);"
         "ptr_Arrays H, D; P_S_calculation(H, D, d); return 0; }\n")
     exe = tmp_path / "bad"
     subprocess.run(["g++", "-I" + os.path.join(ROOT, "include"), str(src), "-o", str(exe), DROPIN,

@@ -28,12 +28,14 @@ def run_gpu(p, state, m, nsteps, K=None, derived=(), diag=False):
             s.set_field("K", K)
         for k, v in state.items():
             s.set_field(k, v)
+        l0 = s.launch_count
         s.step(nsteps)
+        launched = s.launch_count - l0
         out = {k: s.get_field(k) for k in ("P_w", "S_n")}
         out["derived"] = {f: s.get_field(f) for f in derived}
         if diag:
             out["diag"] = s.diag()
-        out["launches"] = s.launch_count
+        out["launches"] = launched
     return out
 
 
