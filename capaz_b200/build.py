@@ -38,6 +38,7 @@ CUDA_SOURCES = [
     ("fields.cu", []),
     ("capaz_api.cu", []),
     ("capaz_run.cu", []),
+    ("batch.cu", []),
 ]
 HEADERS = ["capaz_internal.h", "capaz_ctx.h"]
 

@@ -137,3 +137,24 @@ def config1(form: int = native.FORM_FP64, seed: int = 1, grid=(256, 256, 128), s
     return Workload(f"cfg1 two-phase {Nx}x{Ny}x{Nz} " + ("fp64" if form == native.FORM_FP64 else "fp32c"),
                     p, steps, m, K, {"workload_grid": list(grid), "ref_grid": [nx, ny, nz], "dt": p.dt,
                                      "sigma": 1.0, "ell": 8.0, "seed": seed})
+
+
+def config3(form: int = native.FORM_FP32C, seed: int = 3, count: int = 64, dims=(32, 48, 64, 96, 128),
+            steps: int = 300) -> list:
+    """Ensemble: `count` two-phase instances, grid sizes drawn uniformly per
+    axis from `dims`, each with its own seeded lognormal K (sigma in
+    [0.5, 1.5], correlation length in [4, 16] cells), config-0 fluids and its
+    own stable dt; 300 steps each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(count):
+        Nx, Ny, Nz = (int(v) for v in rng.choice(dims, 3))
+        sigma = float(rng.uniform(0.5, 1.5))
+        ell = float(rng.uniform(4.0, 16.0))
+        nx, ny, nz = Nx, Nz, Ny
+        p = two_phase_params(nx, ny, nz, form=form, percell_k=True)
+        m, K = heterogeneous_fields((nz, ny, nx), sigma, ell, seed * 1000 + q)
+        p.dt = stable_dt(p, m, K)
+        out.append(Workload(f"cfg3[{q}] {Nx}x{Ny}x{Nz}", p, steps, m, K,
+                            {"workload_grid": [Nx, Ny, Nz], "sigma": sigma, "ell": ell, "dt": p.dt}))
+    return out

@@ -105,6 +105,12 @@ PROTOTYPES = {
     "capaz_read_diag": (C.c_int, [_VP, C.POINTER(Diag), _VP]),
     "capaz_set_dt": (C.c_int, [_VP, C.c_double]),
     "capaz_launch_count": (C.c_int64, [_VP]),
+    "capaz_batch_create": (_VP, [C.POINTER(Params), C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "capaz_batch_destroy": (C.c_int, [_VP]),
+    "capaz_batch_instance": (_VP, [_VP, C.c_int]),
+    "capaz_batch_step": (C.c_int, [_VP, C.c_int, _VP]),
+    "capaz_batch_autotune": (C.c_int, [_VP, _VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "capaz_batch_launch_count": (C.c_int64, [_VP]),
     "capaz_sync": (C.c_int, [_VP]),
 }
 

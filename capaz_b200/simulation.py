@@ -65,20 +65,25 @@ def write_ini(p: Params, path: str, extensions: bool = True) -> None:
 class Simulation:
     """A context of the C ABI (capaz_create ... capaz_destroy)."""
 
-    def __init__(self, params: Params, device: int = 0):
+    def __init__(self, params: Params, device: int = 0, _ctx=None):
         self.lib = native.load()
-        st = C.c_int(0)
         self.params = params.copy()
-        self.ctx = self.lib.capaz_create(C.byref(self.params), device, C.byref(st))
-        if not self.ctx:
-            msg = self.lib.capaz_last_error(None)
-            raise native.CapazError(st.value, msg.decode() if msg else "")
+        self._owned = _ctx is None
+        if _ctx is None:
+            st = C.c_int(0)
+            self.ctx = self.lib.capaz_create(C.byref(self.params), device, C.byref(st))
+            if not self.ctx:
+                msg = self.lib.capaz_last_error(None)
+                raise native.CapazError(st.value, msg.decode() if msg else "")
+        else:
+            self.ctx = _ctx
         self.shape = (params.nz, params.ny, params.nx)
 
     # -- lifetime --------------------------------------------------------
     def close(self) -> None:
         if getattr(self, "ctx", None):
-            self.lib.capaz_destroy(self.ctx)
+            if self._owned:
+                self.lib.capaz_destroy(self.ctx)
             self.ctx = None
 
     def __enter__(self):
@@ -130,3 +135,51 @@ class Simulation:
     @property
     def launch_count(self) -> int:
         return int(self.lib.capaz_launch_count(self.ctx))
+
+
+class Ensemble:
+    """A batch of instances stepped by one persistent launch per step
+    (capaz_batch_* in include/capaz_b200.h)."""
+
+    def __init__(self, params_list, device: int = 0):
+        self.lib = native.load()
+        n = len(params_list)
+        arr = (Params * n)(*[p.copy() for p in params_list])
+        st = C.c_int(0)
+        self.b = self.lib.capaz_batch_create(arr, n, device, C.byref(st))
+        if not self.b:
+            msg = self.lib.capaz_last_error(None)
+            raise native.CapazError(st.value, msg.decode() if msg else "")
+        self.instances = [Simulation(params_list[q], device, _ctx=self.lib.capaz_batch_instance(self.b, q))
+                          for q in range(n)]
+
+    def step(self, nsteps: int = 1, stream: int = 0) -> None:
+        check(self.lib.capaz_batch_step(self.b, int(nsteps), stream or None))
+
+    def autotune(self, stream: int = 0) -> dict:
+        zc, per = C.c_int(0), C.c_int(0)
+        check(self.lib.capaz_batch_autotune(self.b, stream or None, C.byref(zc), C.byref(per)))
+        return {"zchunk": zc.value, "ctas_per_sm": per.value}
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.lib.capaz_batch_launch_count(self.b))
+
+    def close(self) -> None:
+        if getattr(self, "b", None):
+            for s in self.instances:
+                s.ctx = None
+            self.lib.capaz_batch_destroy(self.b)
+            self.b = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

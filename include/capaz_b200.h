@@ -216,6 +216,29 @@ int capaz_read_diag(capaz_ctx* ctx, capaz_diag* out, void* stream);
  * consts.dt); host value, no device traffic beyond the kernel argument. */
 int capaz_set_dt(capaz_ctx* ctx, double dt);
 
+/* ---- ensembles ----------------------------------------------------------
+ * A batch steps `count` independent two-phase instances of uneven grid
+ * sizes (each with its own parameters, dt, m, K and state) with ONE
+ * persistent kernel launch per step: CTAs take (instance, tile, z-chunk)
+ * work items from a shared counter.  All instances must share phases (2),
+ * form, flags, and the relative-permeability / capillary class (lambda == 2
+ * or not, P_d == 0 or not); precision-form batches need nx % 4 == 0.
+ * Steps are replayed from a captured CUDA graph.  Fields are read and
+ * written through each instance's context (capaz_batch_instance), which the
+ * batch owns.  There is no counterpart in the reference (one problem per
+ * run, main.cpp:7-79). */
+typedef struct capaz_batch capaz_batch;
+capaz_batch* capaz_batch_create(const capaz_params* params, int count, int device, int* status);
+int capaz_batch_destroy(capaz_batch* b);
+capaz_ctx* capaz_batch_instance(capaz_batch* b, int index);
+int capaz_batch_step(capaz_batch* b, int nsteps, void* stream);
+/* Times candidate launch shapes (z-chunk depth, CTAs per SM) on the batch's
+ * own data for a few steps each, keeps the fastest, and restores every
+ * instance's state afterwards.  Writes the choice to zchunk / ctas_per_sm
+ * (either may be NULL). */
+int capaz_batch_autotune(capaz_batch* b, void* stream, int* zchunk, int* ctas_per_sm);
+int64_t capaz_batch_launch_count(const capaz_batch* b);
+
 /* Number of kernels the library launched on this context so far. */
 int64_t capaz_launch_count(const capaz_ctx* ctx);
 /* Synchronises the context's device and reports any pending CUDA error. */
