@@ -16,7 +16,7 @@ struct capaz_batch {
   std::vector<capaz_ctx*> ctx;
   int device = 0;
   bool fp32 = false;
-  TmaFlags tf{};
+  PhysF phys{};
   bool unik = true, pd0 = true;
   InstT* d_instT = nullptr;
   Inst64* d_inst64 = nullptr;
@@ -59,7 +59,7 @@ int bcuda(capaz_batch* b, cudaError_t e, const char* what) {
 int occupancy(const capaz_batch* b) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-  const int full = b->fp32 ? step2_fp32c_tma_grid(b->device, b->tf) : step2_fp64_batch_grid(b->device);
+  const int full = b->fp32 ? step2_fp32c_tma_grid(b->device, b->unik) : step2_fp64_batch_grid(b->device);
   return std::max(1, full / std::max(1, sms));
 }
 
@@ -80,11 +80,11 @@ int build(capaz_batch* b) {
       BTRY(b, cudaMemcpy(&h[q], x->tma_inst, sizeof(InstT), cudaMemcpyDeviceToHost));
       if (x->p.nz > 1) {
         const int interior = x->p.nz - 2;
-        h[q].c.zchunk = std::min(b->zchunk, interior);
-        h[q].c.nzchunks = (interior + h[q].c.zchunk - 1) / h[q].c.zchunk;
+        h[q].zchunk = std::min(b->zchunk, interior);
+        h[q].nzchunks = (interior + h[q].zchunk - 1) / h[q].zchunk;
       }
-      nz_chunks[q] = h[q].c.nzchunks;
-      ntiles[q] = h[q].c.tiles_x * h[q].c.tiles_y;
+      nz_chunks[q] = h[q].nzchunks;
+      ntiles[q] = h[q].tiles_x * h[q].tiles_y;
     }
     if (!b->d_instT) BTRY(b, cudaMalloc(&b->d_instT, sizeof(InstT) * n));
     BTRY(b, cudaMemcpy(b->d_instT, h.data(), sizeof(InstT) * n, cudaMemcpyHostToDevice));
@@ -154,7 +154,8 @@ bool stale(const capaz_batch* b) {
 
 cudaError_t launch_one(capaz_batch* b, int parity, cudaStream_t s) {
   if (b->fp32)
-    return launch_step2_fp32c_tma(b->d_instT, b->d_items, b->nitems, parity, b->tf, b->counter, nullptr, b->grid, s);
+    return launch_step2_fp32c_tma(b->phys, b->d_instT, b->d_items, b->nitems, parity, b->unik, b->counter, nullptr,
+                                  b->grid, s);
   return launch_step2_fp64_batch(b->d_inst64, b->d_items, b->nitems, parity, b->unik, b->pd0, b->counter, b->grid, s);
 }
 
@@ -237,10 +238,14 @@ capaz_batch* capaz_batch_create(const capaz_params* params, int count, int devic
     const capaz_params& p = params[q];
     const bool same = p.phases == 2 && p.form == p0.form && p.flags == p0.flags &&
                       (p.lambda == 2.0) == (p0.lambda == 2.0) && (p.P_d == 0.) == (p0.P_d == 0.);
-    const bool tma_ok = p.form != CAPAZ_FORM_FP32C || p.nx % 4 == 0;
+    // Precision-form batches run the TMA-staged kernel: nx % 4 == 0, P_d = 0,
+    // lambda = 2, and one set of physics constants for all instances.
+    PhysF a = make_physf(p), z = make_physf(p0);
+    const bool tma_ok = p.form != CAPAZ_FORM_FP32C ||
+                        (p.nx % 4 == 0 && p.P_d == 0. && p.lambda == 2.0 && memcmp(&a, &z, sizeof a) == 0);
     if (!same || !tma_ok) {
       g_batch_error = "batch instances must be two-phase with the same form, flags and model class; "
-                      "precision-form instances need nx % 4 == 0";
+                      "precision-form batches need nx % 4 == 0, P_d = 0, lambda = 2 and identical physics";
       if (status) *status = CAPAZ_ERR_INVALID_ARGUMENT;
       return nullptr;
     }
@@ -250,7 +255,7 @@ capaz_batch* capaz_batch_create(const capaz_params* params, int count, int devic
   b->fp32 = p0.form == CAPAZ_FORM_FP32C;
   b->unik = !(p0.flags & CAPAZ_FLAG_PERCELL_K);
   b->pd0 = p0.P_d == 0.;
-  b->tf = TmaFlags{b->unik, b->pd0, p0.lambda == 2.0};
+  b->phys = make_physf(p0);
   for (int q = 0; q < count; q++) {
     int st = 0;
     capaz_ctx* x = capaz_create(&params[q], device, &st);

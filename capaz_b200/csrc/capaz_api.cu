@@ -173,6 +173,32 @@ Step2FConst make_step2f_const(const capaz_params& p, double S_ref) {
   return c;
 }
 
+PhysF make_physf(const capaz_params& p) {
+  PhysF f;
+  memset(&f, 0, sizeof f);
+  f.inv_one_m_swr = (float)(1. / (1. - p.S_wr));
+  f.ro0w_bw = (float)(p.ro0_w * p.beta_w);
+  f.ro0n_bn = (float)(p.ro0_n * p.beta_n);
+  f.inv_mu_w = (float)(1. / p.mu_w);
+  f.inv_mu_n = (float)(1. / p.mu_n);
+  f.K0 = (float)p.K0;
+  f.inv_hx2 = (float)(1. / (p.hx * p.hx));
+  f.inv_hy2 = (float)(1. / (p.hy * p.hy));
+  f.inv_hz2 = (float)(1. / (p.hz * p.hz));
+  f.g_inv_hy = (float)(p.g_const / p.hy);
+  f.iters = 2;
+  f.ro0_w = p.ro0_w;
+  f.ro0_n = p.ro0_n;
+  f.aw = p.ro0_w * p.beta_w;
+  f.bn = p.ro0_n * p.beta_n;
+  f.P_atm = p.P_atm;
+  f.P_top = p.P_top_offset;
+  f.g = p.g_const;
+  f.hy = p.hy;
+  f.vol = p.hx * p.hy * p.hz;
+  return f;
+}
+
 Step3Const make_step3_const(const capaz_params& p) {
   Step3Const c;
   memset(&c, 0, sizeof c);
@@ -524,11 +550,13 @@ int capaz_ctx::allocate() {
     CUDA_TRY(this, cudaMalloc(&Pref, sizeof(double) * p.ny));
     CUDA_TRY(this, cudaMalloc(&PrelF, sizeof(float) * p.ny));
     CUDA_TRY(this, cudaMalloc(&dPrefF, sizeof(float) * p.ny));
+    CUDA_TRY(this, cudaMalloc(&rowF, sizeof(float4) * p.ny));
     std::vector<double> pref0(p.ny, p.P_atm);
     std::vector<float> z(p.ny, 0.f);
     CUDA_TRY(this, cudaMemcpy(Pref, pref0.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice));
     CUDA_TRY(this, cudaMemcpy(PrelF, z.data(), sizeof(float) * p.ny, cudaMemcpyHostToDevice));
     CUDA_TRY(this, cudaMemcpy(dPrefF, z.data(), sizeof(float) * p.ny, cudaMemcpyHostToDevice));
+    CUDA_TRY(this, launch_row_tables(Pref, p.ny, make_physf(p), rowF, nullptr));
   }
   CUDA_TRY(this, cudaMalloc(&first_bad, sizeof(unsigned long long)));
   CUDA_TRY(this, cudaMalloc(&sum_parts, sizeof(double) * 1024));
@@ -569,6 +597,7 @@ void capaz_ctx::release() {
   if (diag_partials) cudaFree(diag_partials);
   if (scratch) cudaFree(scratch);
   if (Pref) cudaFree(Pref);
+  if (rowF) cudaFree(rowF);
   if (stage) cudaFree(stage);
   if (tma_inst) cudaFree(tma_inst);
   if (tma_items) cudaFree(tma_items);
@@ -629,7 +658,8 @@ int capaz_ctx::set_field(int field, const void* src, bool on_device, cudaStream_
     if (d != dst) CUDA_TRY(this, cudaMemcpyAsync(dst, d, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   } else if (field == CAPAZ_FIELD_P_W) {
     CUDA_TRY(this, launch_encode_pressure(d, p.nx, p.ny, p.nz, p.P_atm, Pref, PrelF, dPrefF, (float*)dst, s));
-    launches += 3;
+    CUDA_TRY(this, launch_row_tables(Pref, p.ny, make_physf(p), rowF, s));
+    launches += 4;
   } else if (field == CAPAZ_FIELD_S_N) {
     CUDA_TRY(this, launch_encode_saturation(d, n, sum_parts, S_ref_dev, (float*)dst, s));
     launches += 3;

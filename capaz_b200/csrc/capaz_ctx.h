@@ -39,6 +39,8 @@ struct capaz_ctx {
   int tma_nitems = 0;
   unsigned int* tma_counter = nullptr;
   double tma_dt = 0., tma_S_ref = 0.;  // values baked into the descriptor
+  float4* rowF = nullptr;              // per-row tables (precision form)
+  bool tma_applies() const;
   int tma_grid = 0;
   bool tma_ready = false;
   int tma_prepare();
@@ -86,6 +88,7 @@ namespace capaz {
 Step2Const make_step2_const(const capaz_params& p);
 Step2FConst make_step2f_const(const capaz_params& p, double S_ref);
 Step3Const make_step3_const(const capaz_params& p);
+PhysF make_physf(const capaz_params& p);
 void reference_init_host(const capaz_params& p, const double* m, double* Pw, double* Sw, double* Sn, double* Pn,
                          double* Pg);
 }

@@ -106,20 +106,33 @@ cudaError_t launch_step2_fp32c_batch(const InstF* insts, const int4* items, int 
 int step2_fp64_batch_grid(int device);
 int step2_fp32c_batch_grid(int device);
 
-// TMA-staged precision-form step (step2_fp32c_tma.cu): one descriptor per
-// instance in global memory, tensor maps of the state ping-pong buffers.
+// TMA-staged precision-form step (step2_fp32c_tma.cu), for P_d = 0 and
+// lambda = 2.  Physics constants shared by every instance of a launch are a
+// kernel parameter; per-instance geometry, dt, S_ref and tensor maps live
+// in one descriptor per instance in global memory.
+struct PhysF {
+  float inv_one_m_swr, ro0w_bw, ro0n_bn, inv_mu_w, inv_mu_n, K0, inv_hx2, inv_hy2, inv_hz2, g_inv_hy;
+  int iters;
+  double ro0_w, ro0_n, aw, bn, P_atm, P_top, g, hy, vol;
+};
 struct alignas(128) InstT {
   CUtensorMap map_p[2], map_s[2], map_K, map_m;
-  Step2FConst c;
-  Step2FArgs a[2];  // a[parity]: reads buffer parity, writes parity ^ 1
+  int nx, ny, nz, tiles_x, tiles_y, zchunk, nzchunks, source;
+  long long sy, sz;
+  float c1_f;       // 1 - S_wr - S_ref
+  float dt_f;
+  float sgr_dev_f;  // S_n_gr - S_ref (stored deviation of the source saturation)
+  float pad_;
+  double S_ref, dt;
+  const float4* rowF;  // ny: (rho_w, rho_n at P_ref(j), (P_ref(j+1)-P_ref(j))/hy^2, 0)
+  const double* Pref;  // ny
+  Step2FArgs a[2];     // a[parity]: state pointers and the error flag
 };
-struct TmaFlags {
-  bool unik, pd0, lam2;
-};
-cudaError_t launch_step2_fp32c_tma(const InstT* insts, const int4* items, int nitems, int parity, const TmaFlags& f,
-                                   unsigned int* counter, double* diag_partials, int grid, cudaStream_t s);
-int step2_fp32c_tma_grid(int device, const TmaFlags& f);
+cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
+                                   bool unik, unsigned int* counter, double* diag_partials, int grid, cudaStream_t s);
+int step2_fp32c_tma_grid(int device, bool unik);
 int encode_field_map(CUtensorMap* map, const float* base, int nx, int ny, int nz);
+cudaError_t launch_row_tables(const double* Pref, int ny, const PhysF& f, float4* rowF, cudaStream_t s);
 
 // Field preparation (fields.cu).
 cudaError_t launch_first_invalid(const double* a, long long n, unsigned long long* first, cudaStream_t s);

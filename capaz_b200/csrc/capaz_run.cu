@@ -42,10 +42,11 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
     }
     return CAPAZ_OK;
   }
-  if (p.phases == 2 && p.form == CAPAZ_FORM_FP32C && p.nx % 4 == 0 && !(p.flags & CAPAZ_FLAG_NO_TMA)) {
+  if (tma_applies()) {
     int st = tma_prepare();
     if (st) return st;
-    const TmaFlags f{!(p.flags & CAPAZ_FLAG_PERCELL_K), p.P_d == 0., p.lambda == 2.0};
+    const PhysF f = make_physf(p);
+    const bool unik = !(p.flags & CAPAZ_FLAG_PERCELL_K);
     if (diag && !diag_partials) {
       diag_blocks = tma_grid;
       e = cudaMalloc(&diag_partials, sizeof(double) * DIAG_STRIDE * diag_blocks);
@@ -53,7 +54,7 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
     }
     for (int t = 0; t < nsteps; t++) {
       const bool last = t == nsteps - 1;
-      e = launch_step2_fp32c_tma(tma_inst, tma_items, tma_nitems, cur, f, tma_counter,
+      e = launch_step2_fp32c_tma(f, tma_inst, tma_items, tma_nitems, cur, unik, tma_counter,
                                  (diag && last) ? diag_partials : nullptr, tma_grid, s);
       launches++;
       if (e != cudaSuccess) return fail_cuda(e, "step2_fp32c_tma launch");
@@ -188,21 +189,44 @@ int capaz_ctx::derived(int field, cudaStream_t s, bool from_current) {
   return fail_msg(CAPAZ_ERR_UNSUPPORTED, "derived fields for this phase/form are not built yet");
 }
 
+bool capaz_ctx::tma_applies() const {
+  return p.phases == 2 && p.form == CAPAZ_FORM_FP32C && p.nx % 4 == 0 && p.P_d == 0. && p.lambda == 2.0 &&
+         !(p.flags & CAPAZ_FLAG_NO_TMA);
+}
+
 // Builds (or refreshes) the device descriptor of the TMA-staged precision
-// step: tensor maps of both state buffers and of K and m, the step constants
-// (which depend on dt and S_ref) and the work-item list.
+// step: tensor maps of both state buffers and of K and m, the geometry, dt
+// and S_ref, and the work-item list.
 int capaz_ctx::tma_prepare() {
   if (tma_ready && tma_dt == p.dt && tma_S_ref == S_ref) return CAPAZ_OK;
   InstT h;
   memset(&h, 0, sizeof h);
-  h.c = make_step2f_const(p, S_ref);
-  // Shorter z-chunks than the plain kernel: the dynamic schedule balances
-  // the work, and 16-plane chunks give enough items for every SM.
+  const Step2Const d = make_step2_const(p);
+  h.nx = p.nx;
+  h.ny = p.ny;
+  h.nz = p.nz;
+  h.tiles_x = d.tiles_x;
+  h.tiles_y = d.tiles_y;
+  h.source = p.source;
+  h.sy = d.sy;
+  h.sz = d.sz;
+  // 16-plane z-chunks: the dynamic schedule balances the work, and the
+  // chunk count gives every SM several items.
   if (p.nz > 1) {
     const int interior = p.nz - 2;
-    h.c.zchunk = std::min(16, interior);
-    h.c.nzchunks = (interior + h.c.zchunk - 1) / h.c.zchunk;
+    h.zchunk = std::min(16, interior);
+    h.nzchunks = (interior + h.zchunk - 1) / h.zchunk;
+  } else {
+    h.zchunk = 1;
+    h.nzchunks = 1;
   }
+  h.c1_f = (float)(1. - p.S_wr - S_ref);
+  h.dt_f = (float)p.dt;
+  h.sgr_dev_f = (float)(p.S_n_gr - S_ref);
+  h.S_ref = S_ref;
+  h.dt = p.dt;
+  h.rowF = rowF;
+  h.Pref = Pref;
   for (int b = 0; b < 2; b++) {
     if (encode_field_map(&h.map_p[b], (const float*)state[b][0], p.nx, p.ny, p.nz) ||
         encode_field_map(&h.map_s[b], (const float*)state[b][1], p.nx, p.ny, p.nz))
@@ -244,17 +268,16 @@ int capaz_ctx::tma_prepare() {
   if (!tma_items) {
     // Items ordered z-chunk-major: CTAs that run together work on the same
     // z range, so the halos of neighbouring tiles meet in L2.
-    const int ntiles = h.c.tiles_x * h.c.tiles_y;
+    const int ntiles = h.tiles_x * h.tiles_y;
     std::vector<int4> items;
-    for (int zc = 0; zc < h.c.nzchunks; zc++)
+    for (int zc = 0; zc < h.nzchunks; zc++)
       for (int t = 0; t < ntiles; t++) items.push_back(make_int4(0, t, zc, 0));
     tma_nitems = (int)items.size();
     e = cudaMalloc(&tma_items, sizeof(int4) * items.size());
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(items)");
     e = cudaMemcpy(tma_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy(items)");
-    const TmaFlags f{!(p.flags & CAPAZ_FLAG_PERCELL_K), p.P_d == 0., p.lambda == 2.0};
-    tma_grid = std::min(tma_nitems, step2_fp32c_tma_grid(device, f));
+    tma_grid = std::min(tma_nitems, step2_fp32c_tma_grid(device, !(p.flags & CAPAZ_FLAG_PERCELL_K)));
   }
   tma_dt = p.dt;
   tma_S_ref = S_ref;

@@ -88,6 +88,15 @@ __global__ void narrow_kernel(const double* __restrict__ a, long long n, float* 
   if (l < n) out[l] = (float)a[l];
 }
 
+__global__ void row_tables_kernel(const double* __restrict__ Pref, int ny, const PhysF f, float4* __restrict__ rowF) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ny) return;
+  const double prel = Pref[j] - f.P_atm;
+  const double dnext = (j + 1 < ny) ? (Pref[j + 1] - Pref[j]) : 0.;
+  rowF[j] = make_float4((float)(f.ro0_w + f.aw * prel), (float)(f.ro0_n + f.bn * prel),
+                        (float)(dnext * (double)f.inv_hy2), 0.f);
+}
+
 unsigned grid_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
 }  // namespace
@@ -111,6 +120,11 @@ cudaError_t launch_encode_saturation(const double* S, long long n, double* part 
   partial_sum_kernel<<<1024, 256, 0, s>>>(S, n, part);
   final_mean_kernel<<<1, 32, 0, s>>>(part, 1024, n, S_ref);
   encode_s_kernel<<<grid_for(n, 256), 256, 0, s>>>(S, S_ref, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_row_tables(const double* Pref, int ny, const PhysF& f, float4* rowF, cudaStream_t s) {
+  row_tables_kernel<<<(ny + 127) / 128, 128, 0, s>>>(Pref, ny, f, rowF);
   return cudaGetLastError();
 }
 
