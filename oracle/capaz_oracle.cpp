@@ -32,6 +32,8 @@
 //     (CAPAZ_FLAG_SOURCE_WINDOW), as the two-phase rule is.
 #include <math.h>
 #include <omp.h>
+
+#include <cmath>
 #include <stdlib.h>
 #include <string.h>
 
@@ -69,14 +71,44 @@ struct Grid {
   }
 };
 
+// Dual numbers (value, derivative) for the forward-mode (tangent-linear)
+// reference gradient: every operation carries its first derivative along one
+// direction.  Branches (upwind choices, |x|) follow the value, as the
+// forward step does.
+using std::fabs;
+using std::pow;
+
+struct Dual {
+  double v, d;
+  Dual(double x = 0.) : v(x), d(0.) {}
+  Dual(double x, double y) : v(x), d(y) {}
+};
+inline Dual operator+(const Dual& a, const Dual& b) { return Dual(a.v + b.v, a.d + b.d); }
+inline Dual operator-(const Dual& a, const Dual& b) { return Dual(a.v - b.v, a.d - b.d); }
+inline Dual operator-(const Dual& a) { return Dual(-a.v, -a.d); }
+inline Dual operator*(const Dual& a, const Dual& b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+inline Dual operator/(const Dual& a, const Dual& b) {
+  return Dual(a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v));
+}
+inline bool operator!(const Dual& a) { return !a.v; }
+inline Dual fabs(const Dual& a) { return a.v < 0 ? -a : a; }
+inline Dual pow(const Dual& a, double e) {
+  const double r = std::pow(a.v, e);
+  return Dual(r, (a.d == 0.) ? 0. : e * std::pow(a.v, e - 1.) * a.d);
+}
+inline double value(double x) { return x; }
+inline double value(const Dual& x) { return x.v; }
+
 // right_difference / left_difference / central_difference (cpu.cpp:185-314).
-inline double rdiff(const double* a, long l, long s, double h) { return (a[l + s] - a[l]) / h; }
-inline double ldiff(const double* a, long l, long s, double h) { return (a[l] - a[l - s]) / h; }
+template <class T>
+inline T rdiff(const T* a, long l, long s, double h) { return (a[l + s] - a[l]) / h; }
+template <class T>
+inline T ldiff(const T* a, long l, long s, double h) { return (a[l] - a[l - s]) / h; }
 inline double cdiff(const double* a, long l, long s, double h) { return (a[l + s] - a[l - s]) / (2. * h); }
 
 // directed_difference (cpu.cpp:236-264): first-order upwind flux difference.
-inline double directed(double x1, double x2, const double* Xi, const double* ro, long l, long s,
-                       double h) {
+template <class T>
+inline T directed(T x1, T x2, const T* Xi, const T* ro, long l, long s, double h) {
   return (((x2 + fabs(x2)) / 2. - (x1 - fabs(x1)) / 2.) * (-1.) * Xi[l] * ro[l] -
           (x1 + fabs(x1)) / 2. * (-1.) * Xi[l - s] * ro[l - s] +
           (x2 - fabs(x2)) / 2. * (-1.) * Xi[l + s] * ro[l + s]) /
@@ -150,34 +182,37 @@ inline double k_n3(double S_w_e, double S_n_e, double A) {
   return k_n;
 }
 
-struct Work {
-  std::vector<double> S_w, S_g, P_n, P_g, ro_w, ro_n, ro_g, Xi_w, Xi_n, Xi_g;
-  std::vector<double> roS_w, roS_n, roS_g, roS_w_old, roS_n_old, roS_g_old;
+template <class T>
+struct WorkT {
+  std::vector<T> S_w, S_g, P_n, P_g, ro_w, ro_n, ro_g, Xi_w, Xi_n, Xi_g;
+  std::vector<T> roS_w, roS_n, roS_g, roS_w_old, roS_n_old, roS_g_old;
   // Three-phase: P_n, P_g as u_calculation sees them (after ro_P_Xi), kept
   // when keep_u_pressures is set.
   bool keep_u_pressures = false;
   std::vector<double> Pn_u, Pg_u;
 };
+using Work = WorkT<double>;
 
 inline bool in_window(const capaz_params* p, int i, int k) {
   return (i >= p->nx / 2 - p->source) && (i <= p->nx / 2 + p->source) && (k >= p->nz / 2 - p->source) &&
          (k <= p->nz / 2 + p->source);
 }
 
-inline double Kc(const capaz_params* p, const double* K, long l) {
-  return ((p->flags & CAPAZ_FLAG_PERCELL_K) && K) ? K[l] : p->K0;
+template <class T>
+inline T Kc(const capaz_params* p, const T* K, long l) {
+  return ((p->flags & CAPAZ_FLAG_PERCELL_K) && K) ? K[l] : T(p->K0);
 }
 
 // ---------------------------------------------------------------------------
 // Two-phase step.
-void step2(const capaz_params* p, const Grid& g, double* P_w, double* S_n, const double* m,
-           const double* K, Work& w) {
+template <class T>
+void step2(const capaz_params* p, const Grid& g, T* P_w, T* S_n, const T* m, const T* K, WorkT<T>& w) {
   const double lam = p->lambda, S_wr = p->S_wr;
   const double e_kw = (2. + 3. * lam) / lam, e_kn = (2. + lam) / lam, e_pk = -1. / lam;
-  double *S_w = w.S_w.data(), *P_n = w.P_n.data(), *ro_w = w.ro_w.data(), *ro_n = w.ro_n.data();
-  double *Xi_w = w.Xi_w.data(), *Xi_n = w.Xi_n.data();
-  double *roS_w = w.roS_w.data(), *roS_n = w.roS_n.data();
-  double *roS_w_old = w.roS_w_old.data(), *roS_n_old = w.roS_n_old.data();
+  T *S_w = w.S_w.data(), *P_n = w.P_n.data(), *ro_w = w.ro_w.data(), *ro_n = w.ro_n.data();
+  T *Xi_w = w.Xi_w.data(), *Xi_n = w.Xi_n.data();
+  T *roS_w = w.roS_w.data(), *roS_n = w.roS_n.data();
+  T *roS_w_old = w.roS_w_old.data(), *roS_n_old = w.roS_n_old.data();
 
   // S_calculation (all cells).
 #pragma omp parallel for schedule(static)
@@ -186,10 +221,10 @@ void step2(const capaz_params* p, const Grid& g, double* P_w, double* S_n, const
   // ro_P_Xi_calculation (all cells are active on one rank).
 #pragma omp parallel for schedule(static)
   for (long l = 0; l < g.n; l++) {
-    double S_e = (1. - S_n[l] - S_wr) / (1. - S_wr);
-    double k_w = pow(S_e, e_kw);
-    double k_n = (1. - S_e) * (1. - S_e) * (1 - pow(S_e, e_kn));
-    double P_k = p->P_d * pow((1. - S_n[l] - S_wr) / (1. - S_wr), e_pk);
+    T S_e = (1. - S_n[l] - S_wr) / (1. - S_wr);
+    T k_w = pow(S_e, e_kw);
+    T k_n = (1. - S_e) * (1. - S_e) * (1 - pow(S_e, e_kn));
+    T P_k = p->P_d * pow((1. - S_n[l] - S_wr) / (1. - S_wr), e_pk);
     P_n[l] = P_w[l] + P_k;
     Xi_w[l] = -1. * Kc(p, K, l) * k_w / p->mu_w;
     Xi_n[l] = -1. * Kc(p, K, l) * k_n / p->mu_n;
@@ -208,7 +243,7 @@ void step2(const capaz_params* p, const Grid& g, double* P_w, double* S_n, const
         const double q_w = 0., q_n = 0.;  // wells_q (two-phase.cpp:187-192)
         roS_w[l] = ro_w[l] * (1. - S_n[l]);
         roS_n[l] = ro_n[l] * S_n[l];
-        double x1, x2, fx_w, fy_w, fz_w, fx_n, fy_n, fz_n;
+        T x1, x2, fx_w, fy_w, fz_w, fx_n, fy_n, fz_n;
         if (g.nz < 2) {
           fz_w = 0.;
           fz_n = 0.;
@@ -237,8 +272,8 @@ void step2(const capaz_params* p, const Grid& g, double* P_w, double* S_n, const
         x2 = -1. * rdiff(P_n, l, g.sy, p->hy) + p->g_const * (ro_n[l]);
         x1 = -1. * ldiff(P_n, l, g.sy, p->hy) + p->g_const * (ro_n[l]);
         fy_n = directed(x1, x2, Xi_n, ro_n, l, g.sy, p->hy);
-        double A1 = roS_w[l] - (p->dt / m[l]) * (-q_w + fx_w + fy_w + fz_w);
-        double A2 = roS_n[l] - (p->dt / m[l]) * (-q_n + fx_n + fy_n + fz_n);
+        T A1 = roS_w[l] - (p->dt / m[l]) * (-q_w + fx_w + fy_w + fz_w);
+        T A2 = roS_n[l] - (p->dt / m[l]) * (-q_n + fx_n + fy_n + fz_n);
         roS_w_old[l] = roS_w[l];
         roS_n_old[l] = roS_n[l];
         roS_w[l] = A1;
@@ -253,21 +288,21 @@ void step2(const capaz_params* p, const Grid& g, double* P_w, double* S_n, const
       for (int i = 0; i < g.nx; i++) {
         if (!g.interior(i, j, k)) continue;
         long l = g.at(i, j, k);
-        double Pw = P_w[l], Sn = S_n[l];
+        T Pw = P_w[l], Sn = S_n[l];
         for (int it = 1; it <= p->newton_iterations; it++) {
-          double S_e = (1 - Sn - S_wr) / (1 - S_wr);
-          double P_k = P_d * pow(S_e, (-1.) / lam);
-          double AAA = pow(S_e, (((-1.) / lam) - 1.));
-          double F1 = p->ro0_w * (1. + (p->beta_w) * (Pw - p->P_atm)) * (1. - Sn) - roS_w[l];
-          double F2 = p->ro0_n * (1. + (p->beta_n) * (Pw + P_k - p->P_atm)) * Sn - roS_n[l];
-          double PkS = AAA * (P_d) / (lam * (1 - S_wr));
-          double F1P = p->ro0_w * (p->beta_w) * (1 - Sn);
-          double F2P = p->ro0_n * (p->beta_n) * Sn;
-          double F1S = (-1) * (p->ro0_w) * (1 + (p->beta_w) * (Pw - p->P_atm));
-          double F2S = p->ro0_n * (1 + (p->beta_n) * (Pw + P_k - p->P_atm + (Sn * PkS)));
-          double det = F1P * F2S - F1S * F2P;
-          double nPw = Pw - (1 / det) * (F2S * F1 - F1S * F2);
-          double nSn = Sn - (1 / det) * (F1P * F2 - F2P * F1);
+          T S_e = (1 - Sn - S_wr) / (1 - S_wr);
+          T P_k = P_d * pow(S_e, (-1.) / lam);
+          T AAA = pow(S_e, (((-1.) / lam) - 1.));
+          T F1 = p->ro0_w * (1. + (p->beta_w) * (Pw - p->P_atm)) * (1. - Sn) - roS_w[l];
+          T F2 = p->ro0_n * (1. + (p->beta_n) * (Pw + P_k - p->P_atm)) * Sn - roS_n[l];
+          T PkS = AAA * (P_d) / (lam * (1 - S_wr));
+          T F1P = p->ro0_w * (p->beta_w) * (1 - Sn);
+          T F2P = p->ro0_n * (p->beta_n) * Sn;
+          T F1S = (-1) * (p->ro0_w) * (1 + (p->beta_w) * (Pw - p->P_atm));
+          T F2S = p->ro0_n * (1 + (p->beta_n) * (Pw + P_k - p->P_atm + (Sn * PkS)));
+          T det = F1P * F2S - F1S * F2P;
+          T nPw = Pw - (1 / det) * (F2S * F1 - F1S * F2);
+          T nSn = Sn - (1 / det) * (F1P * F2 - F2P * F1);
           Pw = nPw;
           Sn = nSn;
         }
@@ -286,13 +321,13 @@ void step2(const capaz_params* p, const Grid& g, double* P_w, double* S_n, const
         long l1 = g.basic(i, j, k);
         long l = g.at(i, j, k);
         if ((j != 0) || (p->source <= 0)) S_n[l] = S_n[l1];
-        if ((j == 0) && (p->source > 0)) S_n[l] = in_window(p, i, k) ? p->S_n_gr : S_n[l1];
+        if ((j == 0) && (p->source > 0)) S_n[l] = in_window(p, i, k) ? T(p->S_n_gr) : S_n[l1];
         if ((j != 0) && (j != g.ny - 1)) {
           P_w[l] = P_w[l1];
         } else if (j == 0) {
-          P_w[l] = p->P_atm + p->P_top_offset;
+          P_w[l] = T(p->P_atm + p->P_top_offset);
         } else {
-          double ro_g_dy = (ro_n[l1] * S_n[l1] + ro_w[l1] * (1 - S_n[l1])) * (m[l1]) * (p->g_const) * (p->hy);
+          T ro_g_dy = (ro_n[l1] * S_n[l1] + ro_w[l1] * (1 - S_n[l1])) * (m[l1]) * (p->g_const) * (p->hy);
           P_w[l] = P_w[l1] + ro_g_dy;
         }
       }
