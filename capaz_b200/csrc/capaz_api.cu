@@ -55,6 +55,8 @@ bool is_state_field(const capaz_params& p, int f) {
 
 }  // namespace
 
+void capaz::set_create_error(const char* msg) { g_create_error = msg; }
+
 // ---------------------------------------------------------------------------
 // Step constants.
 namespace capaz {

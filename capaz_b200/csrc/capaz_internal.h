@@ -9,6 +9,9 @@
 
 namespace capaz {
 
+// Message returned by capaz_last_error(NULL) (calls without a context).
+void set_create_error(const char* msg);
+
 // Output tile of the fused sweep: TX x TY interior cells per z-plane, one
 // thread per column, marching along z with a 3-plane ring in shared memory.
 constexpr int TX = 32;

@@ -25,6 +25,9 @@ ERR_BAD_STATE = 7
 ERR_INI = 8
 ERR_UNSUPPORTED = 9
 
+# Largest (ny-2)*max(nz-2,1) that capaz_mass_noalloc accepts.
+NOALLOC_MAX_ROWS = 131072
+
 FORM_FP64 = 0
 FORM_FP32C = 1
 
@@ -112,6 +115,7 @@ PROTOTYPES = {
     "capaz_batch_autotune": (C.c_int, [_VP, _VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "capaz_batch_launch_count": (C.c_int64, [_VP]),
     "capaz_sync": (C.c_int, [_VP]),
+    "capaz_mass_noalloc": (C.c_int, [C.POINTER(Params), _VP, _VP, _VP, _VP, _VP]),
 }
 
 _lib = None

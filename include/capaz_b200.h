@@ -244,6 +244,23 @@ int64_t capaz_launch_count(const capaz_ctx* ctx);
 /* Synchronises the context's device and reports any pending CUDA error. */
 int capaz_sync(capaz_ctx* ctx);
 
+/* ---- allocation-free mass balance ----------------------------------------
+ * No counterpart in the reference.  Sums, over the interior cells of a
+ * two-phase FP64 state held in caller-owned device memory (nz*ny*nx doubles
+ * each, the layout of the context fields), the quantities of
+ * CAPAZ_FLAG_DIAGNOSTICS: out[0..4] (device memory, the capaz_diag layout)
+ * receive mass_w, mass_n, 0, 0 and the count of cells whose P or S is not
+ * finite.  All scratch is a fixed device array of the library, so no call
+ * allocates memory.  The first call on a device (with that device current)
+ * does a one-time set-up of the scratch address; make it before any stream
+ * capture.  Grids with (ny-2)*max(nz-2,1) > CAPAZ_NOALLOC_MAX_ROWS are
+ * rejected with CAPAZ_ERR_UNSUPPORTED_GRID.  Calls that overlap on one
+ * device (other streams or host threads) share the scratch and race: order
+ * them.  Errors are reported through capaz_last_error(NULL). */
+#define CAPAZ_NOALLOC_MAX_ROWS 131072
+int capaz_mass_noalloc(const capaz_params* p, const double* P_w, const double* S_n, const double* m,
+                       double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
