@@ -279,6 +279,14 @@ def time_form(sim, K, W, stream, ws, local, clocks=None):
     return {"total_ms": reduce_max(total_ms, ws), "kern_ms": kern_ms, "launches": launches}
 
 
+def tma_applies(p) -> bool:
+    """Whether the precision form of `p` runs the TMA-staged kernel (two-phase,
+    nx % 4 == 0, no capillary pressure, lambda == 2, TMA not disabled)."""
+    from capaz_b200 import native
+    return (p.phases == 2 and p.nx % 4 == 0 and p.P_d == 0.0 and p.lambda_ == 2.0
+            and not (p.flags & native.FLAG_NO_TMA))
+
+
 def make_sim(w, form, dev, diag=False):
     from capaz_b200 import Simulation, native
     p = w.params.copy()
@@ -404,7 +412,8 @@ def run_capaz(args) -> None:
     peak, peak_kind = measured_peaks()
     abytes = ALGO_BYTES[(head, percell)] * ncell
     achieved = abytes / (t["kern_ms"] * 1e-3) / 1e9
-    kname = "step2_fp64_kernel" if head == "fp64" else "step2_fp32c_kernel"
+    kname = "step2_fp64_kernel" if head == "fp64" else (
+        "step2_fp32c_tma_kernel" if tma_applies(p) else "step2_fp32c_kernel")
     wl_key = f"{args.grid[0]}x{args.grid[1]}x{args.grid[2]}"
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": load_traffic(kname, wl_key), "kernel": kname,

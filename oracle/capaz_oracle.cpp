@@ -549,6 +549,30 @@ void velocities(const capaz_params* p, const Grid& g, const double* P, const dou
       }
 }
 
+// Two-phase data_initialization (two-phase.cu:6-65 as the GPU build runs
+// it): S_n from the injection window, P_w hydrostatic down each column with
+// the porosity inside the weight (P[j] = P[j-1] + rho_eff(j-1) m(j-1) g hy).
+template <class T>
+void init2(const capaz_params* p, const Grid& g, const T* m, T* P_w, T* S_n) {
+  std::vector<T> ro_w(g.n), ro_n(g.n);
+  for (int i = 0; i < g.nx; i++)
+    for (int j = 0; j < g.ny; j++)
+      for (int k = 0; k < g.nz; k++) {
+        long l = g.at(i, j, k);
+        if ((j == 0) && in_window(p, i, k)) S_n[l] = p->S_n_gr;
+        else S_n[l] = p->S_n_background;
+        if (j == 0) {
+          P_w[l] = p->P_atm;
+        } else {
+          long u = l - g.sy;
+          T ro_g_dy = (ro_n[u] * S_n[u] + ro_w[u] * (1 - S_n[u])) * (m[u]) * (p->g_const) * (p->hy);
+          P_w[l] = P_w[u] + ro_g_dy;
+        }
+        ro_w[l] = p->ro0_w * (1. + (p->beta_w) * (P_w[l] - p->P_atm));
+        ro_n[l] = p->ro0_n * (1. + (p->beta_n) * (P_w[l] - p->P_atm));
+      }
+}
+
 int check_grid(const capaz_params* p) {
   if (!p) return CAPAZ_ERR_INVALID_ARGUMENT;
   if (p->phases != 2 && p->phases != 3) return CAPAZ_ERR_INVALID_ARGUMENT;
@@ -574,24 +598,8 @@ int oracle_init(const capaz_params* p, const double* m_in, double* m, double* P_
   if (rc) return rc;
   Grid g(p);
   if (p->phases == 2) {
-    std::vector<double> ro_w(g.n), ro_n(g.n);
-    for (int i = 0; i < g.nx; i++)
-      for (int j = 0; j < g.ny; j++)
-        for (int k = 0; k < g.nz; k++) {
-          long l = g.at(i, j, k);
-          m[l] = m_in ? m_in[l] : p->porosity;
-          if ((j == 0) && in_window(p, i, k)) S_n[l] = p->S_n_gr;
-          else S_n[l] = p->S_n_background;
-          if (j == 0) {
-            P_w[l] = p->P_atm;
-          } else {
-            long u = l - g.sy;
-            double ro_g_dy = (ro_n[u] * S_n[u] + ro_w[u] * (1 - S_n[u])) * (m[u]) * (p->g_const) * (p->hy);
-            P_w[l] = P_w[u] + ro_g_dy;
-          }
-          ro_w[l] = p->ro0_w * (1. + (p->beta_w) * (P_w[l] - p->P_atm));
-          ro_n[l] = p->ro0_n * (1. + (p->beta_n) * (P_w[l] - p->P_atm));
-        }
+    for (long l = 0; l < g.n; l++) m[l] = m_in ? m_in[l] : p->porosity;
+    init2(p, g, m, P_w, S_n);
   } else {
     for (long l = 0; l < g.n; l++) {
       m[l] = m_in ? m_in[l] : p->porosity;
@@ -746,5 +754,60 @@ int oracle_step(const capaz_params* p, int nsteps, double* P_w, double* S_w, dou
 }
 
 int oracle_max_threads(void) { return omp_get_max_threads(); }
+
+// Forward-mode (tangent-linear) derivative of the observation misfit
+//   J = sum over t = every, 2*every, ... <= nsteps, o < nobs of
+//       ((1 - S_n(t, obs[o])) - data[(t/every - 1)*nobs + o])^2
+// along the direction (dlnK, dm) of (ln K, porosity), through nsteps
+// two-phase steps (the two-phase step above, instantiated on dual numbers:
+// the Newton iterations are differentiated as unrolled).  With init_from_m
+// the initial state is data_initialization's, a function of m; otherwise
+// (P0, S0) is the initial state and does not depend on the parameters.
+// dlnK / dm may be NULL (zero).  Per-cell K is used (the K array).
+int oracle_tangent(const capaz_params* p_in, int nsteps, const double* m, const double* K, const double* dlnK,
+                   const double* dm, int init_from_m, const double* P0, const double* S0, const long* obs,
+                   int nobs, int every, const double* data, double* J, double* dJ, int nthreads) {
+  int rc = check_grid(p_in);
+  if (rc) return rc;
+  if (p_in->phases != 2 || every < 1 || nsteps < 0 || !m || !K) return CAPAZ_ERR_INVALID_ARGUMENT;
+  if (!init_from_m && (!P0 || !S0)) return CAPAZ_ERR_INVALID_ARGUMENT;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  capaz_params pp = *p_in;
+  pp.flags |= CAPAZ_FLAG_PERCELL_K;
+  const capaz_params* p = &pp;
+  Grid g(p);
+  const long n = g.n;
+  std::vector<Dual> md(n), Kd(n), P(n), S(n);
+  for (long l = 0; l < n; l++) {
+    md[l] = Dual(m[l], dm ? dm[l] : 0.);
+    Kd[l] = Dual(K[l], dlnK ? K[l] * dlnK[l] : 0.);
+  }
+  if (init_from_m) {
+    init2(p, g, md.data(), P.data(), S.data());
+  } else {
+    for (long l = 0; l < n; l++) {
+      P[l] = Dual(P0[l]);
+      S[l] = Dual(S0[l]);
+    }
+  }
+  WorkT<Dual> w;
+  for (auto* v : {&w.S_w, &w.P_n, &w.ro_w, &w.ro_n, &w.Xi_w, &w.Xi_n, &w.roS_w, &w.roS_n, &w.roS_w_old,
+                  &w.roS_n_old})
+    v->assign(n, Dual(0.));
+  Dual acc(0.);
+  for (int t = 1; t <= nsteps; t++) {
+    step2(p, g, P.data(), S.data(), md.data(), Kd.data(), w);
+    if (t % every == 0) {
+      const double* d = data ? data + (size_t)(t / every - 1) * nobs : nullptr;
+      for (int o = 0; o < nobs; o++) {
+        Dual r = (1. - S[obs[o]]) - (d ? d[o] : 0.);
+        acc = acc + r * r;
+      }
+    }
+  }
+  if (J) *J = acc.v;
+  if (dJ) *dJ = acc.d;
+  return CAPAZ_OK;
+}
 
 }  // extern "C"

@@ -42,6 +42,9 @@ def load() -> C.CDLL:
                                     C.POINTER(P), C.POINTER(Diag), C.c_int]
         lib.oracle_step.restype = C.c_int
         lib.oracle_max_threads.restype = C.c_int
+        lib.oracle_tangent.argtypes = [C.POINTER(Params), C.c_int, P, P, P, P, C.c_int, P, P,
+                                       C.POINTER(C.c_long), C.c_int, C.c_int, P, P, P, C.c_int]
+        lib.oracle_tangent.restype = C.c_int
         _lib = lib
     return _lib
 
@@ -201,3 +204,21 @@ def ref_run(p: Params, nsteps: int, state: dict | None = None, m: np.ndarray | N
         dn = REF_DERIVED_2PH if p.phases == 2 else REF_DERIVED_3PH
         out["derived"] = {k: draw[a * n:(a + 1) * n].reshape(sh) for a, k in enumerate(dn)}
     return out
+
+
+def tangent(p: Params, nsteps: int, m, K, obs, every: int, data=None, dlnK=None, dm=None,
+            init_from_m: bool = True, P0=None, S0=None, nthreads: int = 0) -> tuple[float, float]:
+    """(J, dJ): the observation misfit after `nsteps` two-phase steps and its
+    forward-mode derivative along (dlnK, dm) (oracle_tangent)."""
+    sh = _shape(p)
+    f = lambda a: None if a is None else np.ascontiguousarray(np.broadcast_to(a, sh), dtype=np.float64)
+    m, K, dlnK, dm, P0, S0 = f(m), f(K), f(dlnK), f(dm), f(P0), f(S0)
+    obs = np.ascontiguousarray(obs, dtype=np.int64)
+    data = None if data is None else np.ascontiguousarray(data, dtype=np.float64)
+    J, dJ = C.c_double(), C.c_double()
+    rc = load().oracle_tangent(C.byref(p), nsteps, _ptr(m), _ptr(K), _ptr(dlnK), _ptr(dm), int(init_from_m),
+                               _ptr(P0), _ptr(S0), obs.ctypes.data_as(C.POINTER(C.c_long)), len(obs), every,
+                               _ptr(data), C.byref(J), C.byref(dJ), nthreads)
+    if rc:
+        raise RuntimeError(f"oracle_tangent failed: {rc}")
+    return J.value, dJ.value
