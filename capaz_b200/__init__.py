@@ -5,4 +5,4 @@ kernels for sm_100a).  This package holds its Python bindings, the
 defines.ini helpers and the benchmark workload generators.
 """
 from .native import FIELDS, CapazError, Params, load  # noqa: F401
-from .simulation import Ensemble, Simulation, default_params, params_from_ini, write_ini  # noqa: F401
+from .simulation import Adjoint, Ensemble, Simulation, default_params, params_from_ini, write_ini  # noqa: F401

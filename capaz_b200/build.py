@@ -39,6 +39,7 @@ CUDA_SOURCES = [
     ("capaz_api.cu", []),
     ("capaz_run.cu", []),
     ("batch.cu", []),
+    ("adjoint.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
 ]
 HEADERS = ["capaz_internal.h", "capaz_ctx.h"]

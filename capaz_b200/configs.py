@@ -158,3 +158,44 @@ def config3(form: int = native.FORM_FP32C, seed: int = 3, count: int = 64, dims=
         out.append(Workload(f"cfg3[{q}] {Nx}x{Ny}x{Nz}", p, steps, m, K,
                             {"workload_grid": [Nx, Ny, Nz], "sigma": sigma, "ell": ell, "dt": p.dt}))
     return out
+
+
+def config4(seed: int = 4, grid=(128, 128, 64), steps: int = 500, obs_every: int = 25,
+            checkpoint_every: int = 50) -> Workload:
+    """Inverse problem, 128x128x64 (gravity on z), FP64, 500 steps.  Truth:
+    lognormal K (sigma 1, ell 8) and its porosity field (seeded).  Prior
+    (the point where the gradient is taken): ln K = ln 1e-12, phi = 0.25.
+    S_w observed on a 4x4 lattice of vertical columns (every vertical cell)
+    every 25 steps: 16 x 64 x 20 = 20,480 observations; checkpoints every 50
+    steps.  `m`/`K` hold the prior; notes hold the truth and the observation
+    layout."""
+    Nx, Ny, Nz = grid
+    nx, ny, nz = Nx, Nz, Ny
+    p = two_phase_params(nx, ny, nz, form=native.FORM_FP64, percell_k=True)
+    m_true, K_true = heterogeneous_fields((nz, ny, nx), 1.0, 8.0, seed)
+    m0 = np.full((nz, ny, nx), 0.25)
+    K0 = np.full((nz, ny, nx), 1e-12)
+    p.dt = min(stable_dt(p, m_true, K_true), stable_dt(p, m0, K0))
+    ci = [nx // 8 + q * nx // 4 for q in range(4)]
+    ck = [nz // 8 + q * nz // 4 for q in range(4)]
+    obs = np.array([i + j * nx + k * nx * ny for i in ci for k in ck for j in range(ny)], dtype=np.int64)
+    return Workload(f"cfg4 two-phase adjoint {Nx}x{Ny}x{Nz}", p, steps, m0, K0,
+                    {"workload_grid": list(grid), "ref_grid": [nx, ny, nz], "dt": p.dt, "seed": seed,
+                     "m_true": m_true, "K_true": K_true, "obs": obs, "obs_every": obs_every,
+                     "checkpoint_every": checkpoint_every, "columns_i": ci, "columns_k": ck})
+
+
+def observe(params: Params, m: np.ndarray, K: np.ndarray, obs: np.ndarray, obs_every: int, steps: int,
+            device: int = 0) -> np.ndarray:
+    """S_w at the observed cells every `obs_every` steps of a run from the
+    reference initial state for porosity m (synthetic data of the truth)."""
+    from .simulation import Simulation
+    out = []
+    with Simulation(params, device=device) as s:
+        s.set_field("m", m)
+        s.set_field("K", K)
+        s.init_state()
+        for _ in range(steps // obs_every):
+            s.step(obs_every)
+            out.append(1.0 - s.get_field("S_n").reshape(-1)[obs])
+    return np.array(out)

@@ -36,6 +36,8 @@ FLAG_DIAGNOSTICS = 0x2
 FLAG_SOURCE_WINDOW = 0x4
 FLAG_NO_TMA = 0x8
 
+ADJ_INIT_FROM_M = 0x1
+
 FIELDS = {
     "P_w": 0, "S_n": 1, "S_w": 2, "m": 3, "K": 4, "P_n": 5, "P_g": 6, "S_g": 7,
     "ro_w": 8, "ro_n": 9, "ro_g": 10, "Xi_w": 11, "Xi_n": 12, "Xi_g": 13,
@@ -115,6 +117,11 @@ PROTOTYPES = {
     "capaz_batch_autotune": (C.c_int, [_VP, _VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "capaz_batch_launch_count": (C.c_int64, [_VP]),
     "capaz_sync": (C.c_int, [_VP]),
+    "capaz_adjoint_create": (_VP, [_VP, C.c_int, C.c_int, _VP, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "capaz_adjoint_destroy": (C.c_int, [_VP]),
+    "capaz_adjoint_set_observations": (C.c_int, [_VP, _VP, C.c_int, _VP]),
+    "capaz_forward_checkpointed": (C.c_int, [_VP, C.POINTER(C.c_double), _VP]),
+    "capaz_backward": (C.c_int, [_VP, _VP, _VP, C.c_int, _VP]),
     "capaz_mass_noalloc": (C.c_int, [C.POINTER(Params), _VP, _VP, _VP, _VP, _VP]),
 }
 

@@ -183,3 +183,56 @@ class Ensemble:
             self.close()
         except Exception:
             pass
+
+
+class Adjoint:
+    """Misfit gradient of a two-phase FP64 context (capaz_adjoint_create ...
+    capaz_backward): J = sum over observation times and cells of
+    (S_w - data)^2, gradients with respect to ln K and porosity per cell."""
+
+    def __init__(self, sim: Simulation, nsteps: int, obs_cells, obs_every: int, checkpoint_every: int = 50,
+                 init_from_m: bool = True):
+        self.sim = sim
+        self.lib = sim.lib
+        self.obs = np.ascontiguousarray(obs_cells, dtype=np.int64)
+        self.nsteps, self.obs_every = int(nsteps), int(obs_every)
+        self.ntimes = self.nsteps // self.obs_every
+        st = C.c_int(0)
+        flags = native.ADJ_INIT_FROM_M if init_from_m else 0
+        self.adj = self.lib.capaz_adjoint_create(sim.ctx, self.nsteps, int(checkpoint_every), self.obs.ctypes.data,
+                                                 len(self.obs), self.obs_every, flags, C.byref(st))
+        if not self.adj:
+            msg = self.lib.capaz_last_error(None)
+            raise native.CapazError(st.value, msg.decode() if msg else "")
+
+    def set_observations(self, data) -> None:
+        d = np.ascontiguousarray(np.asarray(data, dtype=np.float64).reshape(self.ntimes, len(self.obs)))
+        check(self.lib.capaz_adjoint_set_observations(self.adj, d.ctypes.data, 0, None), self.sim.ctx)
+
+    def forward(self, stream: int = 0) -> float:
+        J = C.c_double(0.0)
+        check(self.lib.capaz_forward_checkpointed(self.adj, C.byref(J), stream or None), self.sim.ctx)
+        return J.value
+
+    def backward(self, stream: int = 0):
+        gK = np.empty(self.sim.shape, dtype=np.float64)
+        gm = np.empty(self.sim.shape, dtype=np.float64)
+        check(self.lib.capaz_backward(self.adj, gK.ctypes.data, gm.ctypes.data, 0, stream or None), self.sim.ctx)
+        return gK, gm
+
+    def close(self) -> None:
+        if getattr(self, "adj", None):
+            self.lib.capaz_adjoint_destroy(self.adj)
+            self.adj = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -244,6 +244,33 @@ int64_t capaz_launch_count(const capaz_ctx* ctx);
 /* Synchronises the context's device and reports any pending CUDA error. */
 int capaz_sync(capaz_ctx* ctx);
 
+/* ---- differentiation ------------------------------------------------------
+ * Discrete adjoint of the two-phase FP64 step (CAPAZ_FORM_FP64 with
+ * CAPAZ_FLAG_PERCELL_K).  The misfit is
+ *   J = sum over t = obs_every, 2*obs_every, ... <= nsteps and o < nobs of
+ *       ((1 - S_n(t, obs_cells[o])) - data[(t/obs_every - 1)*nobs + o])^2,
+ * i.e. squared differences of the wetting saturation at the observed cells
+ * (flat indices i + j*nx + k*nx*ny, distinct) every obs_every steps.
+ * capaz_forward_checkpointed runs nsteps steps of the context (from its
+ * current state, or with CAPAZ_ADJ_INIT_FROM_M from data_initialization's
+ * state for the context's porosity, which makes that state a function of m),
+ * saving the state every checkpoint_every steps; the context is left at
+ * step nsteps.  capaz_backward recomputes each checkpoint segment and sweeps
+ * it in reverse, giving dJ/d(ln K) and dJ/dm per cell (nx*ny*nz float64 each,
+ * host or device destinations; either may be NULL).  The Newton recovery is
+ * transposed through the implicit-function theorem at its final iterate.
+ * Memory: (ceil(nsteps/checkpoint_every) + checkpoint_every + 12) * 8 bytes
+ * per cell, plus the observations. */
+#define CAPAZ_ADJ_INIT_FROM_M 0x1
+typedef struct capaz_adjoint capaz_adjoint;
+capaz_adjoint* capaz_adjoint_create(capaz_ctx* ctx, int nsteps, int checkpoint_every, const long long* obs_cells,
+                                    int nobs, int obs_every, int flags, int* status);
+int capaz_adjoint_destroy(capaz_adjoint* a);
+/* data: (nsteps/obs_every) x nobs float64, zero until set. */
+int capaz_adjoint_set_observations(capaz_adjoint* a, const double* data, int on_device, void* stream);
+int capaz_forward_checkpointed(capaz_adjoint* a, double* misfit, void* stream);
+int capaz_backward(capaz_adjoint* a, double* grad_lnK, double* grad_m, int dst_on_device, void* stream);
+
 /* ---- allocation-free mass balance ----------------------------------------
  * No counterpart in the reference.  Sums, over the interior cells of a
  * two-phase FP64 state held in caller-owned device memory (nz*ny*nx doubles
