@@ -68,6 +68,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     return ap.parse_args()
 
 
@@ -327,6 +328,84 @@ def precision_check(w, dev, steps):
     return r
 
 
+def adjoint_leg(dev) -> dict:
+    """Differentiation form on the config-4 inverse problem (128x128x64,
+    FP64, 500 steps, checkpoints every 50): time of one forward solve vs. one
+    gradient (checkpointed forward + backward), and central differences of
+    the misfit (step 1e-6 in ln K and in porosity) at 32 seeded random cells
+    among those whose gradient is at least 1% of the largest."""
+    import torch
+
+    from capaz_b200 import Adjoint, Simulation
+    from capaz_b200.configs import config4, observe
+    w = config4()
+    p, obs, every = w.params, w.notes["obs"], w.notes["obs_every"]
+    steps, cp = w.steps, w.notes["checkpoint_every"]
+    data = observe(p, w.notes["m_true"], w.notes["K_true"], obs, every, steps, device=dev)
+
+    def best_of(fn, reps=3):
+        best, out = float("inf"), None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            best = min(best, time.perf_counter() - t0)
+        return best, out
+
+    with Simulation(p, device=dev) as sim:
+        sim.set_field("m", w.m)
+        sim.set_field("K", w.K)
+
+        def forward_solve():
+            sim.init_state()
+            sim.step(steps)
+            sim.sync()
+        t_fwd, _ = best_of(forward_solve)
+        with Adjoint(sim, steps, obs, every, cp) as adj:
+            adj.set_observations(data)
+            t_grad, (J, (gK, gm)) = best_of(lambda: (adj.forward(), adj.backward()))
+
+    def misfit(m, K):
+        with Simulation(p, device=dev) as sim:
+            sim.set_field("m", m)
+            sim.set_field("K", K)
+            with Adjoint(sim, steps, obs, every, steps) as adj:
+                adj.set_observations(data)
+                return adj.forward()
+
+    h = 1e-6
+    rng = np.random.default_rng(32)
+    fd_out = {}
+    for which, g in (("lnK", gK), ("porosity", gm)):
+        flat = np.abs(g).ravel()
+        pool = np.flatnonzero(flat >= 1e-2 * flat.max())
+        cells = rng.choice(pool, min(32, len(pool)), replace=False)
+        fd, ad = [], []
+        for l in cells:
+            mp, mq = w.m.copy().reshape(-1), w.m.copy().reshape(-1)
+            Kp, Kq = w.K.copy().reshape(-1), w.K.copy().reshape(-1)
+            if which == "lnK":
+                Kp[l] *= math.exp(h)
+                Kq[l] *= math.exp(-h)
+            else:
+                mp[l] += h
+                mq[l] -= h
+            fd.append((misfit(mp.reshape(w.m.shape), Kp.reshape(w.K.shape)) -
+                       misfit(mq.reshape(w.m.shape), Kq.reshape(w.K.shape))) / (2 * h))
+            ad.append(float(g.ravel()[l]))
+        fd, ad = np.array(fd), np.array(ad)
+        fd_out[which] = {"cells": len(cells), "rel_l2": float(np.linalg.norm(fd - ad) / np.linalg.norm(fd)),
+                         "max_rel": float(np.max(np.abs(fd - ad) / np.abs(fd))),
+                         "pool_cells": int(len(pool))}
+    return {"workload": f"cfg4 two-phase inverse problem {w.notes['workload_grid']}, FP64, {steps} steps, "
+                        f"{len(obs)} observed cells every {every} steps, checkpoints every {cp}",
+            "forward_ms": t_fwd * 1e3, "gradient_ms": t_grad * 1e3, "adjoint_over_forward": t_grad / t_fwd,
+            "misfit": J, "fd_step": h, "fd": fd_out,
+            "timing": "wall clock around synchronised calls, best of 3; forward = data_initialization + "
+                      "500 steps; gradient = checkpointed forward (misfit) + backward (recompute + reverse sweep)"}
+
+
 def run_capaz(args) -> None:
     import torch
 
@@ -368,6 +447,14 @@ def run_capaz(args) -> None:
     prec = None
     if not args.no_precision and "fp32c" in forms and "fp64" in forms:
         prec = precision_check(w, dev, w.steps)
+
+    # ---- differentiation form (config 4) ------------------------------------
+    adj = None
+    if not args.no_adjoint and ws == 1:
+        try:
+            adj = adjoint_leg(dev)
+        except Exception as e:  # reported, never fatal to the headline line
+            adj = {"failed": str(e)}
 
     # ---- end to end through the C ABI with host buffers ---------------------
     e2e = None
@@ -453,6 +540,7 @@ def run_capaz(args) -> None:
             "speedup_fp32c_vs_fp64": (forms_out["fp32c"]["value"] / forms_out["fp64"]["value"]
                                       if "fp32c" in forms_out and "fp64" in forms_out else None),
             "precision": prec,
+            "adjoint": adj,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": t["launches"],
         }
         print(json.dumps(line), flush=True)

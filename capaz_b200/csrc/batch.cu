@@ -17,7 +17,7 @@ struct capaz_batch {
   int device = 0;
   bool fp32 = false;
   PhysF phys{};
-  bool unik = true, pd0 = true;
+  bool unik = true, pd0 = true, planar = false;
   InstT* d_instT = nullptr;
   Inst64* d_inst64 = nullptr;
   int4* d_items = nullptr;
@@ -154,8 +154,8 @@ bool stale(const capaz_batch* b) {
 
 cudaError_t launch_one(capaz_batch* b, int parity, cudaStream_t s) {
   if (b->fp32)
-    return launch_step2_fp32c_tma(b->phys, b->d_instT, b->d_items, b->nitems, parity, b->unik, b->counter, nullptr,
-                                  b->grid, s);
+    return launch_step2_fp32c_tma(b->phys, b->d_instT, b->d_items, b->nitems, parity, b->unik, b->planar,
+                                  b->counter, nullptr, b->grid, s);
   return launch_step2_fp64_batch(b->d_inst64, b->d_items, b->nitems, parity, b->unik, b->pd0, b->counter, b->grid, s);
 }
 
@@ -242,10 +242,12 @@ capaz_batch* capaz_batch_create(const capaz_params* params, int count, int devic
     // lambda = 2, and one set of physics constants for all instances.
     PhysF a = make_physf(p), z = make_physf(p0);
     const bool tma_ok = p.form != CAPAZ_FORM_FP32C ||
-                        (p.nx % 4 == 0 && p.P_d == 0. && p.lambda == 2.0 && memcmp(&a, &z, sizeof a) == 0);
+                        (p.nx % 4 == 0 && p.P_d == 0. && p.lambda == 2.0 && memcmp(&a, &z, sizeof a) == 0 &&
+                         (p.nz == 1) == (p0.nz == 1));
     if (!same || !tma_ok) {
       g_batch_error = "batch instances must be two-phase with the same form, flags and model class; "
-                      "precision-form batches need nx % 4 == 0, P_d = 0, lambda = 2 and identical physics";
+                      "precision-form batches need nx % 4 == 0, P_d = 0, lambda = 2, identical physics and "
+                      "all instances planar (nz == 1) or all three-dimensional";
       if (status) *status = CAPAZ_ERR_INVALID_ARGUMENT;
       return nullptr;
     }
@@ -255,6 +257,7 @@ capaz_batch* capaz_batch_create(const capaz_params* params, int count, int devic
   b->fp32 = p0.form == CAPAZ_FORM_FP32C;
   b->unik = !(p0.flags & CAPAZ_FLAG_PERCELL_K);
   b->pd0 = p0.P_d == 0.;
+  b->planar = p0.nz == 1;
   b->phys = make_physf(p0);
   for (int q = 0; q < count; q++) {
     int st = 0;

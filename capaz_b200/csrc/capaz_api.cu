@@ -188,7 +188,7 @@ PhysF make_physf(const capaz_params& p) {
   f.inv_hy2 = (float)(1. / (p.hy * p.hy));
   f.inv_hz2 = (float)(1. / (p.hz * p.hz));
   f.g_inv_hy = (float)(p.g_const / p.hy);
-  f.iters = 2;
+  f.iters = 1;  // one Newton step: the delta-form solve of the TMA kernel
   f.ro0_w = p.ro0_w;
   f.ro0_n = p.ro0_n;
   f.aw = p.ro0_w * p.beta_w;

@@ -131,8 +131,13 @@ struct alignas(128) InstT {
   const double* Pref;  // ny
   Step2FArgs a[2];     // a[parity]: state pointers and the error flag
 };
+// Tile of the TMA-staged precision step: TX x TMA_TILE_Y interior cells
+// (each thread row owns two cell rows).
+constexpr int TMA_TILE_Y = 2 * TY;
+// All instances of one launch are planar (nz == 1) or all three-dimensional.
 cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
-                                   bool unik, unsigned int* counter, double* diag_partials, int grid, cudaStream_t s);
+                                   bool unik, bool planar, unsigned int* counter, double* diag_partials, int grid,
+                                   cudaStream_t s);
 int step2_fp32c_tma_grid(int device, bool unik);
 int encode_field_map(CUtensorMap* map, const float* base, int nx, int ny, int nz);
 cudaError_t launch_row_tables(const double* Pref, int ny, const PhysF& f, float4* rowF, cudaStream_t s);

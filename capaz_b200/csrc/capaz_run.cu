@@ -54,7 +54,7 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
     }
     for (int t = 0; t < nsteps; t++) {
       const bool last = t == nsteps - 1;
-      e = launch_step2_fp32c_tma(f, tma_inst, tma_items, tma_nitems, cur, unik, tma_counter,
+      e = launch_step2_fp32c_tma(f, tma_inst, tma_items, tma_nitems, cur, unik, p.nz == 1, tma_counter,
                                  (diag && last) ? diag_partials : nullptr, tma_grid, s);
       launches++;
       if (e != cudaSuccess) return fail_cuda(e, "step2_fp32c_tma launch");
@@ -206,7 +206,7 @@ int capaz_ctx::tma_prepare() {
   h.ny = p.ny;
   h.nz = p.nz;
   h.tiles_x = d.tiles_x;
-  h.tiles_y = d.tiles_y;
+  h.tiles_y = (p.ny - 2 + TMA_TILE_Y - 1) / TMA_TILE_Y;
   h.source = p.source;
   h.sy = d.sy;
   h.sz = d.sz;

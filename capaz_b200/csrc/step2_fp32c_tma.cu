@@ -8,14 +8,18 @@
 //   - persistent CTAs take (instance, tile, z-chunk) work items from a global
 //     counter, so one launch covers one grid or a whole ensemble of uneven
 //     grids without tail waves;
+//   - a tile is 32 x 16 cells; each of the 256 threads owns two cells of a
+//     column (rows ty and ty + 8), which halves the per-cell share of the
+//     plane loop's fixed work and brings the halo down to 96 cells per 512;
 //   - one elected thread streams the raw planes (p, s, K, m) of the tile's
-//     window (a 36 x 10 box at x = 32*ti, a 128-byte-aligned start) into a
-//     4-stage shared-memory ring with cp.async.bulk.tensor (TMA, 3-D tensor
-//     maps, no multicast) completing on mbarriers, 4 planes ahead of use;
-//   - every thread derives its own cell (halo threads one more cell) into a
-//     4-slot ring of derived planes (p, M_w, M_n), keeps its own column's
-//     k-1/k/k+1 values in registers, and computes the centre plane's fluxes:
-//     one barrier per plane;
+//     window (a 36 x 18 box at x = 32*ti, a 128-byte-aligned start) into a
+//     3-stage shared-memory ring with cp.async.bulk.tensor (TMA, 3-D tensor
+//     maps, no multicast) completing on mbarriers;
+//   - every thread derives its cells (three warps one halo cell more; the
+//     window's corners are never read) into a 3-slot ring of derived planes,
+//     (p, M_w, M_n) packed as float4, and reads the centre plane and its
+//     -z / +z neighbours from the ring: one barrier per plane, and few enough
+//     registers for three CTAs per SM;
 //   - physics constants are kernel parameters (constant-bank operands);
 //     per-row quantities (rho at the row's reference pressure, the scaled
 //     reference-pressure step) come from small per-instance tables.
@@ -24,8 +28,9 @@
 // phases; outflow through the + face is x2 * M(upwind), inflow through the
 // - face x1 * M(upwind); the in/out difference of an axis is formed first
 // (exact when the two nearly cancel, by Sterbenz's lemma) and the three axis
-// terms are Kahan-summed.  d(rho S) = -dt/m * div goes to FP64; the Newton is
-// a chord iteration on (dP, dS) with the Jacobian at the stored state.
+// terms are Kahan-summed.  d(rho S) = -dt/m * div goes to FP64, where one
+// Newton step with the Jacobian at the stored state solves the bilinear
+// system for (dP, dS).
 // Waits on mbarriers are bounded; a wait that runs out sets bit 1 of the
 // error flag and the CTA carries on, so the kernel always finishes.
 #include <cuda.h>
@@ -37,17 +42,21 @@
 namespace capaz {
 namespace {
 
-constexpr int BXW = 36;   // TMA box width (floats): 144 bytes, a multiple of 16
-constexpr int BYW = 10;   // TMA box height: TY + 2
-constexpr int NST = 4;    // raw-plane stages in flight
-constexpr int RAWN = 384; // floats reserved per array per stage (1536 B, 128-B multiple)
+constexpr int TYT = 2 * TY;        // tile height: each thread row owns two cell rows (ty, ty + 8)
+constexpr int WX = TX + 2;         // derived-plane window: tile plus a one-cell halo
+constexpr int WY = TYT + 2;
+constexpr int WCELLS = WX * WY;
+constexpr int NHALO = 2 * TX + 2 * TYT;  // halo cells derived by threads 0..NHALO-1 (no corners)
+constexpr int BXW = 36;            // TMA box width (floats): 144 bytes, a multiple of 16
+constexpr int BYW = WY;            // TMA box height
+constexpr int NST = 3;             // planes in flight (raw stages and derived slots)
+constexpr int RAWN = 672;          // floats reserved per array per stage (2688 B, 128-B multiple)
+static_assert(BXW * BYW <= RAWN, "raw stage too small");
+static_assert(NHALO <= NTHREADS, "halo cells exceed the block");
 constexpr unsigned long long WAIT_LIMIT = 1ull << 22;  // try_wait polls before giving up
 
 struct alignas(128) RawStage {
   float p[RAWN], s[RAWN], K[RAWN], m[RAWN];
-};
-struct DerPlane {
-  float p[PC], Mw[PC], Mn[PC];
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
@@ -147,250 +156,301 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-template <bool UNIK, bool DIAG>
-__global__ void __launch_bounds__(NTHREADS, 3)
+// Boundary cells whose basic coordinate (cpu.cpp:107-141) is interior cell
+// (i, j, k), written from its new state and its start-of-step densities
+// (Border_S / Border_P, two-phase.cpp:59-111).  Out of line: only cells next
+// to a face take it.
+__device__ __forceinline__ void write_boundary(const PhysF& f, const InstT* __restrict__ I, float* __restrict__ p_out,
+                                            float* __restrict__ s_out, int i, int j, int k, float pn, float snew,
+                                            double prel, double rw, double rn, float mc) {
+  const int nx = I->nx, ny = I->ny, nz = I->nz;
+  const bool planar = nz == 1;
+  const long long sy = I->sy, sz = I->sz;
+  const double Snew = I->S_ref + (double)snew;
+  const double Pnew = (prel + f.P_atm) + (double)pn;
+  const double ro_g_dy = (rn * Snew + rw * (1 - Snew)) * (double)mc * f.g * f.hy;
+  const int xo = (i == 1) ? 0 : ((i == nx - 2) ? nx - 1 : -1);
+  const int xo2 = (i == 1 && i == nx - 2) ? nx - 1 : -1;
+  const int yo = (j == 1) ? 0 : ((j == ny - 2) ? ny - 1 : -1);
+  const int yo2 = (j == 1 && j == ny - 2) ? ny - 1 : -1;
+  const int zo = planar ? -1 : ((k == 1) ? 0 : ((k == nz - 2) ? nz - 1 : -1));
+  const int zo2 = (!planar && k == 1 && k == nz - 2) ? nz - 1 : -1;
+  for (int qa = 0; qa < 3; qa++) {
+    const int bi = qa == 0 ? i : (qa == 1 ? xo : xo2);
+    if (bi < 0) continue;
+    for (int qb = 0; qb < 3; qb++) {
+      const int bj = qb == 0 ? j : (qb == 1 ? yo : yo2);
+      if (bj < 0) continue;
+      for (int qd = 0; qd < 3; qd++) {
+        const int bk = qd == 0 ? k : (qd == 1 ? zo : zo2);
+        if (bk < 0) continue;
+        if (qa == 0 && qb == 0 && qd == 0) continue;
+        const long long lb = bi + bj * sy + (long long)bk * sz;
+        float sb = snew;
+        if ((bj == 0) && (I->source > 0) && in_window(nx, nz, I->source, bi, bk)) sb = I->sgr_dev_f;
+        float pbv;
+        if ((bj != 0) && (bj != ny - 1)) pbv = pn;
+        else if (bj == 0) pbv = (float)((f.P_atm + f.P_top) - I->Pref[0]);
+        else pbv = (float)(Pnew + ro_g_dy - I->Pref[ny - 1]);
+        s_out[lb] = sb;
+        p_out[lb] = pbv;
+      }
+    }
+  }
+}
+
+// Shared memory of one CTA (dynamic, 62 KB: three CTAs per SM).
+struct Smem {
+  RawStage raw[NST];
+  float4 der[NST][WCELLS];  // (p, M_w, M_n, -) of the window, one slot per plane in flight
+  uint64_t bar[NST];
+  float4 rowF[WY];          // (rho_w, rho_n at the row's P_ref, dP_ref/hy^2 to the next row, -)
+  double rowPrel[WY];       // P_ref - P_atm
+  double rowPref[WY];
+  double red[NTHREADS / 32][4];  // diagnostics reduction
+  int w_sh;
+};
+constexpr size_t kSmemBytes = sizeof(Smem);
+
+#ifndef CAPAZ_TMA_MIN_BLOCKS
+#define CAPAZ_TMA_MIN_BLOCKS 3
+#endif
+template <bool UNIK, bool DIAG, bool PLANAR>
+__global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
     step2_fp32c_tma_kernel(const __grid_constant__ PhysF f, const InstT* __restrict__ insts,
                            const int4* __restrict__ items, int nitems, int parity, unsigned int* __restrict__ counter,
                            double* __restrict__ diag_partials) {
-  __shared__ RawStage raw[NST];
-  __shared__ DerPlane der[4];
-  __shared__ __align__(8) uint64_t bar[NST];
-  __shared__ int w_sh;
-  __shared__ float4 rowF[BYW];      // (rho_w, rho_n at the row's P_ref, dP_ref/hy^2 to the next row, -)
-  __shared__ double rowPrel[BYW];   // P_ref - P_atm
-  __shared__ double rowPref[BYW];
+  extern __shared__ __align__(128) unsigned char smem_bytes[];
+  Smem& sm = *reinterpret_cast<Smem*>(smem_bytes);
 
-  const int tid = threadIdx.x + TX * threadIdx.y;
   const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + TX * ty;
   if (tid == 0) {
-    for (int q = 0; q < NST; q++) mbar_init(&bar[q], 1);
+    for (int q = 0; q < NST; q++) mbar_init(&sm.bar[q], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
   uint32_t phase = 0;  // bit q: parity of the next completion of stage q
 
-  const int own_slot = (ty + 1) * PX + (tx + 1);
-  int halo_slot = -1;
-  if (tid < PC - NTHREADS) {
-    const int h = tid;
-    if (h < PX) halo_slot = h;
-    else if (h < 2 * PX) halo_slot = (PY - 1) * PX + (h - PX);
-    else if (h < 2 * PX + TY) halo_slot = (h - 2 * PX + 1) * PX;
-    else halo_slot = (h - 2 * PX - TY + 1) * PX + (PX - 1);
+  // The thread's two cells are tile rows ty and ty + 8 (window rows +1).
+  const int ownA = (ty + 1) * WX + (tx + 1), ownB = ownA + 8 * WX;
+  const int rawA = (ty + 1) * BXW + (tx + 1), rawB = rawA + 8 * BXW;
+  // Halo cells of the 7-point stencil (the window's corners are never read):
+  // warp 0 the row above the tile, warp 1 the row below, warp 2 the columns
+  // left (lanes 0-15) and right (lanes 16-31).
+  int halo_slot = -1, halo_raw = 0, halo_row = 0;
+  if (tid < NHALO) {
+    const int wq = tid >> 5, lane = tid & 31;
+    int hx, hy;
+    if (wq == 0) hx = lane + 1, hy = 0;
+    else if (wq == 1) hx = lane + 1, hy = WY - 1;
+    else if (lane < TYT) hx = 0, hy = lane + 1;
+    else hx = WX - 1, hy = lane - TYT + 1;
+    halo_slot = hy * WX + hx;
+    halo_raw = hy * BXW + hx;
+    halo_row = hy;
   }
-  const int own_raw = (ty + 1) * BXW + (tx + 1);
-  const int halo_raw = halo_slot >= 0 ? (halo_slot / PX) * BXW + (halo_slot % PX) : 0;
-  const int halo_row = halo_slot >= 0 ? halo_slot / PX : 0;
 
   double acc_w = 0., acc_n = 0., rmax = 0., nonfinite = 0.;
 
   for (;;) {
-    if (tid == 0) w_sh = (int)atomicAdd(counter, 1u);
+    if (tid == 0) sm.w_sh = (int)atomicAdd(counter, 1u);
     __syncthreads();
-    const int w = w_sh;
+    const int w = sm.w_sh;
     if (w >= nitems) break;
     const int4 it = items[w];
     const InstT* __restrict__ I = insts + it.x;
     const int nx = I->nx, ny = I->ny, nz = I->nz;
-    const long long sy = I->sy, sz = I->sz;
+    const int sy32 = (int)I->sy, sz32 = (int)I->sz;  // instances hold < 2^31 cells
     const float c1 = I->c1_f;
     const float dt_f = I->dt_f;
+    const double S_ref = I->S_ref;
     const Step2FArgs& A = I->a[parity];
     float* __restrict__ p_out = A.p_out;
     float* __restrict__ s_out = A.s_out;
+    unsigned int* __restrict__ err = A.err;
     const int tile = it.y, zc = it.z;
     const int ti = tile % I->tiles_x, tj = tile / I->tiles_x;
-    const int i0 = 1 + ti * TX, j0 = 1 + tj * TY;
+    const int i0 = 1 + ti * TX, j0 = 1 + tj * TYT;
     const int x0 = i0 - 1;  // == 32 * ti: 128-byte aligned TMA start
-    const int i = i0 + tx, j = j0 + ty;
-    const bool active = (i <= nx - 2) && (j <= ny - 2);
-    const bool edge_ij = (i == 1) || (i == nx - 2) || (j == 1) || (j == ny - 2);
-    const bool planar = nz == 1;
-    const int kb = planar ? 0 : 1 + zc * I->zchunk;
-    const int ke = planar ? 0 : min(kb + I->zchunk, nz - 1);  // last plane loaded
-    const int pb = planar ? 0 : kb - 1;                         // first plane loaded
+    const int i = i0 + tx, jA = j0 + ty, jB = jA + 8;
+    const bool activeA = (i <= nx - 2) && (jA <= ny - 2);
+    const bool activeB = (i <= nx - 2) && (jB <= ny - 2);
+    const int kb = PLANAR ? 0 : 1 + zc * I->zchunk;
+    const int ke = PLANAR ? 0 : min(kb + I->zchunk, nz - 1);  // last plane loaded
+    const int pb = PLANAR ? 0 : kb - 1;                         // first plane loaded
     const uint32_t stage_bytes = (UNIK ? 3u : 4u) * (uint32_t)(BXW * BYW * sizeof(float));
 
-    if (tid < BYW) {
+    if (tid < WY) {
       const int gj = min(j0 - 1 + tid, ny - 1);
-      rowF[tid] = I->rowF[gj];
-      rowPrel[tid] = I->Pref[gj] - f.P_atm;
-      rowPref[tid] = I->Pref[gj];
+      sm.rowF[tid] = I->rowF[gj];
+      sm.rowPrel[tid] = I->Pref[gj] - f.P_atm;
+      sm.rowPref[tid] = I->Pref[gj];
     }
     if (tid == 0) {
       for (int q = 0; q < NST && pb + q <= ke; q++) {
         const int pl = pb + q;
-        mbar_expect_tx(&bar[q], stage_bytes);
-        tma_load_3d(raw[q].p, &I->map_p[parity], x0, j0 - 1, pl, &bar[q]);
-        tma_load_3d(raw[q].s, &I->map_s[parity], x0, j0 - 1, pl, &bar[q]);
-        if (!UNIK) tma_load_3d(raw[q].K, &I->map_K, x0, j0 - 1, pl, &bar[q]);
-        tma_load_3d(raw[q].m, &I->map_m, x0, j0 - 1, pl, &bar[q]);
+        mbar_expect_tx(&sm.bar[q], stage_bytes);
+        tma_load_3d(sm.raw[q].p, &I->map_p[parity], x0, j0 - 1, pl, &sm.bar[q]);
+        tma_load_3d(sm.raw[q].s, &I->map_s[parity], x0, j0 - 1, pl, &sm.bar[q]);
+        if (!UNIK) tma_load_3d(sm.raw[q].K, &I->map_K, x0, j0 - 1, pl, &sm.bar[q]);
+        tma_load_3d(sm.raw[q].m, &I->map_m, x0, j0 - 1, pl, &sm.bar[q]);
       }
     }
     __syncthreads();
-    const float4 rowc = rowF[ty + 1];
-    const float dPs_up = rowc.z, dPs_dn = rowF[ty].z;
+    const float4 rowA = sm.rowF[ty + 1], rowB = sm.rowF[ty + 9];
+    const float dnA = sm.rowF[ty].z, dnB = sm.rowF[ty + 8].z;
 
-    Der dm{}, dc{}, dp{};  // own column at k-1, k, k+1 (stencil values)
-    Ctr cc{}, cn{};        // centre extras of planes k and k+1
-    for (int pl = pb; pl <= ke; pl++) {
-      const int st = (pl - pb) % NST;
-      {  // wait for the plane (bounded)
-        const uint32_t par = (phase >> st) & 1u;
-        unsigned long long tries = 0;
-        while (!mbar_try_wait(&bar[st], par)) {
-          if (++tries > WAIT_LIMIT) {
-            atomicOr(A.err, 2u);
-            break;
-          }
-        }
-        phase ^= (1u << st);
-      }
-      const RawStage& R = raw[st];
-      DerPlane& D = der[pl & 3];
-      dm = dc;
-      dc = dp;
-      cc = cn;
-      {
-        const float Kv = UNIK ? f.K0 : R.K[own_raw];
-        derive(f, c1, rowc.x, rowc.y, R.p[own_raw], R.s[own_raw], Kv, dp, cn.rw, cn.rn);
-        cn.s = R.s[own_raw];
-        cn.m = R.m[own_raw];
-        D.p[own_slot] = dp.p;
-        D.Mw[own_slot] = dp.Mw;
-        D.Mn[own_slot] = dp.Mn;
-      }
-      if (halo_slot >= 0) {
-        const float Kv = UNIK ? f.K0 : R.K[halo_raw];
-        const float4 rh = rowF[halo_row];
-        Der h;
-        float rw, rn;
-        derive(f, c1, rh.x, rh.y, R.p[halo_raw], R.s[halo_raw], Kv, h, rw, rn);
-        D.p[halo_slot] = h.p;
-        D.Mw[halo_slot] = h.Mw;
-        D.Mn[halo_slot] = h.Mn;
-      }
-      __syncthreads();
-      // Stage st is consumed by every thread: refill it four planes ahead.
-      if (tid == 0 && pl + NST <= ke) {
-        fence_proxy_async();
-        const int nxt = pl + NST;
-        mbar_expect_tx(&bar[st], stage_bytes);
-        tma_load_3d(raw[st].p, &I->map_p[parity], x0, j0 - 1, nxt, &bar[st]);
-        tma_load_3d(raw[st].s, &I->map_s[parity], x0, j0 - 1, nxt, &bar[st]);
-        if (!UNIK) tma_load_3d(raw[st].K, &I->map_K, x0, j0 - 1, nxt, &bar[st]);
-        tma_load_3d(raw[st].m, &I->map_m, x0, j0 - 1, nxt, &bar[st]);
-      }
-      // Centre plane: pl - 1 (3-D) or pl (planar).
-      if (!planar && pl < kb + 1) continue;
-      if (!active) continue;
-      const int k = planar ? pl : pl - 1;
-      const Der& C0 = planar ? dp : dc;
-      const Ctr& E = planar ? cn : cc;
-      const DerPlane& C = der[k & 3];
+    // The centre-plane update of one cell: D holds the centre plane, Dm / Dp
+    // the planes below and above it; sc, mc are the cell's saturation
+    // deviation and porosity.
+    auto update = [&](const float4* __restrict__ D, const float4* __restrict__ Dm, const float4* __restrict__ Dp,
+                      int own, float4 row, float dPs_dn, int wrow, float sc, float mc, int j, int k) {
+      const float4 c4 = D[own];
+      const Der C0{c4.x, c4.y, c4.z};
       float Dw, Dn;
       {
-        // x
-        const int a = own_slot - 1, b = own_slot + 1;
-        const float x1 = (C.p[a] - C0.p) * f.inv_hx2, x2 = (C0.p - C.p[b]) * f.inv_hx2;
-        const float dxw = face_diff(x1, x2, C0.Mw, C.Mw[a], C.Mw[b]);
-        const float dxn = face_diff(x1, x2, C0.Mn, C.Mn[a], C.Mn[b]);
+        const float4 a = D[own - 1], b = D[own + 1];
+        const float x1 = (a.x - C0.p) * f.inv_hx2, x2 = (C0.p - b.x) * f.inv_hx2;
+        const bool u1 = x1 > 0.f, u2 = x2 > 0.f;
+        const float dxw = x2 * (u2 ? C0.Mw : b.y) - x1 * (u1 ? a.y : C0.Mw);
+        const float dxn = x2 * (u2 ? C0.Mn : b.z) - x1 * (u1 ? a.z : C0.Mn);
         // y (vertical, gravity): P(j+1) - P(j) = dP_ref(j) + p(j+1) - p(j)
-        const int ya = own_slot - PX, yb = own_slot + PX;
-        const float gw = f.g_inv_hy * E.rw, gn = f.g_inv_hy * E.rn;
-        const float y1 = fmaf(C.p[ya] - C0.p, f.inv_hy2, -dPs_dn);
-        const float y2 = fmaf(C0.p - C.p[yb], f.inv_hy2, -dPs_up);
-        const float dyw = face_diff(y1 + gw, y2 + gw, C0.Mw, C.Mw[ya], C.Mw[yb]);
-        const float dyn = face_diff(y1 + gn, y2 + gn, C0.Mn, C.Mn[ya], C.Mn[yb]);
+        const float4 ya = D[own - WX], yb = D[own + WX];
+        const float rw = fmaf(f.ro0w_bw, C0.p, row.x), rn = fmaf(f.ro0n_bn, C0.p, row.y);
+        const float gw = f.g_inv_hy * rw, gn = f.g_inv_hy * rn;
+        const float y1 = fmaf(ya.x - C0.p, f.inv_hy2, -dPs_dn);
+        const float y2 = fmaf(C0.p - yb.x, f.inv_hy2, -row.z);
+        const float dyw = face_diff(y1 + gw, y2 + gw, C0.Mw, ya.y, yb.y);
+        const float dyn = face_diff(y1 + gn, y2 + gn, C0.Mn, ya.z, yb.z);
         Kahan3 kw(dxw), kn(dxn);
         kw.add(dyw);
         kn.add(dyn);
-        if (!planar) {
-          const float z1 = (dm.p - C0.p) * f.inv_hz2, z2 = (C0.p - dp.p) * f.inv_hz2;
-          kw.add(face_diff(z1, z2, C0.Mw, dm.Mw, dp.Mw));
-          kn.add(face_diff(z1, z2, C0.Mn, dm.Mn, dp.Mn));
+        if (!PLANAR) {
+          const float4 m4 = Dm[own], p4 = Dp[own];
+          const Der m1{m4.x, m4.y, m4.z}, p1{p4.x, p4.y, p4.z};
+          const float z1 = (m1.p - C0.p) * f.inv_hz2, z2 = (C0.p - p1.p) * f.inv_hz2;
+          const bool v1 = z1 > 0.f, v2 = z2 > 0.f;
+          kw.add(z2 * (v2 ? C0.Mw : p1.Mw) - z1 * (v1 ? m1.Mw : C0.Mw));
+          kn.add(z2 * (v2 ? C0.Mn : p1.Mn) - z1 * (v1 ? m1.Mn : C0.Mn));
         }
         Dw = kw.s - kw.c;
         Dn = kn.s - kn.c;
       }
-      // Conserved increments d(rho S) = -dt/m * div F (FP32 product, FP64 Newton).
-      const float dtm = __fdividef(dt_f, E.m);
+      // Conserved increments d(rho S) = -dt/m * div F (FP32), Newton in FP64.
+      const float dtm = __fdividef(dt_f, mc);
       const double Aw = (double)(-dtm * Dw);
       const double An = (double)(-dtm * Dn);
-
-      const double S = I->S_ref + (double)E.s;
-      const double prel = rowPrel[ty + 1] + (double)C0.p;
-      const double rw = fma(f.aw, prel, f.ro0_w);
-      const double rn = fma(f.bn, prel, f.ro0_n);
+      const double S = S_ref + (double)sc;
+      const double prel = sm.rowPrel[wrow];
+      const double pr = prel + (double)C0.p;
+      const double rw = fma(f.aw, pr, f.ro0_w);
+      const double rn = fma(f.bn, pr, f.ro0_n);
       const double J11 = f.aw * (1. - S), J21 = f.bn * S;
       const double inv = rcp64(fma(J11, rn, rw * J21));  // det = J11 J22 - J12 J21, J12 = -rw, J22 = rn
-      // Chord iteration: first step from (0, 0) is the linear solve.
-      double dP = (rn * Aw + rw * An) * inv;
-      double dS = (J11 * An - J21 * Aw) * inv;
+      // One Newton step from the stored state: the Jacobian solve of the
+      // bilinear system, exact up to the dP*dS terms (relative size
+      // |dS| / S ~ 1e-8 of the increments).  Diagnostics evaluate the
+      // residual of the reference's Newton functions at the result.
+      const double dP = (rn * Aw + rw * An) * inv;
+      const double dS = (J11 * An - J21 * Aw) * inv;
       double F1 = 0., F2 = 0.;
-      for (int itn = 1; itn < f.iters + (DIAG ? 1 : 0); itn++) {
+      if (DIAG) {
         F1 = fma(f.aw * dP, 1. - S - dS, -rw * dS) - Aw;
         F2 = fma(f.bn * dP, S + dS, rn * dS) - An;
-        if (itn == f.iters) break;  // diagnostics: residual at the final iterate
-        dP -= (rn * F1 + rw * F2) * inv;
-        dS -= (J11 * F2 - J21 * F1) * inv;
       }
-      const float p1 = (float)((double)C0.p + dP);
-      const float s1 = (float)((double)E.s + dS);
-      const long long l = i + j * sy + (long long)k * sz;
-      p_out[l] = p1;
-      s_out[l] = s1;
-      const bool finite = isfinite(p1) && isfinite(s1);
-      if (!finite) atomicOr(A.err, 1u);
+      const float pn = (float)((double)C0.p + dP);
+      const float snew = (float)((double)sc + dS);
+      const int l = i + j * sy32 + k * sz32;
+      p_out[l] = pn;
+      s_out[l] = snew;
+      const bool finite = isfinite(pn) && isfinite(snew);
+      if (!finite) atomicOr(err, 1u);
 
-      if (edge_ij || (!planar && ((k == 1) || (k == nz - 2)))) {
-        const double Snew = I->S_ref + (double)s1;
-        const double Pnew = rowPref[ty + 1] + (double)p1;
-        const double ro_g_dy = (rn * Snew + rw * (1 - Snew)) * (double)E.m * f.g * f.hy;
-        int xs[3], ys[3], zs[3], nxs = 0, nys = 0, nzs = 0;
-        xs[nxs++] = i;
-        if (i == 1) xs[nxs++] = 0;
-        if (i == nx - 2) xs[nxs++] = nx - 1;
-        ys[nys++] = j;
-        if (j == 1) ys[nys++] = 0;
-        if (j == ny - 2) ys[nys++] = ny - 1;
-        zs[nzs++] = k;
-        if (!planar) {
-          if (k == 1) zs[nzs++] = 0;
-          if (k == nz - 2) zs[nzs++] = nz - 1;
-        }
-        for (int qa = 0; qa < nxs; qa++)
-          for (int qb = 0; qb < nys; qb++)
-            for (int qd = 0; qd < nzs; qd++) {
-              if (qa == 0 && qb == 0 && qd == 0) continue;
-              const int bi = xs[qa], bj = ys[qb], bk = zs[qd];
-              const long long lb = bi + bj * sy + (long long)bk * sz;
-              float sb = s1;
-              if ((bj == 0) && (I->source > 0) && in_window(nx, nz, I->source, bi, bk)) sb = I->sgr_dev_f;
-              float pbv;
-              if ((bj != 0) && (bj != ny - 1)) pbv = p1;
-              else if (bj == 0) pbv = (float)((f.P_atm + f.P_top) - I->Pref[0]);
-              else pbv = (float)(Pnew + ro_g_dy - I->Pref[ny - 1]);
-              s_out[lb] = sb;
-              p_out[lb] = pbv;
-            }
-      }
+      if ((i == 1) || (i == nx - 2) || (j == 1) || (j == ny - 2) || (!PLANAR && ((k == 1) || (k == nz - 2))))
+        write_boundary(f, I, p_out, s_out, i, j, k, pn, snew, prel, rw, rn, mc);
       if (DIAG) {
-        const double S1 = I->S_ref + (double)s1;
-        const double P1rel = rowPrel[ty + 1] + (double)p1;
+        const double S1 = S_ref + (double)snew;
+        const double P1rel = prel + (double)pn;
         const double rw1 = fma(f.aw, P1rel, f.ro0_w), rn1 = fma(f.bn, P1rel, f.ro0_n);
-        acc_w += (double)E.m * rw1 * (1. - S1) * f.vol;
-        acc_n += (double)E.m * rn1 * S1 * f.vol;
+        acc_w += (double)mc * rw1 * (1. - S1) * f.vol;
+        acc_n += (double)mc * rn1 * S1 * f.vol;
         const double r = fmax(fabs(F1) / f.ro0_w, fabs(F2) / f.ro0_n);
         if (!(r <= rmax)) rmax = r;
         if (!finite) nonfinite += 1.;
       }
+    };
+
+    // The sweep: plane pl is derived into ring slot u = (pl - pb) mod 3 while
+    // the centre plane pl - 1 is updated from the slots of pl - 2, pl - 1, pl.
+    float sA0 = 0.f, mA0 = 0.f, sB0 = 0.f, mB0 = 0.f;  // centre plane's s, m of the two cells
+    int u = 0;
+    for (int pl = pb; pl <= ke; pl++) {
+      {  // wait for the plane (bounded)
+        const uint32_t par = (phase >> u) & 1u;
+        unsigned long long tries = 0;
+        while (!mbar_try_wait(&sm.bar[u], par)) {
+          if (++tries > WAIT_LIMIT) {
+            atomicOr(err, 2u);
+            break;
+          }
+        }
+        phase ^= (1u << u);
+      }
+      const RawStage& R = sm.raw[u];
+      float4* __restrict__ D = sm.der[u];
+      float sA1, mA1, sB1, mB1;
+      {
+        Der dA, dB;
+        float rw, rn;
+        sA1 = R.s[rawA];
+        sB1 = R.s[rawB];
+        mA1 = R.m[rawA];
+        mB1 = R.m[rawB];
+        derive(f, c1, rowA.x, rowA.y, R.p[rawA], sA1, UNIK ? f.K0 : R.K[rawA], dA, rw, rn);
+        derive(f, c1, rowB.x, rowB.y, R.p[rawB], sB1, UNIK ? f.K0 : R.K[rawB], dB, rw, rn);
+        D[ownA] = make_float4(dA.p, dA.Mw, dA.Mn, 0.f);
+        D[ownB] = make_float4(dB.p, dB.Mw, dB.Mn, 0.f);
+      }
+      if (halo_slot >= 0) {
+        const float4 rh = sm.rowF[halo_row];
+        Der h;
+        float rw, rn;
+        derive(f, c1, rh.x, rh.y, R.p[halo_raw], R.s[halo_raw], UNIK ? f.K0 : R.K[halo_raw], h, rw, rn);
+        D[halo_slot] = make_float4(h.p, h.Mw, h.Mn, 0.f);
+      }
+      __syncthreads();
+      // Stage u has been read by every thread: refill it three planes ahead.
+      if (tid == 0 && pl + NST <= ke) {
+        fence_proxy_async();
+        const int nxt = pl + NST;
+        mbar_expect_tx(&sm.bar[u], stage_bytes);
+        tma_load_3d(sm.raw[u].p, &I->map_p[parity], x0, j0 - 1, nxt, &sm.bar[u]);
+        tma_load_3d(sm.raw[u].s, &I->map_s[parity], x0, j0 - 1, nxt, &sm.bar[u]);
+        if (!UNIK) tma_load_3d(sm.raw[u].K, &I->map_K, x0, j0 - 1, nxt, &sm.bar[u]);
+        tma_load_3d(sm.raw[u].m, &I->map_m, x0, j0 - 1, nxt, &sm.bar[u]);
+      }
+      if (PLANAR) {
+        if (activeA) update(D, D, D, ownA, rowA, dnA, ty + 1, sA1, mA1, jA, pl);
+        if (activeB) update(D, D, D, ownB, rowB, dnB, ty + 9, sB1, mB1, jB, pl);
+      } else if (pl >= pb + 2) {
+        const int uc = u == 0 ? 2 : u - 1, um = u == 2 ? 0 : u + 1;
+        const float4* __restrict__ Dc = sm.der[uc];
+        const float4* __restrict__ Dm = sm.der[um];
+        if (activeA) update(Dc, Dm, D, ownA, rowA, dnA, ty + 1, sA0, mA0, jA, pl - 1);
+        if (activeB) update(Dc, Dm, D, ownB, rowB, dnB, ty + 9, sB0, mB0, jB, pl - 1);
+      }
+      sA0 = sA1;
+      mA0 = mA1;
+      sB0 = sB1;
+      mB0 = mB1;
+      u = u == 2 ? 0 : u + 1;
     }
     __syncthreads();  // the next item's loads reuse the stages and rows
   }
 
   if (DIAG) {
-    __shared__ double red[NTHREADS / 32][4];
+    double(*red)[4] = sm.red;
     const int lane = tid & 31, wid = tid >> 5;
     const double s0 = warp_sum(acc_w), s1 = warp_sum(acc_n), r = warp_max(rmax), nf = warp_sum(nonfinite);
     if (lane == 0) {
@@ -418,38 +478,65 @@ __global__ void __launch_bounds__(NTHREADS, 3)
   }
 }
 
+// Opts the kernel into its dynamic shared memory, once per device.
+template <bool UNIK, bool DIAG, bool PLANAR>
+cudaError_t prepare_t() {
+  static unsigned long long done = 0;  // bit d: set on device d
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (__atomic_load_n(&done, __ATOMIC_ACQUIRE) & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(step2_fp32c_tma_kernel<UNIK, DIAG, PLANAR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kSmemBytes);
+  if (e == cudaSuccess) __atomic_fetch_or(&done, bit, __ATOMIC_ACQ_REL);
+  return e;
+}
+
+template <bool UNIK, bool DIAG, bool PLANAR>
+cudaError_t launch_t(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
+                     unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
+  cudaError_t e = prepare_t<UNIK, DIAG, PLANAR>();
+  if (e != cudaSuccess) return e;
+  step2_fp32c_tma_kernel<UNIK, DIAG, PLANAR><<<grid, dim3(TX, TY), kSmemBytes, s>>>(f, insts, items, nitems, parity,
+                                                                                   counter, diag_partials);
+  return cudaGetLastError();
+}
+
 template <bool UNIK, bool DIAG>
-int occupancy_t() {
-  int per = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<UNIK, DIAG>, NTHREADS, 0);
-  return per;
+cudaError_t launch_p(bool planar, const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
+                     unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
+  return planar ? launch_t<UNIK, DIAG, true>(f, insts, items, nitems, parity, counter, diag_partials, grid, s)
+                : launch_t<UNIK, DIAG, false>(f, insts, items, nitems, parity, counter, diag_partials, grid, s);
 }
 
 }  // namespace
 
 cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
-                                   bool unik, unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
+                                   bool unik, bool planar, unsigned int* counter, double* diag_partials, int grid,
+                                   cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), s);
   if (e != cudaSuccess) return e;
-  const dim3 blk(TX, TY);
-  if (unik) {
-    if (diag_partials)
-      step2_fp32c_tma_kernel<true, true><<<grid, blk, 0, s>>>(f, insts, items, nitems, parity, counter, diag_partials);
-    else
-      step2_fp32c_tma_kernel<true, false><<<grid, blk, 0, s>>>(f, insts, items, nitems, parity, counter, nullptr);
-  } else {
-    if (diag_partials)
-      step2_fp32c_tma_kernel<false, true><<<grid, blk, 0, s>>>(f, insts, items, nitems, parity, counter, diag_partials);
-    else
-      step2_fp32c_tma_kernel<false, false><<<grid, blk, 0, s>>>(f, insts, items, nitems, parity, counter, nullptr);
-  }
-  return cudaGetLastError();
+  if (unik)
+    return diag_partials ? launch_p<true, true>(planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s)
+                         : launch_p<true, false>(planar, f, insts, items, nitems, parity, counter, nullptr, grid, s);
+  return diag_partials ? launch_p<false, true>(planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s)
+                       : launch_p<false, false>(planar, f, insts, items, nitems, parity, counter, nullptr, grid, s);
 }
 
 int step2_fp32c_tma_grid(int device, bool unik) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  int per = unik ? occupancy_t<true, true>() : occupancy_t<false, true>();
+  int per = 0;
+  if (unik) {
+    prepare_t<true, true, false>();
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<true, true, false>, NTHREADS,
+                                                  kSmemBytes);
+  } else {
+    prepare_t<false, true, false>();
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<false, true, false>, NTHREADS,
+                                                  kSmemBytes);
+  }
   if (per < 1) per = 1;
   return sms * per;
 }
