@@ -276,6 +276,11 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
     const int i = i0 + tx, jA = j0 + ty, jB = jA + 8;
     const bool activeA = (i <= nx - 2) && (jA <= ny - 2);
     const bool activeB = (i <= nx - 2) && (jB <= ny - 2);
+    // Tiles next to an x or y face hold cells whose boundary neighbours this
+    // step writes; elsewhere only the first and last interior planes do.
+    const bool tile_edge = (ti == 0) || (ti == I->tiles_x - 1) || (tj == 0) || (tj == I->tiles_y - 1);
+    const int lA0 = i + jA * sy32;
+    bool bad = false;
     const int kb = PLANAR ? 0 : 1 + zc * I->zchunk;
     const int ke = PLANAR ? 0 : min(kb + I->zchunk, nz - 1);  // last plane loaded
     const int pb = PLANAR ? 0 : kb - 1;                         // first plane loaded
@@ -305,13 +310,15 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
     // the planes below and above it; sc, mc are the cell's saturation
     // deviation and porosity.
     auto update = [&](const float4* __restrict__ D, const float4* __restrict__ Dm, const float4* __restrict__ Dp,
-                      int own, float4 row, float dPs_dn, int wrow, float sc, float mc, int j, int k) {
+                      int own, float4 row, float dPs_dn, int wrow, float sc, float mc, int j, int k, int l,
+                      bool active, bool edge_plane) {
       const float4 c4 = D[own];
       const Der C0{c4.x, c4.y, c4.z};
       float Dw, Dn;
       {
         const float4 a = D[own - 1], b = D[own + 1];
-        const float x1 = (a.x - C0.p) * f.inv_hx2, x2 = (C0.p - b.x) * f.inv_hx2;
+        const float cpx = C0.p * f.inv_hx2;
+        const float x1 = fmaf(a.x, f.inv_hx2, -cpx), x2 = fmaf(-b.x, f.inv_hx2, cpx);
         const bool u1 = x1 > 0.f, u2 = x2 > 0.f;
         const float dxw = x2 * (u2 ? C0.Mw : b.y) - x1 * (u1 ? a.y : C0.Mw);
         const float dxn = x2 * (u2 ? C0.Mn : b.z) - x1 * (u1 ? a.z : C0.Mn);
@@ -329,7 +336,8 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
         if (!PLANAR) {
           const float4 m4 = Dm[own], p4 = Dp[own];
           const Der m1{m4.x, m4.y, m4.z}, p1{p4.x, p4.y, p4.z};
-          const float z1 = (m1.p - C0.p) * f.inv_hz2, z2 = (C0.p - p1.p) * f.inv_hz2;
+          const float cpz = C0.p * f.inv_hz2;
+          const float z1 = fmaf(m1.p, f.inv_hz2, -cpz), z2 = fmaf(-p1.p, f.inv_hz2, cpz);
           const bool v1 = z1 > 0.f, v2 = z2 > 0.f;
           kw.add(z2 * (v2 ? C0.Mw : p1.Mw) - z1 * (v1 ? m1.Mw : C0.Mw));
           kn.add(z2 * (v2 ? C0.Mn : p1.Mn) - z1 * (v1 ? m1.Mn : C0.Mn));
@@ -361,15 +369,19 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
       }
       const float pn = (float)((double)C0.p + dP);
       const float snew = (float)((double)sc + dS);
-      const int l = i + j * sy32 + k * sz32;
-      p_out[l] = pn;
-      s_out[l] = snew;
+      // Cells beyond the grid's interior (partial tiles) compute on the
+      // window's fill values and store nothing.
+      if (active) {
+        p_out[l] = pn;
+        s_out[l] = snew;
+      }
       const bool finite = isfinite(pn) && isfinite(snew);
-      if (!finite) atomicOr(err, 1u);
-
-      if ((i == 1) || (i == nx - 2) || (j == 1) || (j == ny - 2) || (!PLANAR && ((k == 1) || (k == nz - 2))))
-        write_boundary(f, I, p_out, s_out, i, j, k, pn, snew, prel, rw, rn, mc);
-      if (DIAG) {
+      bad |= active && !finite;
+      if (edge_plane) {
+        if (active && ((i == 1) || (i == nx - 2) || (j == 1) || (j == ny - 2) || (!PLANAR && ((k == 1) || (k == nz - 2)))))
+          write_boundary(f, I, p_out, s_out, i, j, k, pn, snew, prel, rw, rn, mc);
+      }
+      if (DIAG && active) {
         const double S1 = S_ref + (double)snew;
         const double P1rel = prel + (double)pn;
         const double rw1 = fma(f.aw, P1rel, f.ro0_w), rn1 = fma(f.bn, P1rel, f.ro0_n);
@@ -431,14 +443,18 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
         tma_load_3d(sm.raw[u].m, &I->map_m, x0, j0 - 1, nxt, &sm.bar[u]);
       }
       if (PLANAR) {
-        if (activeA) update(D, D, D, ownA, rowA, dnA, ty + 1, sA1, mA1, jA, pl);
-        if (activeB) update(D, D, D, ownB, rowB, dnB, ty + 9, sB1, mB1, jB, pl);
+        const int lA = lA0, lB = lA0 + 8 * sy32;
+        update(D, D, D, ownA, rowA, dnA, ty + 1, sA1, mA1, jA, pl, lA, activeA, tile_edge);
+        update(D, D, D, ownB, rowB, dnB, ty + 9, sB1, mB1, jB, pl, lB, activeB, tile_edge);
       } else if (pl >= pb + 2) {
+        const int k = pl - 1;
         const int uc = u == 0 ? 2 : u - 1, um = u == 2 ? 0 : u + 1;
         const float4* __restrict__ Dc = sm.der[uc];
         const float4* __restrict__ Dm = sm.der[um];
-        if (activeA) update(Dc, Dm, D, ownA, rowA, dnA, ty + 1, sA0, mA0, jA, pl - 1);
-        if (activeB) update(Dc, Dm, D, ownB, rowB, dnB, ty + 9, sB0, mB0, jB, pl - 1);
+        const int lA = lA0 + k * sz32, lB = lA + 8 * sy32;
+        const bool edge_plane = tile_edge || (k == 1) || (k == nz - 2);
+        update(Dc, Dm, D, ownA, rowA, dnA, ty + 1, sA0, mA0, jA, k, lA, activeA, edge_plane);
+        update(Dc, Dm, D, ownB, rowB, dnB, ty + 9, sB0, mB0, jB, k, lB, activeB, edge_plane);
       }
       sA0 = sA1;
       mA0 = mA1;
@@ -446,6 +462,7 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
       mB0 = mB1;
       u = u == 2 ? 0 : u + 1;
     }
+    if (__any_sync(0xffffffffu, bad) && (tid & 31) == 0) atomicOr(err, 1u);
     __syncthreads();  // the next item's loads reuse the stages and rows
   }
 
