@@ -69,6 +69,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-three-phase", action="store_true")
     return ap.parse_args()
 
 
@@ -328,6 +329,43 @@ def precision_check(w, dev, steps):
     return r
 
 
+def three_phase_leg(dev, steps: int = 200, warmup: int = 5) -> dict:
+    """Three-phase FP64 step on the config-2 workload (192x192x96, gravity on
+    z, lognormal K, 3x3 NAPL source): cell-steps/s over `steps` steps with
+    the state in HBM (CUDA events), and the kernel's algorithmic HBM bytes
+    (64 B/cell-step: P_w, S_w, S_n, m, K read, P_w, S_w, S_n written)."""
+    import torch
+
+    from capaz_b200 import Simulation
+    from capaz_b200.configs import config2
+    w = config2()
+    p = w.params
+    with Simulation(p, device=dev) as sim:
+        sim.set_field("m", w.m)
+        sim.set_field("K", w.K)
+        sim.init_state()
+        st = torch.cuda.Stream(device=dev)
+        sim.step(warmup, st.cuda_stream)
+        torch.cuda.synchronize()
+        l0 = sim.launch_count
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        sim.step(steps, st.cuda_stream)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        launches = sim.launch_count - l0
+        S = sim.get_field("S_n")
+    peak, _ = measured_peaks()
+    gbs = 64 * p.ncell / (ms * 1e-3) / 1e9
+    return {"workload": f"cfg2 three-phase {w.notes['workload_grid']} (reference axes {w.notes['ref_grid']}), "
+                        f"FP64, dt {p.dt:.3g} s, per-cell K, 3x3 top source",
+            "value": p.ncell / (ms * 1e-3), "unit": "cell-steps/s", "ms_per_step": ms, "steps": steps,
+            "launches": launches, "algorithmic_bytes_per_cell": 64, "achieved_gbs": gbs, "hbm_frac": gbs / peak,
+            "finite": bool(np.isfinite(S).all()), "kernel": "step3_fp64_kernel (FP64-bound: 13 pow per cell, "
+                                                                  "7 Newton iterations with Gauss-Jordan)"}
+
+
 def adjoint_leg(dev) -> dict:
     """Differentiation form on the config-4 inverse problem (128x128x64,
     FP64, 500 steps, checkpoints every 50): time of one forward solve vs. one
@@ -448,6 +486,14 @@ def run_capaz(args) -> None:
     if not args.no_precision and "fp32c" in forms and "fp64" in forms:
         prec = precision_check(w, dev, w.steps)
 
+    # ---- three-phase form (config 2) -----------------------------------------
+    three = None
+    if not args.no_three_phase and ws == 1:
+        try:
+            three = three_phase_leg(dev)
+        except Exception as e:  # reported, never fatal to the headline line
+            three = {"failed": str(e)}
+
     # ---- differentiation form (config 4) ------------------------------------
     adj = None
     if not args.no_adjoint and ws == 1:
@@ -541,6 +587,7 @@ def run_capaz(args) -> None:
                                       if "fp32c" in forms_out and "fp64" in forms_out else None),
             "precision": prec,
             "adjoint": adj,
+            "three_phase": three,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": t["launches"],
         }
         print(json.dumps(line), flush=True)

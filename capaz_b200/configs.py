@@ -199,3 +199,47 @@ def observe(params: Params, m: np.ndarray, K: np.ndarray, obs: np.ndarray, obs_e
             s.step(obs_every)
             out.append(1.0 - s.get_field("S_n").reshape(-1)[obs])
     return np.array(out)
+
+
+def three_phase_params(nx_ref: int, ny_ref: int, nz_ref: int, percell_k: bool = True) -> Params:
+    """Three-phase fluids (config 2): water / NAPL / gas densities 1000 / 850 /
+    1.2 (ideal gas, rho_g = rho_0g P / P_atm), viscosities 1e-3 / 3e-3 /
+    1.8e-5, residual saturations 0.1 / 0.05 / 0.02, the reference CPU
+    relative permeabilities with A = 2 and no capillarity (three-phase.cpp:
+    11-186), 7 Newton iterations; initial S_w = 0.2, S_n = 0.3; NAPL enters
+    through a 3x3 window of the top face at S_n = 0.7 (S_w = 0.2)."""
+    from .simulation import default_params
+    p = default_params()
+    p.nx, p.ny, p.nz = nx_ref, ny_ref, nz_ref
+    p.phases = 3
+    p.form = native.FORM_FP64
+    p.hx = p.hy = p.hz = 1.0
+    p.ro0_w, p.ro0_n, p.ro0_g = 1000.0, 850.0, 1.2
+    p.mu_w, p.mu_n, p.mu_g = 1e-3, 3e-3, 1.8e-5
+    p.beta_w = p.beta_n = 1e-9
+    p.lambda_ = 2.0
+    p.S_wr, p.S_nr, p.S_gr = 0.1, 0.05, 0.02
+    p.S_w_init, p.S_n_init = 0.2, 0.3
+    p.S_w_gr, p.S_n_gr = 0.2, 0.7
+    p.source = 1                          # 3x3 window with CAPAZ_FLAG_SOURCE_WINDOW
+    p.P_d = 0.0
+    p.g_const = 9.81
+    p.P_atm = 1e5
+    p.K0 = 1e-12
+    p.porosity = 0.25
+    p.newton_iterations = 7
+    p.flags = native.FLAG_SOURCE_WINDOW | (native.FLAG_PERCELL_K if percell_k else 0)
+    return p
+
+
+def config2(seed: int = 2, grid=(192, 192, 96), steps: int = 500) -> Workload:
+    """192x192x96 (gravity on z) three-phase, 500 steps, FP64, lognormal K
+    (sigma 1, ell 8) and its porosity field, 3x3 NAPL source on the top face."""
+    Nx, Ny, Nz = grid
+    nx, ny, nz = Nx, Nz, Ny
+    p = three_phase_params(nx, ny, nz)
+    m, K = heterogeneous_fields((nz, ny, nx), 1.0, 8.0, seed)
+    p.dt = stable_dt(p, m, K)
+    return Workload(f"cfg2 three-phase {Nx}x{Ny}x{Nz} fp64", p, steps, m, K,
+                    {"workload_grid": list(grid), "ref_grid": [nx, ny, nz], "dt": p.dt, "sigma": 1.0, "ell": 8.0,
+                     "seed": seed})

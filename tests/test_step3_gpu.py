@@ -93,3 +93,25 @@ def test_gpu3_percell_k_window_source_and_diag():
         assert rel_err(out[k], ref[k]) <= TOL, k
     for i in range(3):
         assert abs(out["diag"]["mass"][i] - ref["diag"]["mass"][i]) <= 1e-12 * abs(ref["diag"]["mass"][i])
+
+
+def test_gpu3_config2_workload_shape():
+    """The config-2 setup (per-cell K and porosity fields, 3x3 NAPL window,
+    the workload's stable dt) on a reduced grid, 30 steps from
+    capaz_init_state's state, against the oracle."""
+    from capaz_b200.configs import config2
+    w = config2(grid=(40, 40, 20))
+    p = w.params
+    st = O.init(p, w.m)
+    state = {k: st[k] for k in STATE}
+    ref = O.step(p, state, 30, w.m, w.K)
+    with Simulation(p) as s:
+        s.set_field("m", w.m)
+        s.set_field("K", w.K)
+        s.init_state()
+        for k in STATE:
+            assert np.array_equal(s.get_field(k), st[k]), k
+        s.step(30)
+        out = {k: s.get_field(k) for k in STATE}
+    for k in STATE:
+        assert rel_err(out[k], ref[k]) <= TOL, k
