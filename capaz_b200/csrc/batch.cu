@@ -22,6 +22,8 @@ struct capaz_batch {
   Inst64* d_inst64 = nullptr;
   int4* d_items = nullptr;
   int nitems = 0;
+  int2* d_bitems = nullptr;  // boundary-kernel blocks (precision form)
+  int nbitems = 0;
   size_t items_cap = 0;
   unsigned int* counter = nullptr;
   int zchunk = 16;
@@ -125,6 +127,17 @@ int build(capaz_batch* b) {
     b->items_cap = items.size();
   }
   BTRY(b, cudaMemcpy(b->d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
+  if (b->fp32 && !b->d_bitems) {
+    std::vector<int2> bitems;
+    for (int q = 0; q < n; q++) {
+      const capaz_params& pq = b->ctx[q]->p;
+      const int nb = boundary_cells(pq.nx, pq.ny, pq.nz);
+      for (int f0 = 0; f0 < nb; f0 += BOUND_BLOCK) bitems.push_back(make_int2(q, f0));
+    }
+    b->nbitems = (int)bitems.size();
+    BTRY(b, cudaMalloc(&b->d_bitems, sizeof(int2) * bitems.size()));
+    BTRY(b, cudaMemcpy(b->d_bitems, bitems.data(), sizeof(int2) * bitems.size(), cudaMemcpyHostToDevice));
+  }
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
   const int per = b->ctas_per_sm > 0 ? std::min(b->ctas_per_sm, occupancy(b)) : occupancy(b);
@@ -152,10 +165,14 @@ bool stale(const capaz_batch* b) {
   return false;
 }
 
+// Kernels one step launches: the precision form's sweep is followed by its
+// boundary kernel.
+int kernels_per_step(const capaz_batch* b) { return b->fp32 ? 2 : 1; }
+
 cudaError_t launch_one(capaz_batch* b, int parity, cudaStream_t s) {
   if (b->fp32)
-    return launch_step2_fp32c_tma(b->phys, b->d_instT, b->d_items, b->nitems, parity, b->unik, b->planar,
-                                  b->counter, nullptr, b->grid, s);
+    return launch_step2_fp32c_tma(b->phys, b->d_instT, b->d_items, b->nitems, b->d_bitems, b->nbitems, parity,
+                                  b->unik, b->planar, b->counter, nullptr, b->grid, s);
   return launch_step2_fp64_batch(b->d_inst64, b->d_items, b->nitems, parity, b->unik, b->pd0, b->counter, b->grid, s);
 }
 
@@ -203,21 +220,21 @@ int run_steps(capaz_batch* b, int nsteps, cudaStream_t s, bool use_graph) {
     // The pair graph starts at parity 0: align with one plain launch first.
     if (cur == 1) {
       BTRY(b, launch_one(b, 1, s));
-      b->launches++;
+      b->launches += kernels_per_step(b);
       advance(b, 1);
       done = 1;
       cur = 0;
     }
     while (nsteps - done >= 2) {
       BTRY(b, cudaGraphLaunch(b->pair, s));
-      b->launches += 2;
+      b->launches += 2 * kernels_per_step(b);
       advance(b, 2);
       done += 2;
     }
   }
   while (done < nsteps) {
     BTRY(b, launch_one(b, b->ctx[0]->cur, s));
-    b->launches++;
+    b->launches += kernels_per_step(b);
     advance(b, 1);
     done++;
   }
@@ -287,6 +304,7 @@ int capaz_batch_destroy(capaz_batch* b) {
   if (b->d_instT) cudaFree(b->d_instT);
   if (b->d_inst64) cudaFree(b->d_inst64);
   if (b->d_items) cudaFree(b->d_items);
+  if (b->d_bitems) cudaFree(b->d_bitems);
   if (b->counter) cudaFree(b->counter);
   for (auto* x : b->ctx) capaz_destroy(x);
   delete b;

@@ -603,6 +603,7 @@ void capaz_ctx::release() {
   if (stage) cudaFree(stage);
   if (tma_inst) cudaFree(tma_inst);
   if (tma_items) cudaFree(tma_items);
+  if (tma_bitems) cudaFree(tma_bitems);
   if (tma_counter) cudaFree(tma_counter);
   if (first_bad) cudaFree(first_bad);
   if (sum_parts) cudaFree(sum_parts);

@@ -37,6 +37,8 @@ struct capaz_ctx {
   capaz::InstT* tma_inst = nullptr;  // device descriptor
   int4* tma_items = nullptr;
   int tma_nitems = 0;
+  int2* tma_bitems = nullptr;  // boundary-kernel blocks
+  int tma_nbitems = 0;
   unsigned int* tma_counter = nullptr;
   double tma_dt = 0., tma_S_ref = 0.;  // values baked into the descriptor
   float4* rowF = nullptr;              // per-row tables (precision form)

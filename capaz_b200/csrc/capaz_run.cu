@@ -54,9 +54,9 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
     }
     for (int t = 0; t < nsteps; t++) {
       const bool last = t == nsteps - 1;
-      e = launch_step2_fp32c_tma(f, tma_inst, tma_items, tma_nitems, cur, unik, p.nz == 1, tma_counter,
-                                 (diag && last) ? diag_partials : nullptr, tma_grid, s);
-      launches++;
+      e = launch_step2_fp32c_tma(f, tma_inst, tma_items, tma_nitems, tma_bitems, tma_nbitems, cur, unik, p.nz == 1,
+                                 tma_counter, (diag && last) ? diag_partials : nullptr, tma_grid, s);
+      launches += 2;
       if (e != cudaSuccess) return fail_cuda(e, "step2_fp32c_tma launch");
       cur ^= 1;
       steps_done++;
@@ -223,6 +223,7 @@ int capaz_ctx::tma_prepare() {
   h.c1_f = (float)(1. - p.S_wr - S_ref);
   h.dt_f = (float)p.dt;
   h.sgr_dev_f = (float)(p.S_n_gr - S_ref);
+  h.nbound = boundary_cells(p.nx, p.ny, p.nz);
   h.S_ref = S_ref;
   h.dt = p.dt;
   h.rowF = rowF;
@@ -278,6 +279,13 @@ int capaz_ctx::tma_prepare() {
     e = cudaMemcpy(tma_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy(items)");
     tma_grid = std::min(tma_nitems, step2_fp32c_tma_grid(device, !(p.flags & CAPAZ_FLAG_PERCELL_K)));
+    std::vector<int2> bitems;
+    for (int q = 0; q < h.nbound; q += BOUND_BLOCK) bitems.push_back(make_int2(0, q));
+    tma_nbitems = (int)bitems.size();
+    e = cudaMalloc(&tma_bitems, sizeof(int2) * bitems.size());
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(items)");
+    e = cudaMemcpy(tma_bitems, bitems.data(), sizeof(int2) * bitems.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy(items)");
   }
   tma_dt = p.dt;
   tma_S_ref = S_ref;

@@ -31,6 +31,8 @@
 // terms are Kahan-summed.  d(rho S) = -dt/m * div goes to FP64, where one
 // Newton step with the Jacobian at the stored state solves the bilinear
 // system for (dP, dS).
+// Boundary cells are written by a second, small kernel over the boundary
+// shell after the sweep, which keeps the sweep free of per-cell face tests.
 // Waits on mbarriers are bounded; a wait that runs out sets bit 1 of the
 // error flag and the CTA carries on, so the kernel always finishes.
 #include <cuda.h>
@@ -42,7 +44,9 @@
 namespace capaz {
 namespace {
 
-constexpr int TYT = 2 * TY;        // tile height: each thread row owns two cell rows (ty, ty + 8)
+constexpr int TYK = TMA_TY;        // thread rows of a CTA
+constexpr int NTK = TX * TYK;      // threads of a CTA
+constexpr int TYT = TMA_TILE_Y;    // tile height: each thread row owns two cell rows (ty, ty + TYK)
 constexpr int WX = TX + 2;         // derived-plane window: tile plus a one-cell halo
 constexpr int WY = TYT + 2;
 constexpr int WCELLS = WX * WY;
@@ -50,9 +54,9 @@ constexpr int NHALO = 2 * TX + 2 * TYT;  // halo cells derived by threads 0..NHA
 constexpr int BXW = 36;            // TMA box width (floats): 144 bytes, a multiple of 16
 constexpr int BYW = WY;            // TMA box height
 constexpr int NST = 3;             // planes in flight (raw stages and derived slots)
-constexpr int RAWN = 672;          // floats reserved per array per stage (2688 B, 128-B multiple)
+constexpr int RAWN = (BXW * BYW + 31) / 32 * 32;  // floats reserved per array per stage (128-B multiple)
 static_assert(BXW * BYW <= RAWN, "raw stage too small");
-static_assert(NHALO <= NTHREADS, "halo cells exceed the block");
+static_assert(NHALO <= NTK && 2 * TYT <= 32, "halo cells exceed the block");
 constexpr unsigned long long WAIT_LIMIT = 1ull << 22;  // try_wait polls before giving up
 
 struct alignas(128) RawStage {
@@ -156,49 +160,6 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-// Boundary cells whose basic coordinate (cpu.cpp:107-141) is interior cell
-// (i, j, k), written from its new state and its start-of-step densities
-// (Border_S / Border_P, two-phase.cpp:59-111).  Out of line: only cells next
-// to a face take it.
-__device__ __forceinline__ void write_boundary(const PhysF& f, const InstT* __restrict__ I, float* __restrict__ p_out,
-                                            float* __restrict__ s_out, int i, int j, int k, float pn, float snew,
-                                            double prel, double rw, double rn, float mc) {
-  const int nx = I->nx, ny = I->ny, nz = I->nz;
-  const bool planar = nz == 1;
-  const long long sy = I->sy, sz = I->sz;
-  const double Snew = I->S_ref + (double)snew;
-  const double Pnew = (prel + f.P_atm) + (double)pn;
-  const double ro_g_dy = (rn * Snew + rw * (1 - Snew)) * (double)mc * f.g * f.hy;
-  const int xo = (i == 1) ? 0 : ((i == nx - 2) ? nx - 1 : -1);
-  const int xo2 = (i == 1 && i == nx - 2) ? nx - 1 : -1;
-  const int yo = (j == 1) ? 0 : ((j == ny - 2) ? ny - 1 : -1);
-  const int yo2 = (j == 1 && j == ny - 2) ? ny - 1 : -1;
-  const int zo = planar ? -1 : ((k == 1) ? 0 : ((k == nz - 2) ? nz - 1 : -1));
-  const int zo2 = (!planar && k == 1 && k == nz - 2) ? nz - 1 : -1;
-  for (int qa = 0; qa < 3; qa++) {
-    const int bi = qa == 0 ? i : (qa == 1 ? xo : xo2);
-    if (bi < 0) continue;
-    for (int qb = 0; qb < 3; qb++) {
-      const int bj = qb == 0 ? j : (qb == 1 ? yo : yo2);
-      if (bj < 0) continue;
-      for (int qd = 0; qd < 3; qd++) {
-        const int bk = qd == 0 ? k : (qd == 1 ? zo : zo2);
-        if (bk < 0) continue;
-        if (qa == 0 && qb == 0 && qd == 0) continue;
-        const long long lb = bi + bj * sy + (long long)bk * sz;
-        float sb = snew;
-        if ((bj == 0) && (I->source > 0) && in_window(nx, nz, I->source, bi, bk)) sb = I->sgr_dev_f;
-        float pbv;
-        if ((bj != 0) && (bj != ny - 1)) pbv = pn;
-        else if (bj == 0) pbv = (float)((f.P_atm + f.P_top) - I->Pref[0]);
-        else pbv = (float)(Pnew + ro_g_dy - I->Pref[ny - 1]);
-        s_out[lb] = sb;
-        p_out[lb] = pbv;
-      }
-    }
-  }
-}
-
 // Shared memory of one CTA (dynamic, 62 KB: three CTAs per SM).
 struct Smem {
   RawStage raw[NST];
@@ -207,7 +168,7 @@ struct Smem {
   float4 rowF[WY];          // (rho_w, rho_n at the row's P_ref, dP_ref/hy^2 to the next row, -)
   double rowPrel[WY];       // P_ref - P_atm
   double rowPref[WY];
-  double red[NTHREADS / 32][4];  // diagnostics reduction
+  double red[NTK / 32][4];  // diagnostics reduction
   int w_sh;
 };
 constexpr size_t kSmemBytes = sizeof(Smem);
@@ -216,7 +177,7 @@ constexpr size_t kSmemBytes = sizeof(Smem);
 #define CAPAZ_TMA_MIN_BLOCKS 3
 #endif
 template <bool UNIK, bool DIAG, bool PLANAR>
-__global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
+__global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
     step2_fp32c_tma_kernel(const __grid_constant__ PhysF f, const InstT* __restrict__ insts,
                            const int4* __restrict__ items, int nitems, int parity, unsigned int* __restrict__ counter,
                            double* __restrict__ diag_partials) {
@@ -232,9 +193,9 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
   __syncthreads();
   uint32_t phase = 0;  // bit q: parity of the next completion of stage q
 
-  // The thread's two cells are tile rows ty and ty + 8 (window rows +1).
-  const int ownA = (ty + 1) * WX + (tx + 1), ownB = ownA + 8 * WX;
-  const int rawA = (ty + 1) * BXW + (tx + 1), rawB = rawA + 8 * BXW;
+  // The thread's two cells are tile rows ty and ty + TYK (window rows +1).
+  const int ownA = (ty + 1) * WX + (tx + 1), ownB = ownA + TYK * WX;
+  const int rawA = (ty + 1) * BXW + (tx + 1), rawB = rawA + TYK * BXW;
   // Halo cells of the 7-point stencil (the window's corners are never read):
   // warp 0 the row above the tile, warp 1 the row below, warp 2 the columns
   // left (lanes 0-15) and right (lanes 16-31).
@@ -273,12 +234,9 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
     const int ti = tile % I->tiles_x, tj = tile / I->tiles_x;
     const int i0 = 1 + ti * TX, j0 = 1 + tj * TYT;
     const int x0 = i0 - 1;  // == 32 * ti: 128-byte aligned TMA start
-    const int i = i0 + tx, jA = j0 + ty, jB = jA + 8;
+    const int i = i0 + tx, jA = j0 + ty, jB = jA + TYK;
     const bool activeA = (i <= nx - 2) && (jA <= ny - 2);
     const bool activeB = (i <= nx - 2) && (jB <= ny - 2);
-    // Tiles next to an x or y face hold cells whose boundary neighbours this
-    // step writes; elsewhere only the first and last interior planes do.
-    const bool tile_edge = (ti == 0) || (ti == I->tiles_x - 1) || (tj == 0) || (tj == I->tiles_y - 1);
     const int lA0 = i + jA * sy32;
     bool bad = false;
     const int kb = PLANAR ? 0 : 1 + zc * I->zchunk;
@@ -303,15 +261,14 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
       }
     }
     __syncthreads();
-    const float4 rowA = sm.rowF[ty + 1], rowB = sm.rowF[ty + 9];
-    const float dnA = sm.rowF[ty].z, dnB = sm.rowF[ty + 8].z;
+    const float4 rowA = sm.rowF[ty + 1], rowB = sm.rowF[ty + TYK + 1];
+    const float dnA = sm.rowF[ty].z, dnB = sm.rowF[ty + TYK].z;
 
     // The centre-plane update of one cell: D holds the centre plane, Dm / Dp
     // the planes below and above it; sc, mc are the cell's saturation
     // deviation and porosity.
     auto update = [&](const float4* __restrict__ D, const float4* __restrict__ Dm, const float4* __restrict__ Dp,
-                      int own, float4 row, float dPs_dn, int wrow, float sc, float mc, int j, int k, int l,
-                      bool active, bool edge_plane) {
+                      int own, float4 row, float dPs_dn, int wrow, float sc, float mc, int l, bool active) {
       const float4 c4 = D[own];
       const Der C0{c4.x, c4.y, c4.z};
       float Dw, Dn;
@@ -377,10 +334,6 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
       }
       const bool finite = isfinite(pn) && isfinite(snew);
       bad |= active && !finite;
-      if (edge_plane) {
-        if (active && ((i == 1) || (i == nx - 2) || (j == 1) || (j == ny - 2) || (!PLANAR && ((k == 1) || (k == nz - 2)))))
-          write_boundary(f, I, p_out, s_out, i, j, k, pn, snew, prel, rw, rn, mc);
-      }
       if (DIAG && active) {
         const double S1 = S_ref + (double)snew;
         const double P1rel = prel + (double)pn;
@@ -443,18 +396,17 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
         tma_load_3d(sm.raw[u].m, &I->map_m, x0, j0 - 1, nxt, &sm.bar[u]);
       }
       if (PLANAR) {
-        const int lA = lA0, lB = lA0 + 8 * sy32;
-        update(D, D, D, ownA, rowA, dnA, ty + 1, sA1, mA1, jA, pl, lA, activeA, tile_edge);
-        update(D, D, D, ownB, rowB, dnB, ty + 9, sB1, mB1, jB, pl, lB, activeB, tile_edge);
+        const int lA = lA0, lB = lA0 + TYK * sy32;
+        update(D, D, D, ownA, rowA, dnA, ty + 1, sA1, mA1, lA, activeA);
+        update(D, D, D, ownB, rowB, dnB, ty + TYK + 1, sB1, mB1, lB, activeB);
       } else if (pl >= pb + 2) {
         const int k = pl - 1;
         const int uc = u == 0 ? 2 : u - 1, um = u == 2 ? 0 : u + 1;
         const float4* __restrict__ Dc = sm.der[uc];
         const float4* __restrict__ Dm = sm.der[um];
-        const int lA = lA0 + k * sz32, lB = lA + 8 * sy32;
-        const bool edge_plane = tile_edge || (k == 1) || (k == nz - 2);
-        update(Dc, Dm, D, ownA, rowA, dnA, ty + 1, sA0, mA0, jA, k, lA, activeA, edge_plane);
-        update(Dc, Dm, D, ownB, rowB, dnB, ty + 9, sB0, mB0, jB, k, lB, activeB, edge_plane);
+        const int lA = lA0 + k * sz32, lB = lA + TYK * sy32;
+        update(Dc, Dm, D, ownA, rowA, dnA, ty + 1, sA0, mA0, lA, activeA);
+        update(Dc, Dm, D, ownB, rowB, dnB, ty + TYK + 1, sB0, mB0, lB, activeB);
       }
       sA0 = sA1;
       mA0 = mA1;
@@ -479,7 +431,7 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
     __syncthreads();
     if (tid == 0) {
       double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-      for (int q = 0; q < NTHREADS / 32; q++) {
+      for (int q = 0; q < NTK / 32; q++) {
         t0 += red[q][0];
         t1 += red[q][1];
         t2 = fmax(t2, red[q][2]);
@@ -493,6 +445,78 @@ __global__ void __launch_bounds__(NTHREADS, CAPAZ_TMA_MIN_BLOCKS)
       out[4] = t3;
     }
   }
+}
+
+// Boundary cells after the sweep (boundary_conditions, two-phase.cpp:59-111):
+// each takes the new state of its basic-coordinate cell (cpu.cpp:107-141),
+// an interior cell; the top row holds P_atm (+ the top offset) and, inside
+// the injection window, S_n_gr; the bottom row adds the weight
+// (rho_n S_n + rho_w (1 - S_n)) m g hy of the basic cell with its new S_n and
+// start-of-step densities (Border_P, main.cpp:255-267).  One thread per
+// boundary cell; items are (instance, first cell) blocks of BOUND_BLOCK.
+__global__ void __launch_bounds__(BOUND_BLOCK) boundary_fp32c_kernel(const __grid_constant__ PhysF f,
+                                                                     const InstT* __restrict__ insts,
+                                                                     const int2* __restrict__ bitems, int parity) {
+  const int2 it = bitems[blockIdx.x];
+  const InstT* __restrict__ I = insts + it.x;
+  const int q0 = it.y + (int)threadIdx.x;
+  if (q0 >= I->nbound) return;
+  const int nx = I->nx, ny = I->ny, nz = I->nz;
+  int q = q0, i, j, k;
+  if (nz == 1) {
+    k = 0;
+    if (q < 2 * nx) {
+      j = q < nx ? 0 : ny - 1;
+      i = q % nx;
+    } else {
+      q -= 2 * nx;
+      i = q < ny - 2 ? 0 : nx - 1;
+      j = 1 + q % (ny - 2);
+    }
+  } else {
+    const int A = nx * nz, B = (ny - 2) * nz, C = (nx - 2) * (ny - 2);
+    if (q < 2 * A) {
+      j = q < A ? 0 : ny - 1;
+      q %= A;
+      i = q % nx;
+      k = q / nx;
+    } else if ((q -= 2 * A) < 2 * B) {
+      i = q < B ? 0 : nx - 1;
+      q %= B;
+      j = 1 + q % (ny - 2);
+      k = q / (ny - 2);
+    } else {
+      q -= 2 * B;
+      k = q < C ? 0 : nz - 1;
+      q %= C;
+      i = 1 + q % (nx - 2);
+      j = 1 + q / (nx - 2);
+    }
+  }
+  const int i1 = min(max(i, 1), nx - 2), j1 = min(max(j, 1), ny - 2);
+  const int k1 = nz == 1 ? 0 : min(max(k, 1), nz - 2);
+  const long long sy = I->sy, sz = I->sz;
+  const long long lb = i + j * sy + (long long)k * sz, l1 = i1 + j1 * sy + (long long)k1 * sz;
+  const Step2FArgs& A = I->a[parity];
+  const float s1 = A.s_out[l1];
+  float sb = s1;
+  if ((j == 0) && (I->source > 0) && in_window(nx, nz, I->source, i, k)) sb = I->sgr_dev_f;
+  float pb;
+  if ((j != 0) && (j != ny - 1)) {
+    pb = A.p_out[l1];
+  } else if (j == 0) {
+    pb = (float)((f.P_atm + f.P_top) - I->Pref[0]);
+  } else {
+    const double prel = I->Pref[j1] - f.P_atm;
+    const double pr = prel + (double)A.p_in[l1];  // start-of-step pressure of the basic cell
+    const double rw = fma(f.aw, pr, f.ro0_w), rn = fma(f.bn, pr, f.ro0_n);
+    const double Snew = I->S_ref + (double)s1;
+    const double Pnew = (prel + f.P_atm) + (double)A.p_out[l1];
+    const double ro_g_dy = (rn * Snew + rw * (1 - Snew)) * (double)A.m[l1] * f.g * f.hy;
+    pb = (float)(Pnew + ro_g_dy - I->Pref[ny - 1]);
+  }
+  A.s_out[lb] = sb;
+  A.p_out[lb] = pb;
 }
 
 // Opts the kernel into its dynamic shared memory, once per device.
@@ -515,7 +539,7 @@ cudaError_t launch_t(const PhysF& f, const InstT* insts, const int4* items, int 
                      unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
   cudaError_t e = prepare_t<UNIK, DIAG, PLANAR>();
   if (e != cudaSuccess) return e;
-  step2_fp32c_tma_kernel<UNIK, DIAG, PLANAR><<<grid, dim3(TX, TY), kSmemBytes, s>>>(f, insts, items, nitems, parity,
+  step2_fp32c_tma_kernel<UNIK, DIAG, PLANAR><<<grid, dim3(TX, TYK), kSmemBytes, s>>>(f, insts, items, nitems, parity,
                                                                                    counter, diag_partials);
   return cudaGetLastError();
 }
@@ -529,16 +553,20 @@ cudaError_t launch_p(bool planar, const PhysF& f, const InstT* insts, const int4
 
 }  // namespace
 
-cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
-                                   bool unik, bool planar, unsigned int* counter, double* diag_partials, int grid,
-                                   cudaStream_t s) {
+cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems,
+                                   const int2* bitems, int nbitems, int parity, bool unik, bool planar,
+                                   unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), s);
   if (e != cudaSuccess) return e;
   if (unik)
-    return diag_partials ? launch_p<true, true>(planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s)
-                         : launch_p<true, false>(planar, f, insts, items, nitems, parity, counter, nullptr, grid, s);
-  return diag_partials ? launch_p<false, true>(planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s)
-                       : launch_p<false, false>(planar, f, insts, items, nitems, parity, counter, nullptr, grid, s);
+    e = diag_partials ? launch_p<true, true>(planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s)
+                      : launch_p<true, false>(planar, f, insts, items, nitems, parity, counter, nullptr, grid, s);
+  else
+    e = diag_partials ? launch_p<false, true>(planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s)
+                      : launch_p<false, false>(planar, f, insts, items, nitems, parity, counter, nullptr, grid, s);
+  if (e != cudaSuccess) return e;
+  boundary_fp32c_kernel<<<nbitems, BOUND_BLOCK, 0, s>>>(f, insts, bitems, parity);
+  return cudaGetLastError();
 }
 
 int step2_fp32c_tma_grid(int device, bool unik) {
@@ -547,11 +575,11 @@ int step2_fp32c_tma_grid(int device, bool unik) {
   int per = 0;
   if (unik) {
     prepare_t<true, true, false>();
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<true, true, false>, NTHREADS,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<true, true, false>, NTK,
                                                   kSmemBytes);
   } else {
     prepare_t<false, true, false>();
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<false, true, false>, NTHREADS,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<false, true, false>, NTK,
                                                   kSmemBytes);
   }
   if (per < 1) per = 1;
