@@ -39,6 +39,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "capaz_internal.h"
 
 namespace capaz {
@@ -348,9 +350,10 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
 
     // The sweep: plane pl is derived into ring slot u = (pl - pb) mod 3 while
     // the centre plane pl - 1 is updated from the slots of pl - 2, pl - 1, pl.
+    // Unrolled by three so that every slot index is a compile-time constant.
     float sA0 = 0.f, mA0 = 0.f, sB0 = 0.f, mB0 = 0.f;  // centre plane's s, m of the two cells
-    int u = 0;
-    for (int pl = pb; pl <= ke; pl++) {
+    auto plane = [&](auto U, int pl) {
+      constexpr int u = decltype(U)::value;
       {  // wait for the plane (bounded)
         const uint32_t par = (phase >> u) & 1u;
         unsigned long long tries = 0;
@@ -400,19 +403,23 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
         update(D, D, D, ownA, rowA, dnA, ty + 1, sA1, mA1, lA, activeA);
         update(D, D, D, ownB, rowB, dnB, ty + TYK + 1, sB1, mB1, lB, activeB);
       } else if (pl >= pb + 2) {
+        constexpr int uc = (u + 2) % NST, um = (u + 1) % NST;
         const int k = pl - 1;
-        const int uc = u == 0 ? 2 : u - 1, um = u == 2 ? 0 : u + 1;
-        const float4* __restrict__ Dc = sm.der[uc];
-        const float4* __restrict__ Dm = sm.der[um];
         const int lA = lA0 + k * sz32, lB = lA + TYK * sy32;
-        update(Dc, Dm, D, ownA, rowA, dnA, ty + 1, sA0, mA0, lA, activeA);
-        update(Dc, Dm, D, ownB, rowB, dnB, ty + TYK + 1, sB0, mB0, lB, activeB);
+        update(sm.der[uc], sm.der[um], D, ownA, rowA, dnA, ty + 1, sA0, mA0, lA, activeA);
+        update(sm.der[uc], sm.der[um], D, ownB, rowB, dnB, ty + TYK + 1, sB0, mB0, lB, activeB);
       }
       sA0 = sA1;
       mA0 = mA1;
       sB0 = sB1;
       mB0 = mB1;
-      u = u == 2 ? 0 : u + 1;
+    };
+    for (int base = pb; base <= ke; base += NST) {
+      plane(std::integral_constant<int, 0>{}, base);
+      if (base + 1 > ke) break;
+      plane(std::integral_constant<int, 1>{}, base + 1);
+      if (base + 2 > ke) break;
+      plane(std::integral_constant<int, 2>{}, base + 2);
     }
     if (__any_sync(0xffffffffu, bad) && (tid & 31) == 0) atomicOr(err, 1u);
     __syncthreads();  // the next item's loads reuse the stages and rows
