@@ -287,7 +287,10 @@ capaz_batch* capaz_batch_create(const capaz_params* params, int count, int devic
     }
     b->ctx.push_back(x);
   }
-  if (cudaMalloc(&b->counter, sizeof(unsigned int)) != cudaSuccess) {
+  // The work counter starts at zero; the precision form's boundary kernel
+  // rearms it after every sweep.
+  if (cudaMalloc(&b->counter, sizeof(unsigned int)) != cudaSuccess ||
+      cudaMemset(b->counter, 0, sizeof(unsigned int)) != cudaSuccess) {
     capaz_batch_destroy(b);
     if (status) *status = CAPAZ_ERR_OUT_OF_MEMORY;
     return nullptr;

@@ -188,6 +188,10 @@ PhysF make_physf(const capaz_params& p) {
   f.inv_hy2 = (float)(1. / (p.hy * p.hy));
   f.inv_hz2 = (float)(1. / (p.hz * p.hz));
   f.g_inv_hy = (float)(p.g_const / p.hy);
+  f.cw_mu = (float)(p.ro0_w * p.beta_w / p.mu_w);
+  f.cn_mu = (float)(p.ro0_n * p.beta_n / p.mu_n);
+  f.g_mu_w = (float)(p.g_const * p.mu_w / p.hy);
+  f.g_mu_n = (float)(p.g_const * p.mu_n / p.hy);
   f.iters = 1;  // one Newton step: the delta-form solve of the TMA kernel
   f.ro0_w = p.ro0_w;
   f.ro0_n = p.ro0_n;
@@ -198,6 +202,8 @@ PhysF make_physf(const capaz_params& p) {
   f.g = p.g_const;
   f.hy = p.hy;
   f.vol = p.hx * p.hy * p.hz;
+  f.mu_w = p.mu_w;
+  f.mu_n = p.mu_n;
   return f;
 }
 

@@ -115,8 +115,11 @@ int step2_fp32c_batch_grid(int device);
 // in one descriptor per instance in global memory.
 struct PhysF {
   float inv_one_m_swr, ro0w_bw, ro0n_bn, inv_mu_w, inv_mu_n, K0, inv_hx2, inv_hy2, inv_hz2, g_inv_hy;
+  // rho_p / mu_p is formed directly: (rho_0p beta_p / mu_p) p + rho_p(P_ref)/mu_p
+  // (per-row table); the gravity force g rho_p / hy is then (g mu_p / hy) times it.
+  float cw_mu, cn_mu, g_mu_w, g_mu_n;
   int iters;
-  double ro0_w, ro0_n, aw, bn, P_atm, P_top, g, hy, vol;
+  double ro0_w, ro0_n, aw, bn, P_atm, P_top, g, hy, vol, mu_w, mu_n;
 };
 struct alignas(128) InstT {
   CUtensorMap map_p[2], map_s[2], map_K, map_m;
@@ -127,7 +130,7 @@ struct alignas(128) InstT {
   float sgr_dev_f;  // S_n_gr - S_ref (stored deviation of the source saturation)
   int nbound;       // boundary cells (written by the boundary kernel after the sweep)
   double S_ref, dt;
-  const float4* rowF;  // ny: (rho_w, rho_n at P_ref(j), (P_ref(j+1)-P_ref(j))/hy^2, 0)
+  const float4* rowF;  // ny: (rho_w/mu_w, rho_n/mu_n at P_ref(j), (P_ref(j+1)-P_ref(j))/hy^2, 0)
   const double* Pref;  // ny
   Step2FArgs a[2];     // a[parity]: state pointers and the error flag
 };

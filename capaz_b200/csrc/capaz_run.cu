@@ -263,6 +263,8 @@ int capaz_ctx::tma_prepare() {
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(tma)");
     e = cudaMalloc(&tma_counter, sizeof(unsigned int));
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(tma)");
+    e = cudaMemset(tma_counter, 0, sizeof(unsigned int));
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemset(tma)");
   }
   e = cudaMemcpy(tma_inst, &h, sizeof h, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy(tma descriptor)");

@@ -93,7 +93,7 @@ __global__ void row_tables_kernel(const double* __restrict__ Pref, int ny, const
   if (j >= ny) return;
   const double prel = Pref[j] - f.P_atm;
   const double dnext = (j + 1 < ny) ? (Pref[j + 1] - Pref[j]) : 0.;
-  rowF[j] = make_float4((float)(f.ro0_w + f.aw * prel), (float)(f.ro0_n + f.bn * prel),
+  rowF[j] = make_float4((float)((f.ro0_w + f.aw * prel) / f.mu_w), (float)((f.ro0_n + f.bn * prel) / f.mu_n),
                         (float)(dnext * (double)f.inv_hy2), 0.f);
 }
 

@@ -108,17 +108,17 @@ struct Ctr {
 };
 
 __device__ __forceinline__ void derive(const PhysF& f, float c1, float Aw, float An, float p, float s, float K,
-                                       Der& d, float& rw, float& rn) {
+                                       Der& d) {
+  // Aw, An: rho_p / mu_p at the row's reference pressure; rho_p(P) / mu_p is
+  // linear in the pressure deviation p.
   const float S_e = (c1 - s) * f.inv_one_m_swr;
   const float e2 = S_e * S_e;
   const float om = 1.f - S_e;
   const float kw = e2 * e2;
   const float kn = om * om * (1.f - e2);
-  rw = fmaf(f.ro0w_bw, p, Aw);
-  rn = fmaf(f.ro0n_bn, p, An);
   d.p = p;
-  d.Mw = (K * f.inv_mu_w) * kw * rw;
-  d.Mn = (K * f.inv_mu_n) * kn * rn;
+  d.Mw = K * kw * fmaf(f.cw_mu, p, Aw);
+  d.Mn = K * kn * fmaf(f.cn_mu, p, An);
 }
 
 // In/out difference of one axis for one phase: x1, x2 are the scaled driving
@@ -141,10 +141,10 @@ struct Kahan3 {  // Kahan sum of three terms, first term taken as the start
 };
 
 __device__ __forceinline__ double rcp64(double x) {
-  // FP32 seed refined by two Newton-Raphson steps r <- r (2 - x r): each
-  // step squares the relative error (2^-23 -> 2^-46 -> below 2^-53).
+  // FP32 seed refined by one Newton-Raphson step r <- r (2 - x r), which
+  // squares the relative error: 2^-23 -> 2^-46, far below the FP32 storage
+  // of the result.
   double r = (double)__frcp_rn((float)x);
-  r = r * fma(-x, r, 2.0);
   r = r * fma(-x, r, 2.0);
   return r;
 }
@@ -167,7 +167,7 @@ struct Smem {
   RawStage raw[NST];
   float4 der[NST][WCELLS];  // (p, M_w, M_n, -) of the window, one slot per plane in flight
   uint64_t bar[NST];
-  float4 rowF[WY];          // (rho_w, rho_n at the row's P_ref, dP_ref/hy^2 to the next row, -)
+  float4 rowF[WY];          // (rho_w/mu_w, rho_n/mu_n at the row's P_ref, dP_ref/hy^2 to the next row, -)
   double rowPrel[WY];       // P_ref - P_atm
   double rowPref[WY];
   double red[NTK / 32][4];  // diagnostics reduction
@@ -283,8 +283,7 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
         const float dxn = x2 * (u2 ? C0.Mn : b.z) - x1 * (u1 ? a.z : C0.Mn);
         // y (vertical, gravity): P(j+1) - P(j) = dP_ref(j) + p(j+1) - p(j)
         const float4 ya = D[own - WX], yb = D[own + WX];
-        const float rw = fmaf(f.ro0w_bw, C0.p, row.x), rn = fmaf(f.ro0n_bn, C0.p, row.y);
-        const float gw = f.g_inv_hy * rw, gn = f.g_inv_hy * rn;
+        const float gw = f.g_mu_w * fmaf(f.cw_mu, C0.p, row.x), gn = f.g_mu_n * fmaf(f.cn_mu, C0.p, row.y);
         const float y1 = fmaf(ya.x - C0.p, f.inv_hy2, -dPs_dn);
         const float y2 = fmaf(C0.p - yb.x, f.inv_hy2, -row.z);
         const float dyw = face_diff(y1 + gw, y2 + gw, C0.Mw, ya.y, yb.y);
@@ -370,21 +369,19 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
       float sA1, mA1, sB1, mB1;
       {
         Der dA, dB;
-        float rw, rn;
         sA1 = R.s[rawA];
         sB1 = R.s[rawB];
         mA1 = R.m[rawA];
         mB1 = R.m[rawB];
-        derive(f, c1, rowA.x, rowA.y, R.p[rawA], sA1, UNIK ? f.K0 : R.K[rawA], dA, rw, rn);
-        derive(f, c1, rowB.x, rowB.y, R.p[rawB], sB1, UNIK ? f.K0 : R.K[rawB], dB, rw, rn);
+        derive(f, c1, rowA.x, rowA.y, R.p[rawA], sA1, UNIK ? f.K0 : R.K[rawA], dA);
+        derive(f, c1, rowB.x, rowB.y, R.p[rawB], sB1, UNIK ? f.K0 : R.K[rawB], dB);
         D[ownA] = make_float4(dA.p, dA.Mw, dA.Mn, 0.f);
         D[ownB] = make_float4(dB.p, dB.Mw, dB.Mn, 0.f);
       }
       if (halo_slot >= 0) {
         const float4 rh = sm.rowF[halo_row];
         Der h;
-        float rw, rn;
-        derive(f, c1, rh.x, rh.y, R.p[halo_raw], R.s[halo_raw], UNIK ? f.K0 : R.K[halo_raw], h, rw, rn);
+        derive(f, c1, rh.x, rh.y, R.p[halo_raw], R.s[halo_raw], UNIK ? f.K0 : R.K[halo_raw], h);
         D[halo_slot] = make_float4(h.p, h.Mw, h.Mn, 0.f);
       }
       __syncthreads();
@@ -463,7 +460,11 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
 // boundary cell; items are (instance, first cell) blocks of BOUND_BLOCK.
 __global__ void __launch_bounds__(BOUND_BLOCK) boundary_fp32c_kernel(const __grid_constant__ PhysF f,
                                                                      const InstT* __restrict__ insts,
-                                                                     const int2* __restrict__ bitems, int parity) {
+                                                                     const int2* __restrict__ bitems, int parity,
+                                                                     unsigned int* __restrict__ counter) {
+  // The sweep before this launch has taken all its work items: rearm its
+  // work counter for the next step (stream order makes this safe).
+  if (blockIdx.x == 0 && threadIdx.x == 0) *counter = 0u;
   const int2 it = bitems[blockIdx.x];
   const InstT* __restrict__ I = insts + it.x;
   const int q0 = it.y + (int)threadIdx.x;
@@ -563,8 +564,9 @@ cudaError_t launch_p(bool planar, const PhysF& f, const InstT* insts, const int4
 cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems,
                                    const int2* bitems, int nbitems, int parity, bool unik, bool planar,
                                    unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), s);
-  if (e != cudaSuccess) return e;
+  // `counter` is zero on entry: zeroed at allocation and rearmed by every
+  // boundary launch.
+  cudaError_t e;
   if (unik)
     e = diag_partials ? launch_p<true, true>(planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s)
                       : launch_p<true, false>(planar, f, insts, items, nitems, parity, counter, nullptr, grid, s);
@@ -572,7 +574,7 @@ cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int
     e = diag_partials ? launch_p<false, true>(planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s)
                       : launch_p<false, false>(planar, f, insts, items, nitems, parity, counter, nullptr, grid, s);
   if (e != cudaSuccess) return e;
-  boundary_fp32c_kernel<<<nbitems, BOUND_BLOCK, 0, s>>>(f, insts, bitems, parity);
+  boundary_fp32c_kernel<<<nbitems, BOUND_BLOCK, 0, s>>>(f, insts, bitems, parity, counter);
   return cudaGetLastError();
 }
 
