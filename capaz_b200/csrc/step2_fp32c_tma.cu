@@ -40,6 +40,7 @@
 #include <stdint.h>
 
 #include <type_traits>
+#include <utility>
 
 #include "capaz_internal.h"
 
@@ -92,6 +93,10 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
       : "memory");
 }
+// Programmatic dependent launch: wait until the grids this launch depends on
+// have completed and their memory is visible (a no-op for an ordinary launch).
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -215,12 +220,20 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
   }
 
   double acc_w = 0., acc_n = 0., rmax = 0., nonfinite = 0.;
+  // Everything above overlaps the previous kernel's tail; the work counter and
+  // the state are touched only after it has completed.
+  grid_dependency_wait();
 
   for (;;) {
     if (tid == 0) sm.w_sh = (int)atomicAdd(counter, 1u);
     __syncthreads();
     const int w = sm.w_sh;
-    if (w >= nitems) break;
+    if (w >= nitems) {
+      // No work left for this CTA: the boundary kernel may be scheduled (it
+      // waits for the whole sweep with griddepcontrol.wait).
+      asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+      break;
+    }
     const int4 it = items[w];
     const InstT* __restrict__ I = insts + it.x;
     const int nx = I->nx, ny = I->ny, nz = I->nz;
@@ -462,8 +475,9 @@ __global__ void __launch_bounds__(BOUND_BLOCK) boundary_fp32c_kernel(const __gri
                                                                      const InstT* __restrict__ insts,
                                                                      const int2* __restrict__ bitems, int parity,
                                                                      unsigned int* __restrict__ counter) {
+  grid_dependency_wait();  // the sweep's interior values and its use of the counter
   // The sweep before this launch has taken all its work items: rearm its
-  // work counter for the next step (stream order makes this safe).
+  // work counter for the next step.
   if (blockIdx.x == 0 && threadIdx.x == 0) *counter = 0u;
   const int2 it = bitems[blockIdx.x];
   const InstT* __restrict__ I = insts + it.x;
@@ -527,6 +541,25 @@ __global__ void __launch_bounds__(BOUND_BLOCK) boundary_fp32c_kernel(const __gri
   A.p_out[lb] = pb;
 }
 
+// Launches with programmatic stream serialisation: the kernel may start
+// while the previous kernel in the stream finishes, and waits for it with
+// griddepcontrol.wait before touching what that kernel writes.
+template <typename... Params, typename... Args>
+cudaError_t launch_dependent(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                             Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // Opts the kernel into its dynamic shared memory, once per device.
 template <bool UNIK, bool DIAG, bool PLANAR>
 cudaError_t prepare_t() {
@@ -547,9 +580,8 @@ cudaError_t launch_t(const PhysF& f, const InstT* insts, const int4* items, int 
                      unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
   cudaError_t e = prepare_t<UNIK, DIAG, PLANAR>();
   if (e != cudaSuccess) return e;
-  step2_fp32c_tma_kernel<UNIK, DIAG, PLANAR><<<grid, dim3(TX, TYK), kSmemBytes, s>>>(f, insts, items, nitems, parity,
-                                                                                   counter, diag_partials);
-  return cudaGetLastError();
+  return launch_dependent(step2_fp32c_tma_kernel<UNIK, DIAG, PLANAR>, dim3(grid), dim3(TX, TYK), kSmemBytes, s, f,
+                          insts, items, nitems, parity, counter, diag_partials);
 }
 
 template <bool UNIK, bool DIAG>
@@ -574,8 +606,8 @@ cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int
     e = diag_partials ? launch_p<false, true>(planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s)
                       : launch_p<false, false>(planar, f, insts, items, nitems, parity, counter, nullptr, grid, s);
   if (e != cudaSuccess) return e;
-  boundary_fp32c_kernel<<<nbitems, BOUND_BLOCK, 0, s>>>(f, insts, bitems, parity, counter);
-  return cudaGetLastError();
+  return launch_dependent(boundary_fp32c_kernel, dim3(nbitems), dim3(BOUND_BLOCK), 0, s, f, insts, bitems, parity,
+                          counter);
 }
 
 int step2_fp32c_tma_grid(int device, bool unik) {
