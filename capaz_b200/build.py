@@ -41,6 +41,7 @@ CUDA_SOURCES = [
     ("batch.cu", []),
     ("adjoint.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
+    ("io.cu", []),
 ]
 HEADERS = ["capaz_internal.h", "capaz_ctx.h"]
 

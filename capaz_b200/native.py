@@ -117,6 +117,9 @@ PROTOTYPES = {
     "capaz_batch_autotune": (C.c_int, [_VP, _VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "capaz_batch_launch_count": (C.c_int64, [_VP]),
     "capaz_sync": (C.c_int, [_VP]),
+    "capaz_write_plot": (C.c_int, [_VP, C.c_char_p, C.c_double]),
+    "capaz_save": (C.c_int, [_VP, C.c_char_p, C.c_int]),
+    "capaz_restore": (C.c_int, [_VP, C.c_char_p, C.POINTER(C.c_int)]),
     "capaz_adjoint_create": (_VP, [_VP, C.c_int, C.c_int, _VP, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     "capaz_adjoint_destroy": (C.c_int, [_VP]),
     "capaz_adjoint_set_observations": (C.c_int, [_VP, _VP, C.c_int, _VP]),

@@ -8,6 +8,7 @@ reference's index i + j*nx + k*nx*ny (main.cpp:695) with y vertical
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -131,6 +132,20 @@ class Simulation:
 
     def sync(self) -> None:
         check(self.lib.capaz_sync(self.ctx), self.ctx)
+
+    # -- files in the reference's formats ---------------------------------
+    def write_plot(self, dirpath: str, t: float) -> str:
+        """Tecplot plot file <dirpath>/S=%012.4f.dat; returns its path."""
+        check(self.lib.capaz_write_plot(self.ctx, os.fsencode(dirpath), float(t)), self.ctx)
+        return os.path.join(dirpath, "S=%012.4f.dat" % t)
+
+    def save(self, path: str, time_counter: int = 0) -> None:
+        check(self.lib.capaz_save(self.ctx, os.fsencode(path), int(time_counter)), self.ctx)
+
+    def restore(self, path: str) -> int:
+        tc = C.c_int(0)
+        check(self.lib.capaz_restore(self.ctx, os.fsencode(path), C.byref(tc)), self.ctx)
+        return tc.value
 
     @property
     def launch_count(self) -> int:

@@ -244,6 +244,21 @@ int64_t capaz_launch_count(const capaz_ctx* ctx);
 /* Synchronises the context's device and reports any pending CUDA error. */
 int capaz_sync(capaz_ctx* ctx);
 
+/* ---- output and checkpoint files (the reference's formats) --------------
+ * capaz_write_plot: the Tecplot point file print_plots writes
+ * (main.cpp:549-781), <dir>/S=%012.4f.dat with the reference's header and
+ * rows (i outer, j, k; y flipped), `t` the file's time; creates `dir`.
+ * Velocities are those of the last step (zero before the first step, as the
+ * reference's arrays are).  capaz_save / capaz_restore: save.dat of
+ * save/restore (main.cpp:1035-1145): int32 time counter, then nx*ny*nz
+ * float64 each of [S_w], P_w, S_n, roS_w_old, roS_n_old, [roS_g_old], m
+ * ([..]: three-phase).  Restore reads exactly those sizes (the reference's
+ * restore reads locNy*locNy planes) and loads m and the state; three-phase
+ * P_n and P_g are set to P_w (the CPU model has no capillary pressure). */
+int capaz_write_plot(capaz_ctx* ctx, const char* dir, double t);
+int capaz_save(capaz_ctx* ctx, const char* path, int time_counter);
+int capaz_restore(capaz_ctx* ctx, const char* path, int* time_counter);
+
 /* ---- differentiation ------------------------------------------------------
  * Discrete adjoint of the two-phase FP64 step (CAPAZ_FORM_FP64 with
  * CAPAZ_FLAG_PERCELL_K).  The misfit is
