@@ -42,6 +42,7 @@ CUDA_SOURCES = [
     ("adjoint.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
     ("io.cu", []),
+    ("media.cu", []),
 ]
 HEADERS = ["capaz_internal.h", "capaz_ctx.h"]
 

@@ -117,6 +117,10 @@ PROTOTYPES = {
     "capaz_batch_autotune": (C.c_int, [_VP, _VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "capaz_batch_launch_count": (C.c_int64, [_VP]),
     "capaz_sync": (C.c_int, [_VP]),
+    "capaz_read_permeability_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _VP]),
+    "capaz_load_permeability": (C.c_int, [_VP, C.c_char_p]),
+    "capaz_generate_media": (C.c_int, [_VP, C.c_ulonglong, C.c_double, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, C.c_int]),
     "capaz_write_plot": (C.c_int, [_VP, C.c_char_p, C.c_double]),
     "capaz_save": (C.c_int, [_VP, C.c_char_p, C.c_int]),
     "capaz_restore": (C.c_int, [_VP, C.c_char_p, C.POINTER(C.c_int)]),

@@ -133,6 +133,18 @@ class Simulation:
     def sync(self) -> None:
         check(self.lib.capaz_sync(self.ctx), self.ctx)
 
+    # -- heterogeneous media ----------------------------------------------
+    def load_permeability(self, path: str) -> None:
+        """K per cell from a permeability file (load_permeability's format)."""
+        check(self.lib.capaz_load_permeability(self.ctx, os.fsencode(path)), self.ctx)
+
+    def generate_media(self, seed: int, sigma: float = 1.0, ell: float = 8.0, K_mean: float = 1e-12,
+                       phi0: float = 0.25, dphi: float = 0.02, nmodes: int = 1024) -> None:
+        """Seeded Gaussian field on the device: K = K_mean exp(sigma G),
+        porosity = clip(phi0 + dphi G, 0.1, 0.4), covariance exp(-r/ell)."""
+        check(self.lib.capaz_generate_media(self.ctx, int(seed), float(sigma), float(ell), float(K_mean),
+                                            float(phi0), float(dphi), int(nmodes)), self.ctx)
+
     # -- files in the reference's formats ---------------------------------
     def write_plot(self, dirpath: str, t: float) -> str:
         """Tecplot plot file <dirpath>/S=%012.4f.dat; returns its path."""
@@ -251,3 +263,14 @@ class Adjoint:
             self.close()
         except Exception:
             pass
+
+
+def read_permeability_file(path: str, nx: int, ny: int, nz: int) -> np.ndarray:
+    """K (nz, ny, nx) from a permeability file in load_permeability's format."""
+    lib = native.load()
+    K = np.empty((nz, ny, nx), dtype=np.float64)
+    st = lib.capaz_read_permeability_file(os.fsencode(path), nx, ny, nz, K.ctypes.data)
+    if st:
+        msg = lib.capaz_last_error(None)
+        raise native.CapazError(st, msg.decode() if msg else "")
+    return K

@@ -190,8 +190,10 @@ int capaz_get_field(capaz_ctx* ctx, int field, double* host, void* stream);
 enum capaz_state_sel { CAPAZ_STATE_STEP_START = 0, CAPAZ_STATE_CURRENT = 1 };
 int capaz_get_derived(capaz_ctx* ctx, int field, int state_sel, void* dst, int dst_on_device, void* stream);
 /* Device-resident variants: `dev` is a device pointer of the context's device
- * holding nx*ny*nz values of the storage type of the form (float64 for
- * CAPAZ_FORM_FP64, float32 for the state of CAPAZ_FORM_FP32C). */
+ * holding nx*ny*nz values: float64 for capaz_set_field_device (either form;
+ * the precision form encodes them), the storage type of the form for
+ * capaz_get_field_device (float64 for CAPAZ_FORM_FP64, float32 for the state
+ * of CAPAZ_FORM_FP32C). */
 int capaz_set_field_device(capaz_ctx* ctx, int field, const void* dev, void* stream);
 int capaz_get_field_device(capaz_ctx* ctx, int field, void* dev, void* stream);
 
@@ -243,6 +245,23 @@ int64_t capaz_batch_launch_count(const capaz_batch* b);
 int64_t capaz_launch_count(const capaz_ctx* ctx);
 /* Synchronises the context's device and reports any pending CUDA error. */
 int capaz_sync(capaz_ctx* ctx);
+
+/* ---- heterogeneous media -------------------------------------------------
+ * capaz_read_permeability_file: the permeability file of load_permeability
+ * (main.cpp:918-1032, LOAD_K_FROM_FILE): a header "Nx Ny" (nz == 1) or
+ * "Nx Ny Nz" that must equal the grid (the reference only warns), then Ny
+ * rows of Nx blank-separated values v; K = 1e-10 exp(v) in every z layer.
+ * Host only (no context); K receives nx*ny*nz values.  Errors through
+ * capaz_last_error(NULL).  capaz_load_permeability reads the file into the
+ * context's per-cell K (needs CAPAZ_FLAG_PERCELL_K).
+ * capaz_generate_media (no counterpart in the reference): a seeded Gaussian
+ * field G with covariance exp(-r/ell) (r in cells) by the randomisation
+ * method with `nmodes` Fourier modes, generated on the device; sets
+ * K = K_mean exp(sigma G) and porosity = clip(phi0 + dphi G, 0.1, 0.4). */
+int capaz_read_permeability_file(const char* path, int nx, int ny, int nz, double* K);
+int capaz_load_permeability(capaz_ctx* ctx, const char* path);
+int capaz_generate_media(capaz_ctx* ctx, unsigned long long seed, double sigma, double ell, double K_mean,
+                         double phi0, double dphi, int nmodes);
 
 /* ---- output and checkpoint files (the reference's formats) --------------
  * capaz_write_plot: the Tecplot point file print_plots writes
