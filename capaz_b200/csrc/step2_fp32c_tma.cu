@@ -28,9 +28,9 @@
 // phases; outflow through the + face is x2 * M(upwind), inflow through the
 // - face x1 * M(upwind); the in/out difference of an axis is formed first
 // (exact when the two nearly cancel, by Sterbenz's lemma) and the three axis
-// terms are Kahan-summed.  d(rho S) = -dt/m * div goes to FP64, where one
-// Newton step with the Jacobian at the stored state solves the bilinear
-// system for (dP, dS).
+// terms are Kahan-summed, both phases at once in packed f32x2 arithmetic.
+// d(rho S) = -dt/m * div goes to FP64, where one Newton step with the
+// Jacobian at the stored state solves the bilinear system for (dP, dS).
 // Boundary cells are written by a second, small kernel over the boundary
 // shell after the sweep, which keeps the sweep free of per-cell face tests.
 // Waits on mbarriers are bounded; a wait that runs out sets bit 1 of the
@@ -134,15 +134,46 @@ __device__ __forceinline__ float face_diff(float x1, float x2, float Mc, float M
   return out - in;
 }
 
-struct Kahan3 {  // Kahan sum of three terms, first term taken as the start
-  float s, c;
-  __device__ __forceinline__ explicit Kahan3(float a) : s(a), c(0.f) {}
-  __device__ __forceinline__ void add(float x) {
-    const float y = x - c;
-    const float t = s + y;
-    c = (t - s) - y;
+// Two FP32 values in one 64-bit register pair for sm_100's packed f32x2
+// arithmetic: every lane is an ordinary round-to-nearest FP32 operation, one
+// instruction for both phases.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pack2(float a, float b) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void unpack2(f32x2 r, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+// Kahan sum of three terms of both phases at once, the first term taken as
+// the start.
+struct Kahan2 {
+  f32x2 s, c;
+  __device__ __forceinline__ explicit Kahan2(f32x2 a) : s(a), c(0ull) {}
+  __device__ __forceinline__ void add(f32x2 x) {
+    const f32x2 y = sub2(x, c);
+    const f32x2 t = add2(s, y);
+    c = sub2(sub2(t, s), y);
     s = t;
   }
+  __device__ __forceinline__ f32x2 sum() const { return sub2(s, c); }
 };
 
 __device__ __forceinline__ double rcp64(double x) {
@@ -183,7 +214,7 @@ constexpr size_t kSmemBytes = sizeof(Smem);
 #ifndef CAPAZ_TMA_MIN_BLOCKS
 #define CAPAZ_TMA_MIN_BLOCKS 3
 #endif
-template <bool UNIK, bool DIAG, bool PLANAR>
+template <bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
 __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
     step2_fp32c_tma_kernel(const __grid_constant__ PhysF f, const InstT* __restrict__ insts,
                            const int4* __restrict__ items, int nitems, int parity, unsigned int* __restrict__ counter,
@@ -286,40 +317,42 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
                       int own, float4 row, float dPs_dn, int wrow, float sc, float mc, int l, bool active) {
       const float4 c4 = D[own];
       const Der C0{c4.x, c4.y, c4.z};
-      float Dw, Dn;
+      f32x2 D2;  // (div F_w, div F_n)
       {
         const float4 a = D[own - 1], b = D[own + 1];
-        const float cpx = C0.p * f.inv_hx2;
-        const float x1 = fmaf(a.x, f.inv_hx2, -cpx), x2 = fmaf(-b.x, f.inv_hx2, cpx);
+        // Forces: pressure differences of neighbours (exact when they are
+        // close), scaled by 1/h^2 unless the spacing is 1.
+        const float x1 = UNITH ? a.x - C0.p : (a.x - C0.p) * f.inv_hx2;
+        const float x2 = UNITH ? C0.p - b.x : (C0.p - b.x) * f.inv_hx2;
         const bool u1 = x1 > 0.f, u2 = x2 > 0.f;
         const float dxw = x2 * (u2 ? C0.Mw : b.y) - x1 * (u1 ? a.y : C0.Mw);
         const float dxn = x2 * (u2 ? C0.Mn : b.z) - x1 * (u1 ? a.z : C0.Mn);
         // y (vertical, gravity): P(j+1) - P(j) = dP_ref(j) + p(j+1) - p(j)
         const float4 ya = D[own - WX], yb = D[own + WX];
         const float gw = f.g_mu_w * fmaf(f.cw_mu, C0.p, row.x), gn = f.g_mu_n * fmaf(f.cn_mu, C0.p, row.y);
-        const float y1 = fmaf(ya.x - C0.p, f.inv_hy2, -dPs_dn);
-        const float y2 = fmaf(C0.p - yb.x, f.inv_hy2, -row.z);
+        const float y1 = UNITH ? (ya.x - C0.p) - dPs_dn : fmaf(ya.x - C0.p, f.inv_hy2, -dPs_dn);
+        const float y2 = UNITH ? (C0.p - yb.x) - row.z : fmaf(C0.p - yb.x, f.inv_hy2, -row.z);
         const float dyw = face_diff(y1 + gw, y2 + gw, C0.Mw, ya.y, yb.y);
         const float dyn = face_diff(y1 + gn, y2 + gn, C0.Mn, ya.z, yb.z);
-        Kahan3 kw(dxw), kn(dxn);
-        kw.add(dyw);
-        kn.add(dyn);
+        Kahan2 k(pack2(dxw, dxn));
+        k.add(pack2(dyw, dyn));
         if (!PLANAR) {
           const float4 m4 = Dm[own], p4 = Dp[own];
           const Der m1{m4.x, m4.y, m4.z}, p1{p4.x, p4.y, p4.z};
-          const float cpz = C0.p * f.inv_hz2;
-          const float z1 = fmaf(m1.p, f.inv_hz2, -cpz), z2 = fmaf(-p1.p, f.inv_hz2, cpz);
+          const float z1 = UNITH ? m1.p - C0.p : (m1.p - C0.p) * f.inv_hz2;
+          const float z2 = UNITH ? C0.p - p1.p : (C0.p - p1.p) * f.inv_hz2;
           const bool v1 = z1 > 0.f, v2 = z2 > 0.f;
-          kw.add(z2 * (v2 ? C0.Mw : p1.Mw) - z1 * (v1 ? m1.Mw : C0.Mw));
-          kn.add(z2 * (v2 ? C0.Mn : p1.Mn) - z1 * (v1 ? m1.Mn : C0.Mn));
+          k.add(pack2(z2 * (v2 ? C0.Mw : p1.Mw) - z1 * (v1 ? m1.Mw : C0.Mw),
+                      z2 * (v2 ? C0.Mn : p1.Mn) - z1 * (v1 ? m1.Mn : C0.Mn)));
         }
-        Dw = kw.s - kw.c;
-        Dn = kn.s - kn.c;
+        D2 = k.sum();
       }
       // Conserved increments d(rho S) = -dt/m * div F (FP32), Newton in FP64.
       const float dtm = __fdividef(dt_f, mc);
-      const double Aw = (double)(-dtm * Dw);
-      const double An = (double)(-dtm * Dn);
+      float Awf, Anf;
+      unpack2(mul2(pack2(-dtm, -dtm), D2), Awf, Anf);
+      const double Aw = (double)Awf;
+      const double An = (double)Anf;
       const double S = S_ref + (double)sc;
       const double prel = sm.rowPrel[wrow];
       const double pr = prel + (double)C0.p;
@@ -561,7 +594,7 @@ cudaError_t launch_dependent(void (*kernel)(Params...), dim3 grid, dim3 block, s
 }
 
 // Opts the kernel into its dynamic shared memory, once per device.
-template <bool UNIK, bool DIAG, bool PLANAR>
+template <bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
 cudaError_t prepare_t() {
   static unsigned long long done = 0;  // bit d: set on device d
   int dev = 0;
@@ -569,26 +602,35 @@ cudaError_t prepare_t() {
   if (e != cudaSuccess) return e;
   const unsigned long long bit = 1ull << (dev & 63);
   if (__atomic_load_n(&done, __ATOMIC_ACQUIRE) & bit) return cudaSuccess;
-  e = cudaFuncSetAttribute(step2_fp32c_tma_kernel<UNIK, DIAG, PLANAR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)kSmemBytes);
+  e = cudaFuncSetAttribute(step2_fp32c_tma_kernel<UNIK, DIAG, PLANAR, UNITH>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
   if (e == cudaSuccess) __atomic_fetch_or(&done, bit, __ATOMIC_ACQ_REL);
   return e;
 }
 
-template <bool UNIK, bool DIAG, bool PLANAR>
+template <bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
 cudaError_t launch_t(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
                      unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
-  cudaError_t e = prepare_t<UNIK, DIAG, PLANAR>();
+  cudaError_t e = prepare_t<UNIK, DIAG, PLANAR, UNITH>();
   if (e != cudaSuccess) return e;
-  return launch_dependent(step2_fp32c_tma_kernel<UNIK, DIAG, PLANAR>, dim3(grid), dim3(TX, TYK), kSmemBytes, s, f,
-                          insts, items, nitems, parity, counter, diag_partials);
+  return launch_dependent(step2_fp32c_tma_kernel<UNIK, DIAG, PLANAR, UNITH>, dim3(grid), dim3(TX, TYK), kSmemBytes,
+                          s, f, insts, items, nitems, parity, counter, diag_partials);
+}
+
+template <bool UNIK, bool DIAG, bool PLANAR>
+cudaError_t launch_h(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
+                     unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
+  // Unit spacing (the workloads' h = 1 m): forces are plain differences.
+  const bool unith = f.inv_hx2 == 1.f && f.inv_hy2 == 1.f && f.inv_hz2 == 1.f;
+  return unith ? launch_t<UNIK, DIAG, PLANAR, true>(f, insts, items, nitems, parity, counter, diag_partials, grid, s)
+               : launch_t<UNIK, DIAG, PLANAR, false>(f, insts, items, nitems, parity, counter, diag_partials, grid, s);
 }
 
 template <bool UNIK, bool DIAG>
 cudaError_t launch_p(bool planar, const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
                      unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
-  return planar ? launch_t<UNIK, DIAG, true>(f, insts, items, nitems, parity, counter, diag_partials, grid, s)
-                : launch_t<UNIK, DIAG, false>(f, insts, items, nitems, parity, counter, diag_partials, grid, s);
+  return planar ? launch_h<UNIK, DIAG, true>(f, insts, items, nitems, parity, counter, diag_partials, grid, s)
+                : launch_h<UNIK, DIAG, false>(f, insts, items, nitems, parity, counter, diag_partials, grid, s);
 }
 
 }  // namespace
@@ -615,12 +657,12 @@ int step2_fp32c_tma_grid(int device, bool unik) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   int per = 0;
   if (unik) {
-    prepare_t<true, true, false>();
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<true, true, false>, NTK,
+    prepare_t<true, true, false, false>();
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<true, true, false, false>, NTK,
                                                   kSmemBytes);
   } else {
-    prepare_t<false, true, false>();
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<false, true, false>, NTK,
+    prepare_t<false, true, false, false>();
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<false, true, false, false>, NTK,
                                                   kSmemBytes);
   }
   if (per < 1) per = 1;

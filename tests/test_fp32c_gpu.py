@@ -128,13 +128,15 @@ def test_fp32c_derived_fields_decode():
             assert rel_l2(a, ref["derived"][f]) <= 1e-5, f
 
 
-@pytest.mark.parametrize("shape,steps", [((68, 21, 19), 40), ((256, 30, 20), 20), ((36, 9, 1), 30)])
-def test_fp32c_tma_path_matches_plain_load_path(shape, steps):
+@pytest.mark.parametrize("shape,steps,h", [((68, 21, 19), 40, (1.0, 1.0, 1.0)), ((256, 30, 20), 20, (1.0, 1.0, 1.0)),
+                                            ((36, 9, 1), 30, (1.0, 1.0, 1.0)), ((44, 19, 13), 30, (0.5, 2.0, 1.5))])
+def test_fp32c_tma_path_matches_plain_load_path(shape, steps, h):
     """The TMA-staged kernel (nx a multiple of 4) against the plain-load
-    kernel and the FP64 oracle, on ragged tiles, several z-chunks and a
-    planar grid."""
+    kernel and the FP64 oracle, on ragged tiles, several z-chunks, a planar
+    grid and a non-unit spacing."""
     nx, ny, nz = shape
     p = two_phase_params(nx, ny, nz, form=native.FORM_FP32C)
+    p.hx, p.hy, p.hz = h
     m, K = heterogeneous_fields((nz, ny, nx), 1.0, 4.0, 17)
     p.dt = stable_dt(p, m, K)
     st = O.init(p, m)
