@@ -43,6 +43,7 @@ CUDA_SOURCES = [
     ("noalloc.cu", ["-fmad=false"]),
     ("io.cu", []),
     ("media.cu", []),
+    ("slab.cu", []),
 ]
 HEADERS = ["capaz_internal.h", "capaz_ctx.h"]
 

@@ -42,7 +42,7 @@ using namespace capaz;
 namespace {
 
 struct AdjConst {
-  int nx, ny, nz, planar, source;
+  int nx, ny, nz, planar, source, win_k0, win_k1;
   long long sy, sz, n;
   double hx, hy, hz, dt, g, P_atm, ro0_w, ro0_n, beta_w, beta_n, mu_w, mu_n, S_wr, P_d, lambda;
   double e_kw, e_kn, e_pk;
@@ -55,6 +55,7 @@ AdjConst make_adj_const(const capaz_params& p) {
   c.nz = p.nz;
   c.planar = p.nz < 2;
   c.source = p.source;
+  window_k(p, &c.win_k0, &c.win_k1);
   c.sy = p.nx;
   c.sz = (long long)p.nx * p.ny;
   c.n = c.sz * p.nz;
@@ -84,8 +85,7 @@ __device__ __forceinline__ bool is_interior(const AdjConst& c, int i, int j, int
 }
 
 __device__ __forceinline__ bool in_window(const AdjConst& c, int i, int k) {
-  return (i >= c.nx / 2 - c.source) && (i <= c.nx / 2 + c.source) && (k >= c.nz / 2 - c.source) &&
-         (k <= c.nz / 2 + c.source);
+  return (i >= c.nx / 2 - c.source) && (i <= c.nx / 2 + c.source) && (k >= c.win_k0) && (k <= c.win_k1);
 }
 
 // Constitutive relations and their S-derivatives (two-phase.cpp:11-23,

@@ -68,6 +68,7 @@ Step2Const make_step2_const(const capaz_params& p) {
   c.ny = p.ny;
   c.nz = p.nz;
   c.source = p.source;
+  window_k(p, &c.win_k0, &c.win_k1);
   c.iters = p.newton_iterations;
   c.sy = p.nx;
   c.sz = (long long)p.nx * p.ny;
@@ -128,6 +129,8 @@ Step2FConst make_step2f_const(const capaz_params& p, double S_ref) {
   c.ny = d.ny;
   c.nz = d.nz;
   c.source = d.source;
+  c.win_k0 = d.win_k0;
+  c.win_k1 = d.win_k1;
   c.iters = 2;  // delta-form Newton: the system is bilinear and starts within one step's change
   c.tiles_x = d.tiles_x;
   c.tiles_y = d.tiles_y;
@@ -214,6 +217,7 @@ Step3Const make_step3_const(const capaz_params& p) {
   c.ny = p.ny;
   c.nz = p.nz;
   c.source = p.source;
+  window_k(p, &c.win_k0, &c.win_k1);
   c.iters = p.newton_iterations;
   c.source_window = (p.flags & CAPAZ_FLAG_SOURCE_WINDOW) ? 1 : 0;
   // Interior x range: [1, nx-2], or the single column of an nx == 1 grid.
@@ -273,8 +277,9 @@ void reference_init_host(const capaz_params& p, const double* m, double* Pw, dou
       for (int j = 0; j < p.ny; j++)
         for (int k = 0; k < p.nz; k++) {
           long long l = i + j * sy + (long long)k * sz;
-          bool win = (i >= p.nx / 2 - p.source) && (i <= p.nx / 2 + p.source) && (k >= p.nz / 2 - p.source) &&
-                     (k <= p.nz / 2 + p.source);
+          int wk0, wk1;
+          window_k(p, &wk0, &wk1);
+          bool win = (i >= p.nx / 2 - p.source) && (i <= p.nx / 2 + p.source) && (k >= wk0) && (k <= wk1);
           Sn[l] = ((j == 0) && win) ? p.S_n_gr : p.S_n_background;
           if (j == 0) {
             Pw[l] = p.P_atm;
@@ -419,6 +424,8 @@ int capaz_params_validate(const capaz_params* p) {
   if (!nx_ok || p->ny < 3 || p->nz < 1 || p->nz == 2)
     return fail(nullptr, CAPAZ_ERR_UNSUPPORTED_GRID, "grid %dx%dx%d unsupported (need nx,ny>=3, nz==1 or >=3)",
                 p->nx, p->ny, p->nz);
+  if (p->z_offset < 0 || p->nz_global < 0 || (p->nz_global > 0 && p->z_offset + p->nz > p->nz_global))
+    return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "z_offset/nz_global do not place the slab inside the grid");
   if ((long long)p->nx * p->ny * p->nz > (1LL << 34))
     return fail(nullptr, CAPAZ_ERR_UNSUPPORTED_GRID, "grid too large");
   if (!(p->hx > 0) || !(p->hy > 0) || !(p->hz > 0) || !(p->dt > 0))

@@ -24,9 +24,17 @@ constexpr int NTHREADS = TX * TY;
 // Per-step constants of the two-phase FP64 step, passed by value.  Every
 // derived constant is computed on the host with the same expression the
 // reference evaluates inline, so its double value is identical.
+// Injection window in z, in local plane indices: k in [win_k0, win_k1]
+// (|k_global - NZ_global/2| <= SOURCE).
+inline void window_k(const capaz_params& p, int* k0, int* k1) {
+  const int nzg = p.nz_global > 0 ? p.nz_global : p.nz;
+  *k0 = nzg / 2 - p.source - p.z_offset;
+  *k1 = nzg / 2 + p.source - p.z_offset;
+}
+
 struct Step2Const {
   int nx, ny, nz;
-  int source, iters;
+  int source, iters, win_k0, win_k1;
   int tiles_x, tiles_y, zchunk, nzchunks;
   long long sy, sz, ncell;
   double hx, hy, hz, dt, g, P_atm, P_top;
@@ -43,7 +51,7 @@ struct Step2Const {
 // Constants of the two-phase precision-form step (step2_fp32c.cu).
 struct Step2FConst {
   int nx, ny, nz;
-  int source, iters;
+  int source, iters, win_k0, win_k1;
   int tiles_x, tiles_y, zchunk, nzchunks;
   int intpow, n_kw, n_kn;  // relative-permeability exponents are small integers
   long long sy, sz;
@@ -71,7 +79,7 @@ cudaError_t launch_widen(const float* a, long long n, double* out, cudaStream_t 
 
 // Constants of the three-phase FP64 step (step3_fp64.cu).
 struct Step3Const {
-  int nx, ny, nz, source, iters, source_window;
+  int nx, ny, nz, source, iters, source_window, win_k0, win_k1;
   int tiles_x, tiles_y, zchunk, nzchunks, i_lo, i_hi;
   long long sy, sz, ncell;
   double hx, hy, hz, dt, g, P_atm;
@@ -123,7 +131,7 @@ struct PhysF {
 };
 struct alignas(128) InstT {
   CUtensorMap map_p[2], map_s[2], map_K, map_m;
-  int nx, ny, nz, tiles_x, tiles_y, zchunk, nzchunks, source;
+  int nx, ny, nz, tiles_x, tiles_y, zchunk, nzchunks, source, win_k0, win_k1;
   long long sy, sz;
   float c1_f;       // 1 - S_wr - S_ref
   float dt_f;

@@ -208,6 +208,7 @@ int capaz_ctx::tma_prepare() {
   h.tiles_x = d.tiles_x;
   h.tiles_y = (p.ny - 2 + TMA_TILE_Y - 1) / TMA_TILE_Y;
   h.source = p.source;
+  window_k(p, &h.win_k0, &h.win_k1);
   h.sy = d.sy;
   h.sz = d.sz;
   // 16-plane z-chunks: the dynamic schedule balances the work, and the

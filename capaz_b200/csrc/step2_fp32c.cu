@@ -97,8 +97,7 @@ __device__ __forceinline__ void axis_terms(CSum& acc, float x1, float x2, float 
 }
 
 __device__ __forceinline__ bool in_window(const Step2FConst& c, int i, int k) {
-  return (i >= c.nx / 2 - c.source) && (i <= c.nx / 2 + c.source) && (k >= c.nz / 2 - c.source) &&
-         (k <= c.nz / 2 + c.source);
+  return (i >= c.nx / 2 - c.source) && (i <= c.nx / 2 + c.source) && (k >= c.win_k0) && (k <= c.win_k1);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

@@ -185,8 +185,8 @@ __device__ __forceinline__ double rcp64(double x) {
   return r;
 }
 
-__device__ __forceinline__ bool in_window(int nx, int nz, int source, int i, int k) {
-  return (i >= nx / 2 - source) && (i <= nx / 2 + source) && (k >= nz / 2 - source) && (k <= nz / 2 + source);
+__device__ __forceinline__ bool in_window(const InstT* I, int i, int k) {
+  return (i >= I->nx / 2 - I->source) && (i <= I->nx / 2 + I->source) && (k >= I->win_k0) && (k <= I->win_k1);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(BOUND_BLOCK) boundary_fp32c_kernel(const __gri
   const Step2FArgs& A = I->a[parity];
   const float s1 = A.s_out[l1];
   float sb = s1;
-  if ((j == 0) && (I->source > 0) && in_window(nx, nz, I->source, i, k)) sb = I->sgr_dev_f;
+  if ((j == 0) && (I->source > 0) && in_window(I, i, k)) sb = I->sgr_dev_f;
   float pb;
   if ((j != 0) && (j != ny - 1)) {
     pb = A.p_out[l1];

@@ -107,8 +107,7 @@ __device__ __forceinline__ double residual2(const Step2Const& c, double roS_w, d
 }
 
 __device__ __forceinline__ bool in_window(const Step2Const& c, int i, int k) {
-  return (i >= c.nx / 2 - c.source) && (i <= c.nx / 2 + c.source) && (k >= c.nz / 2 - c.source) &&
-         (k <= c.nz / 2 + c.source);
+  return (i >= c.nx / 2 - c.source) && (i <= c.nx / 2 + c.source) && (k >= c.win_k0) && (k <= c.win_k1);
 }
 
 // Border_S + Border_P for every boundary cell whose basic coordinate is the

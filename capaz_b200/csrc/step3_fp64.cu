@@ -145,8 +145,7 @@ __device__ __forceinline__ bool reverse_matrix3(double* a) {
 }
 
 __device__ __forceinline__ bool in_window3(const Step3Const& c, int i, int k) {
-  return (i >= c.nx / 2 - c.source) && (i <= c.nx / 2 + c.source) && (k >= c.nz / 2 - c.source) &&
-         (k <= c.nz / 2 + c.source);
+  return (i >= c.nx / 2 - c.source) && (i <= c.nx / 2 + c.source) && (k >= c.win_k0) && (k <= c.win_k1);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

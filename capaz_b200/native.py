@@ -64,7 +64,8 @@ class Params(C.Structure):
         ("S_n_gr", C.c_double), ("S_w_gr", C.c_double), ("S_w_init", C.c_double),
         ("S_n_init", C.c_double), ("porosity", C.c_double), ("K0", C.c_double),
         ("timeX", C.c_double), ("P_top_offset", C.c_double), ("S_n_background", C.c_double),
-        ("reserved", C.c_double * 8),
+        ("z_offset", C.c_int32), ("nz_global", C.c_int32),
+        ("reserved", C.c_double * 7),
     ]
 
     def copy(self) -> "Params":
@@ -117,6 +118,8 @@ PROTOTYPES = {
     "capaz_batch_autotune": (C.c_int, [_VP, _VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "capaz_batch_launch_count": (C.c_int64, [_VP]),
     "capaz_sync": (C.c_int, [_VP]),
+    "capaz_get_plane": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),
+    "capaz_set_plane": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),
     "capaz_read_permeability_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _VP]),
     "capaz_load_permeability": (C.c_int, [_VP, C.c_char_p]),
     "capaz_generate_media": (C.c_int, [_VP, C.c_ulonglong, C.c_double, C.c_double, C.c_double, C.c_double,

@@ -133,6 +133,13 @@ class Simulation:
     def sync(self) -> None:
         check(self.lib.capaz_sync(self.ctx), self.ctx)
 
+    # -- z-planes of the state (slab halo exchange) -----------------------
+    def get_plane(self, name: str, k: int, dev_ptr: int, stream: int = 0) -> None:
+        check(self.lib.capaz_get_plane(self.ctx, FIELDS[name], int(k), dev_ptr, stream or None), self.ctx)
+
+    def set_plane(self, name: str, k: int, dev_ptr: int, stream: int = 0) -> None:
+        check(self.lib.capaz_set_plane(self.ctx, FIELDS[name], int(k), dev_ptr, stream or None), self.ctx)
+
     # -- heterogeneous media ----------------------------------------------
     def load_permeability(self, path: str) -> None:
         """K per cell from a permeability file (load_permeability's format)."""

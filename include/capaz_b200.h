@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define CAPAZ_ABI_VERSION 1
+#define CAPAZ_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 enum capaz_status {
@@ -101,7 +101,12 @@ typedef struct capaz_params {
   /* ---- extensions (neutral values reproduce the reference exactly) ---- */
   double P_top_offset;       /* top-face P_w = P_atm + P_top_offset (0)       */
   double S_n_background;     /* two-phase initial S_n off the source (0)      */
-  double reserved[8];
+  /* A z-slab of a larger grid (multi-GPU decomposition): the global index of
+   * local plane 0 and the global NZ, which place the injection window
+   * |k - NZ/2| <= SOURCE in global coordinates.  0, 0: the whole grid. */
+  int32_t z_offset;
+  int32_t nz_global;
+  double reserved[7];
 } capaz_params;
 
 /* Field identifiers for capaz_set_field / capaz_get_field. */
@@ -191,9 +196,8 @@ enum capaz_state_sel { CAPAZ_STATE_STEP_START = 0, CAPAZ_STATE_CURRENT = 1 };
 int capaz_get_derived(capaz_ctx* ctx, int field, int state_sel, void* dst, int dst_on_device, void* stream);
 /* Device-resident variants: `dev` is a device pointer of the context's device
  * holding nx*ny*nz values: float64 for capaz_set_field_device (either form;
- * the precision form encodes them), the storage type of the form for
- * capaz_get_field_device (float64 for CAPAZ_FORM_FP64, float32 for the state
- * of CAPAZ_FORM_FP32C). */
+ * the precision form encodes them); float64 for capaz_get_field_device,
+ * except m and K of CAPAZ_FORM_FP32C, which come as their float32 storage. */
 int capaz_set_field_device(capaz_ctx* ctx, int field, const void* dev, void* stream);
 int capaz_get_field_device(capaz_ctx* ctx, int field, void* dev, void* stream);
 
@@ -245,6 +249,16 @@ int64_t capaz_batch_launch_count(const capaz_batch* b);
 int64_t capaz_launch_count(const capaz_ctx* ctx);
 /* Synchronises the context's device and reports any pending CUDA error. */
 int capaz_sync(capaz_ctx* ctx);
+
+/* ---- z-slab decomposition (multi-GPU) -----------------------------------
+ * One z-plane k of a state field of the current state as float64 in device
+ * memory (nx*ny values, index i + j*nx); the precision form decodes /
+ * encodes with the context's reference state.  A slab of a decomposed grid
+ * (capaz_params.z_offset / nz_global) exchanges its first and last owned
+ * planes with its neighbours after every step and writes theirs into its
+ * halo planes (P_S_exchange, mpi.cpp:113-294, once per step). */
+int capaz_get_plane(capaz_ctx* ctx, int field, int k, double* dst_device, void* stream);
+int capaz_set_plane(capaz_ctx* ctx, int field, int k, const double* src_device, void* stream);
 
 /* ---- heterogeneous media -------------------------------------------------
  * capaz_read_permeability_file: the permeability file of load_permeability

@@ -193,9 +193,13 @@ struct WorkT {
 };
 using Work = WorkT<double>;
 
+// |I - NX/2| <= SOURCE and |K - NZ/2| <= SOURCE in global indices (a z-slab
+// of a decomposed grid has its own plane 0 at global index z_offset).
 inline bool in_window(const capaz_params* p, int i, int k) {
-  return (i >= p->nx / 2 - p->source) && (i <= p->nx / 2 + p->source) && (k >= p->nz / 2 - p->source) &&
-         (k <= p->nz / 2 + p->source);
+  const int nzg = p->nz_global > 0 ? p->nz_global : p->nz;
+  const int kg = k + p->z_offset;
+  return (i >= p->nx / 2 - p->source) && (i <= p->nx / 2 + p->source) && (kg >= nzg / 2 - p->source) &&
+         (kg <= nzg / 2 + p->source);
 }
 
 template <class T>
