@@ -608,8 +608,8 @@ capaz_adjoint* capaz_adjoint_create(capaz_ctx* ctx, int nsteps, int checkpoint_e
   };
   if (!ctx) return ret(CAPAZ_ERR_INVALID_ARGUMENT, "capaz_adjoint_create: null context");
   const capaz_params& p = ctx->p;
-  if (p.phases != 2 || p.form != CAPAZ_FORM_FP64)
-    return ret(CAPAZ_ERR_UNSUPPORTED, "capaz_adjoint_create: the adjoint covers the two-phase FP64 form");
+  if (p.phases != 2 || p.form != CAPAZ_FORM_FP64 || p.model != CAPAZ_MODEL_DEFAULT)
+    return ret(CAPAZ_ERR_UNSUPPORTED, "capaz_adjoint_create: the adjoint covers the two-phase task, FP64 form");
   if (!(p.flags & CAPAZ_FLAG_PERCELL_K))
     return ret(CAPAZ_ERR_UNSUPPORTED, "capaz_adjoint_create: needs CAPAZ_FLAG_PERCELL_K (gradient per cell)");
   if (nsteps < 1 || checkpoint_every < 1 || obs_every < 1 || nobs < 0 || (nobs > 0 && !obs_cells) ||

@@ -253,7 +253,7 @@ capaz_batch* capaz_batch_create(const capaz_params* params, int count, int devic
   const capaz_params& p0 = params[0];
   for (int q = 0; q < count; q++) {
     const capaz_params& p = params[q];
-    const bool same = p.phases == 2 && p.form == p0.form && p.flags == p0.flags &&
+    const bool same = p.phases == 2 && p.model == CAPAZ_MODEL_DEFAULT && p.form == p0.form && p.flags == p0.flags &&
                       (p.lambda == 2.0) == (p0.lambda == 2.0) && (p.P_d == 0.) == (p0.P_d == 0.);
     // Precision-form batches run the TMA-staged kernel: nx % 4 == 0, P_d = 0,
     // lambda = 2, and one set of physics constants for all instances.

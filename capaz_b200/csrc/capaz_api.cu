@@ -121,6 +121,16 @@ Step2Const make_step2_const(const capaz_params& p) {
   return c;
 }
 
+BLConst make_bl_const(const capaz_params& p) {
+  BLConst b;
+  memset(&b, 0, sizeof b);
+  b.c = make_step2_const(p);
+  b.Q = p.Q;
+  b.injwell_Pw = p.injwell_Pw;
+  b.outwell_Pw = p.outwell_Pw;
+  return b;
+}
+
 Step2FConst make_step2f_const(const capaz_params& p, double S_ref) {
   const Step2Const d = make_step2_const(p);
   Step2FConst c;
@@ -271,6 +281,20 @@ Step3Const make_step3_const(const capaz_params& p) {
 void reference_init_host(const capaz_params& p, const double* m, double* Pw, double* Sw, double* Sn, double* Pn,
                          double* Pg) {
   const long long sy = p.nx, sz = (long long)p.nx * p.ny, n = sz * p.nz;
+  if (p.model == CAPAZ_MODEL_BUCKLEY_LEVERETT) {
+    // Buckley-Leverett data_initialization (b-l.cpp:173-219): uniform
+    // BACKGROUND_Sn; BACKGROUND_Pw on the top row and down each column the
+    // weight of the cell itself, taken with the reference densities.
+    for (int i = 0; i < p.nx; i++)
+      for (int j = 0; j < p.ny; j++)
+        for (int k = 0; k < p.nz; k++) {
+          long long l = i + j * sy + (long long)k * sz;
+          Sn[l] = p.background_Sn;
+          double ro_g_dy = (p.ro0_n * Sn[l] + p.ro0_w * (1 - Sn[l])) * (m[l]) * (p.g_const) * (p.hy);
+          Pw[l] = (j == 0) ? p.background_Pw : Pw[l - sy] + ro_g_dy;
+        }
+    return;
+  }
   if (p.phases == 2) {
     std::vector<double> ro_w(n), ro_n(n);
     for (int i = 0; i < p.nx; i++)
@@ -407,6 +431,13 @@ int capaz_params_from_ini(const char* path, capaz_params* p) {
     else if (name == "S_N_BACKGROUND") p->S_n_background = d;
     else if (name == "PERCELL_K") p->flags = n ? (p->flags | CAPAZ_FLAG_PERCELL_K) : (p->flags & ~CAPAZ_FLAG_PERCELL_K);
     else if (name == "PHASES") p->phases = n;
+    // Buckley-Leverett task keys (main.cpp:1436-1480).
+    else if (name == "Q") p->Q = d;
+    else if (name == "BACKGROUND_Pw") p->background_Pw = d;
+    else if (name == "BACKGROUND_Sn") p->background_Sn = d;
+    else if (name == "INJECTION_WELL_Pw") p->injwell_Pw = d;
+    else if (name == "OUTPUT_WELL_Pw") p->outwell_Pw = d;
+    else if (name == "MODEL") p->model = n;
   }
   fclose(f);
   return CAPAZ_OK;
@@ -435,6 +466,17 @@ int capaz_params_validate(const capaz_params* p) {
   if (!(p->mu_w > 0) || !(p->mu_n > 0) || !(p->P_atm > 0) || !(p->lambda != 0))
     return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "mu, P_atm must be > 0 and lambda != 0");
   if (!(p->K0 > 0)) return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "K_0 must be > 0");
+  if (p->model != CAPAZ_MODEL_DEFAULT && p->model != CAPAZ_MODEL_BUCKLEY_LEVERETT)
+    return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "unknown model %d", p->model);
+  if (p->model == CAPAZ_MODEL_BUCKLEY_LEVERETT && (p->phases != 2 || p->form != CAPAZ_FORM_FP64))
+    return fail(nullptr, CAPAZ_ERR_UNSUPPORTED, "the Buckley-Leverett task is two-phase, FP64 form");
+  // The injection and production well blocks (2x2 corners, b-l.cpp:221-237)
+  // must neither overlap nor be the basic coordinate of a non-well boundary
+  // cell; with nx, ny >= 4 the boundary rules need no particular cell order.
+  if (p->model == CAPAZ_MODEL_BUCKLEY_LEVERETT && (p->nx < 4 || p->ny < 4))
+    return fail(nullptr, CAPAZ_ERR_UNSUPPORTED_GRID, "the Buckley-Leverett task needs nx, ny >= 4");
+  if (p->model == CAPAZ_MODEL_BUCKLEY_LEVERETT && (p->flags & CAPAZ_FLAG_DIAGNOSTICS))
+    return fail(nullptr, CAPAZ_ERR_UNSUPPORTED, "diagnostics are not built for the Buckley-Leverett task");
   return CAPAZ_OK;
 }
 

@@ -88,6 +88,7 @@ struct capaz_ctx {
 
 namespace capaz {
 Step2Const make_step2_const(const capaz_params& p);
+BLConst make_bl_const(const capaz_params& p);
 Step2FConst make_step2f_const(const capaz_params& p, double S_ref);
 Step3Const make_step3_const(const capaz_params& p);
 PhysF make_physf(const capaz_params& p);

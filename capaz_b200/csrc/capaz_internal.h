@@ -189,4 +189,15 @@ cudaError_t launch_derived2_fp64(const Step2Const& c, int field, const double* P
                                  cudaStream_t s);
 int step2_grid_blocks(const Step2Const& c);
 
+// Buckley-Leverett task (step_bl.cu): the two-phase constants plus the
+// wells' rate and pressures.
+struct BLConst {
+  Step2Const c;
+  double Q, injwell_Pw, outwell_Pw;
+};
+cudaError_t launch_step_bl(const BLConst& b, const double* Pw_in, const double* Sn_in, double* Pw_out, double* Sn_out,
+                           const double* m, const double* K, bool percell_k, unsigned int* err, cudaStream_t s);
+cudaError_t launch_derived_bl(const BLConst& b, int field, const double* Pw, const double* Sn, const double* m,
+                              const double* K, bool percell_k, double* out, cudaStream_t s);
+
 }  // namespace capaz

@@ -14,6 +14,20 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
   if (e != cudaSuccess) return fail_cuda(e, "cudaSetDevice");
   if (nsteps == 0) return CAPAZ_OK;
   const bool diag = (p.flags & CAPAZ_FLAG_DIAGNOSTICS) != 0;
+  if (p.model == CAPAZ_MODEL_BUCKLEY_LEVERETT) {
+    const BLConst b = make_bl_const(p);
+    const bool percell = (p.flags & CAPAZ_FLAG_PERCELL_K) != 0;
+    for (int t = 0; t < nsteps; t++) {
+      const int nxt = cur ^ 1;
+      e = launch_step_bl(b, (const double*)state[cur][0], (const double*)state[cur][1], (double*)state[nxt][0],
+                         (double*)state[nxt][1], (const double*)m, (const double*)K, percell, err_flag, s);
+      launches += 2;
+      if (e != cudaSuccess) return fail_cuda(e, "step_bl launch");
+      cur = nxt;
+      steps_done++;
+    }
+    return CAPAZ_OK;
+  }
   if (p.phases == 2 && p.form == CAPAZ_FORM_FP64) {
     const Step2Const c = make_step2_const(p);
     if (diag && !diag_partials) {
@@ -138,6 +152,18 @@ int capaz_ctx::derived(int field, cudaStream_t s, bool from_current) {
   if (st) return st;
   // Start-of-step state of the last step (the current state before any step).
   const int src = (steps_done > 0 && !from_current) ? (cur ^ 1) : cur;
+  if (p.model == CAPAZ_MODEL_BUCKLEY_LEVERETT) {
+    if (field == CAPAZ_FIELD_S_G || field == CAPAZ_FIELD_RO_G || field == CAPAZ_FIELD_XI_G ||
+        field == CAPAZ_FIELD_UX_G || field == CAPAZ_FIELD_UY_G || field == CAPAZ_FIELD_UZ_G ||
+        field == CAPAZ_FIELD_ROS_G || field == CAPAZ_FIELD_ROS_G_OLD || field == CAPAZ_FIELD_P_G)
+      return fail_msg(CAPAZ_ERR_INVALID_ARGUMENT, "gas fields exist in three-phase only");
+    cudaError_t e = launch_derived_bl(make_bl_const(p), field, (const double*)state[src][0],
+                                      (const double*)state[src][1], (const double*)m, (const double*)K,
+                                      (p.flags & CAPAZ_FLAG_PERCELL_K) != 0, scratch, s);
+    launches++;
+    if (e != cudaSuccess) return fail_cuda(e, "derived launch");
+    return CAPAZ_OK;
+  }
   if (p.phases == 2 && p.form == CAPAZ_FORM_FP64) {
     const Step2Const c = make_step2_const(p);
     const bool percell = (p.flags & CAPAZ_FLAG_PERCELL_K) != 0;

@@ -40,7 +40,7 @@ int fetch(capaz_ctx* ctx, int field, std::vector<double>& out) {
 }
 
 struct PlotFields {
-  std::vector<double> Pw, Sn, Sw, Sg, m, uxw, uyw, uzw, uxn, uyn, uzn, uxg, uyg, uzg;
+  std::vector<double> Pw, Sn, Sw, Sg, m, K, uxw, uyw, uzw, uxn, uyn, uzn, uxg, uyg, uzg;
 };
 
 // One row of print_plot_row for cell l = (i, j, k).
@@ -49,7 +49,16 @@ void plot_row(const capaz_params& p, const PlotFields& F, int i, int j, int k, s
   const long long l = i + (long long)j * p.nx + (long long)k * p.nx * p.ny;
   const int I = i, J = p.ny - 1 - j, K = k;
   int n;
-  if (p.phases == 2) {
+  if (p.model == CAPAZ_MODEL_BUCKLEY_LEVERETT) {
+    // The B_L branch of print_plot_row (main.cpp:769-779): S_w, u_y unflipped
+    // in the planar row, the permeability instead of the porosity.
+    if (p.nz < 2)
+      n = snprintf(buf, sizeof buf, "%.2e %.2e %.3e %.3e %.3e %.3e %.3e\n", I * (p.hx), J * (p.hy), 1. - F.Sn[l],
+                   F.Pw[l], F.uxn[l], F.uyn[l], F.K[l]);
+    else
+      n = snprintf(buf, sizeof buf, "%.2e %.2e %.2e %.3e %.3e %.3e %.3e %.3e %.3e\n", I * (p.hx), K * (p.hz),
+                   J * (p.hy), 1 - F.Sn[l], F.Pw[l], F.uxn[l], F.uzn[l], (-1) * F.uyn[l], F.K[l]);
+  } else if (p.phases == 2) {
     if (p.nz < 2)
       n = snprintf(buf, sizeof buf, "%.2e %.2e %.3e %.3e %.3e %.3e %.3e\n", I * (p.hx), J * (p.hy), F.Sn[l], F.Pw[l],
                    F.uxn[l], (-1) * F.uyn[l], F.m[l]);
@@ -121,6 +130,10 @@ int capaz_write_plot(capaz_ctx* ctx, const char* dir, double t) {
                          {CAPAZ_FIELD_UY_W, &F.uyw}, {CAPAZ_FIELD_UZ_W, &F.uzw}, {CAPAZ_FIELD_UX_G, &F.uxg},
                          {CAPAZ_FIELD_UY_G, &F.uyg}, {CAPAZ_FIELD_UZ_G, &F.uzg}};
     want.insert(want.end(), std::begin(more), std::end(more));
+  }
+  if (p.model == CAPAZ_MODEL_BUCKLEY_LEVERETT) {
+    if (p.flags & CAPAZ_FLAG_PERCELL_K) want.push_back({CAPAZ_FIELD_K, &F.K});
+    else F.K.assign(ctx->n, p.K0);
   }
   for (const Want& w : want) {
     // Before the first step the reference's velocity arrays hold no values

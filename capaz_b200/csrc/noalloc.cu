@@ -192,7 +192,7 @@ extern "C" int capaz_mass_noalloc(const capaz_params* p, const double* P_w, cons
   c.rows = (int)rows;
   c.planar = p->nz == 1;
   c.S_wr = p->S_wr;
-  c.P_d = p->P_d;
+  c.P_d = p->model == CAPAZ_MODEL_BUCKLEY_LEVERETT ? 0. : p->P_d;  // the B-L task has P_n = P_w
   c.e_pk = -1. / p->lambda;
   c.ro0_w = p->ro0_w;
   c.ro0_n = p->ro0_n;

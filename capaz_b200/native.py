@@ -28,6 +28,9 @@ ERR_UNSUPPORTED = 9
 # Largest (ny-2)*max(nz-2,1) that capaz_mass_noalloc accepts.
 NOALLOC_MAX_ROWS = 131072
 
+MODEL_DEFAULT = 0
+MODEL_BUCKLEY_LEVERETT = 1
+
 FORM_FP64 = 0
 FORM_FP32C = 1
 
@@ -65,7 +68,9 @@ class Params(C.Structure):
         ("S_n_init", C.c_double), ("porosity", C.c_double), ("K0", C.c_double),
         ("timeX", C.c_double), ("P_top_offset", C.c_double), ("S_n_background", C.c_double),
         ("z_offset", C.c_int32), ("nz_global", C.c_int32),
-        ("reserved", C.c_double * 7),
+        ("model", C.c_int32), ("pad_", C.c_int32), ("Q", C.c_double), ("background_Pw", C.c_double),
+        ("background_Sn", C.c_double), ("injwell_Pw", C.c_double), ("outwell_Pw", C.c_double),
+        ("reserved", C.c_double * 1),
     ]
 
     def copy(self) -> "Params":
@@ -74,7 +79,7 @@ class Params(C.Structure):
         return q
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        return {k: getattr(self, k) for k, _ in self._fields_ if k not in ("reserved", "pad_")}
 
     @property
     def ncell(self) -> int:

@@ -26,6 +26,21 @@ def default_params(**overrides) -> Params:
     return p
 
 
+def buckley_leverett_params(**overrides) -> Params:
+    """The reference's Backley-Leverett/defines.ini (its B_L build): the
+    Buckley-Leverett model, fluids, wells and 100 x 100 grid, then
+    `overrides`.  K per cell comes from a permeability file
+    (Simulation.load_permeability, with FLAG_PERCELL_K)."""
+    base = dict(model=native.MODEL_BUCKLEY_LEVERETT, nx=100, ny=100, nz=1, hx=15.0, hy=15.0, hz=10.0,
+                dt=86400.0, timeX=1.5e6, source=0, Q=3.5e-6, injwell_Pw=2e5, outwell_Pw=0.9e5,
+                background_Pw=3e5, background_Sn=0.7, beta_w=4.35e-5, beta_n=1.0e-5, K0=6.64e-11,
+                mu_w=1.2e-3, mu_n=6e-3, ro0_w=1e3, ro0_n=0.848978559e3, lambda_=2.7, S_wr=0.2, S_n_gr=0.4,
+                porosity=0.2, P_d=755.0, P_atm=100000.0, g_const=0.0, newton_iterations=10,
+                flags=native.FLAG_PERCELL_K)
+    base.update(overrides)
+    return default_params(**base)
+
+
 def params_from_ini(path: str, base: Params | None = None) -> Params:
     """Parses a defines.ini the way the reference's read_defines does."""
     lib = native.load()
@@ -50,13 +65,14 @@ def write_ini(p: Params, path: str, extensions: bool = True) -> None:
         ("S_N_GR", p.S_n_gr), ("S_W_GR", p.S_w_gr), ("S_W_INIT", p.S_w_init), ("S_N_INIT", p.S_n_init),
         ("SOURCE", p.source), ("ITERATIONS", p.newton_iterations), ("TIMEX", p.timeX),
         ("SAVE_PLOTS", 1000000), ("PRINT_SCREEN", 1000000),
-        ("Q", 0.0), ("BACKGROUND_Pw", p.P_atm), ("BACKGROUND_Sn", 0.0),
-        ("INJECTION_WELL_Pw", p.P_atm), ("INJECTION_WELL_Sn", 0.0),
-        ("OUTPUT_WELL_Pw", p.P_atm), ("OUTPUT_WELL_Sn", 0.0),
+        ("Q", p.Q), ("BACKGROUND_Pw", p.background_Pw), ("BACKGROUND_Sn", p.background_Sn),
+        ("INJECTION_WELL_Pw", p.injwell_Pw), ("INJECTION_WELL_Sn", 0.0),
+        ("OUTPUT_WELL_Pw", p.outwell_Pw), ("OUTPUT_WELL_Sn", 0.0),
     ]
     if extensions:
         keys += [("P_TOP_OFFSET", p.P_top_offset), ("S_N_BACKGROUND", p.S_n_background),
-                 ("PERCELL_K", 1 if p.flags & native.FLAG_PERCELL_K else 0), ("PHASES", p.phases)]
+                 ("PERCELL_K", 1 if p.flags & native.FLAG_PERCELL_K else 0), ("PHASES", p.phases),
+                 ("MODEL", p.model)]
     with open(path, "w") as f:
         f.write("# written by capaz_b200.simulation.write_ini\n")
         for k, v in keys:

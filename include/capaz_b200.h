@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define CAPAZ_ABI_VERSION 2
+#define CAPAZ_ABI_VERSION 3
 
 /* ---- status codes ------------------------------------------------------ */
 enum capaz_status {
@@ -106,8 +106,27 @@ typedef struct capaz_params {
    * |k - NZ/2| <= SOURCE in global coordinates.  0, 0: the whole grid. */
   int32_t z_offset;
   int32_t nz_global;
-  double reserved[7];
+  /* ---- model selection and the Buckley-Leverett task (B_L build,
+   * Backley-Leverett/b-l.cpp); read from defines.ini as Q, BACKGROUND_Pw,
+   * BACKGROUND_Sn, INJECTION_WELL_Pw, OUTPUT_WELL_Pw (main.cpp:1436-1480) ---- */
+  int32_t model;             /* enum capaz_model                              */
+  int32_t pad_;
+  double Q;                  /* Q: well rate                                  */
+  double background_Pw;      /* BACKGROUND_Pw: P_w of the top row at t = 0    */
+  double background_Sn;      /* BACKGROUND_Sn: initial S_n                    */
+  double injwell_Pw;         /* INJECTION_WELL_Pw                             */
+  double outwell_Pw;         /* OUTPUT_WELL_Pw                                */
+  double reserved[1];
 } capaz_params;
+
+/* Physics of the step (capaz_params.model). */
+enum capaz_model {
+  CAPAZ_MODEL_DEFAULT = 0, /* two-phase (two-phase.cpp) or three-phase (three-phase.cpp) by `phases` */
+  /* Buckley-Leverett task (Backley-Leverett/b-l.cpp): two phases, piecewise
+   * relative permeabilities, per-cell K, an injection and a production well
+   * in opposite corners of every z-plane; FP64 form only. */
+  CAPAZ_MODEL_BUCKLEY_LEVERETT = 1
+};
 
 /* Field identifiers for capaz_set_field / capaz_get_field. */
 enum capaz_field {

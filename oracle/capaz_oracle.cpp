@@ -338,6 +338,180 @@ void step2(const capaz_params* p, const Grid& g, T* P_w, T* S_n, const T* m, con
 }
 
 // ---------------------------------------------------------------------------
+// Buckley-Leverett task (B_L build: Backley-Leverett/b-l.cpp with cpu.cpp).
+
+// assing_k (b-l.cpp:5-55), the "IPM" relative permeabilities of S_w.
+inline void bl_relperm(double S_w, double* k_w, double* k_n) {
+  const double S_sv = 0.1, S_zv = 0.8, S_1 = 0.70324;
+  if ((S_sv <= S_w) && (S_w <= S_zv))
+    *k_n = ((S_zv - S_w) / (S_zv - S_sv)) * ((S_zv - S_w) / (S_zv - S_sv));
+  else if ((0 <= S_w) && (S_w <= S_sv))
+    *k_n = 1.;
+  else
+    *k_n = 0.;
+  if ((S_sv <= S_w) && (S_w <= S_1))
+    *k_w = ((S_w - S_sv) / (S_zv - S_sv)) * ((S_w - S_sv) / (S_zv - S_sv));
+  else if ((0 <= S_w) && (S_w <= S_sv))
+    *k_w = 0.;
+  else if ((S_1 <= S_w) && (S_w <= S_zv))
+    *k_w = 0.8 * pow((S_w - S_sv) / (S_zv - S_sv), 0.5);
+  else
+    *k_w = 1.;
+}
+
+// is_injection_well / is_output_well (b-l.cpp:221-237): two 2x2 corners of
+// every z-plane.
+inline bool bl_injection(const Grid& g, int i, int j) {
+  return ((i == 1) && (j == 1)) || ((i == 0) && (j == 0)) || ((i == 1) && (j == 0)) || ((i == 0) && (j == 1));
+}
+inline bool bl_output(const Grid& g, int i, int j) {
+  return ((i == g.nx - 2) && (j == g.ny - 2)) || ((i == g.nx - 1) && (j == g.ny - 1)) ||
+         ((i == g.nx - 1) && (j == g.ny - 2)) || ((i == g.nx - 2) && (j == g.ny - 1));
+}
+
+// data_initialization (b-l.cpp:173-219): S_n = BACKGROUND_Sn, P_w from
+// BACKGROUND_Pw at the top down each column, the weight taken with the
+// reference densities and the cell's own S_n and m.
+void init_bl(const capaz_params* p, const Grid& g, const double* m, double* P_w, double* S_n) {
+  for (int i = 0; i < g.nx; i++)
+    for (int j = 0; j < g.ny; j++)
+      for (int k = 0; k < g.nz; k++) {
+        long l = g.at(i, j, k);
+        S_n[l] = p->background_Sn;
+        double ro_g_dy = (p->ro0_n * S_n[l] + p->ro0_w * (1 - S_n[l])) * (m[l]) * (p->g_const) * (p->hy);
+        if (j == 0) P_w[l] = p->background_Pw;
+        else P_w[l] = P_w[l - g.sy] + ro_g_dy;
+      }
+}
+
+void step_bl(const capaz_params* p, const Grid& g, double* P_w, double* S_n, const double* m, const double* K,
+             Work& w) {
+  double *S_w = w.S_w.data(), *P_n = w.P_n.data(), *ro_w = w.ro_w.data(), *ro_n = w.ro_n.data();
+  double *Xi_w = w.Xi_w.data(), *Xi_n = w.Xi_n.data();
+  double *roS_w = w.roS_w.data(), *roS_n = w.roS_n.data();
+  double *roS_w_old = w.roS_w_old.data(), *roS_n_old = w.roS_n_old.data();
+
+#pragma omp parallel for schedule(static)
+  for (long l = 0; l < g.n; l++) S_w[l] = 1. - S_n[l];
+
+  // assign_P_Xi (b-l.cpp:57-72) and assign_ro (cpu.cpp).
+#pragma omp parallel for schedule(static)
+  for (long l = 0; l < g.n; l++) {
+    double k_w = 0., k_n = 0.;
+    bl_relperm(1. - S_n[l], &k_w, &k_n);
+    P_n[l] = P_w[l];
+    Xi_w[l] = -1. * Kc(p, K, l) * k_w / p->mu_w;
+    Xi_n[l] = -1. * Kc(p, K, l) * k_n / p->mu_n;
+    ro_w[l] = p->ro0_w * (1. + (p->beta_w) * (P_w[l] - p->P_atm));
+    ro_n[l] = p->ro0_n * (1. + (p->beta_n) * (P_n[l] - p->P_atm));
+  }
+
+  // assign_roS_nr (cpu.cpp:619-731) with wells_q (b-l.cpp:239-262).
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        if (!g.interior(i, j, k)) continue;
+        long l = g.at(i, j, k);
+        if (!m[l]) continue;
+        double q_w = 0., q_n = 0.;
+        if (bl_injection(g, i, j)) {
+          q_w = p->Q;
+          q_n = 0.;
+        }
+        if (bl_output(g, i, j)) {
+          double k_w = 0., k_n = 0.;
+          bl_relperm(1. - S_n[l], &k_w, &k_n);
+          double F_bl = (k_w / p->mu_w) / (k_w / p->mu_w + k_n / p->mu_n);
+          q_w = -1. * p->Q * F_bl;
+          q_n = -1. * p->Q * (1. - F_bl);
+        }
+        roS_w[l] = ro_w[l] * (1. - S_n[l]);
+        roS_n[l] = ro_n[l] * S_n[l];
+        double x1, x2, fx_w, fy_w, fz_w, fx_n, fy_n, fz_n;
+        if (g.nz < 2) {
+          fz_w = 0.;
+          fz_n = 0.;
+        } else {
+          x2 = -1. * rdiff(P_w, l, g.sz, p->hz);
+          x1 = -1. * ldiff(P_w, l, g.sz, p->hz);
+          fz_w = directed(x1, x2, Xi_w, ro_w, l, g.sz, p->hz);
+          x2 = -1. * rdiff(P_n, l, g.sz, p->hz);
+          x1 = -1. * ldiff(P_n, l, g.sz, p->hz);
+          fz_n = directed(x1, x2, Xi_n, ro_n, l, g.sz, p->hz);
+        }
+        if (g.nx < 2) {
+          fx_w = 0.;
+          fx_n = 0.;
+        } else {
+          x2 = -1. * rdiff(P_w, l, g.sx, p->hx);
+          x1 = -1. * ldiff(P_w, l, g.sx, p->hx);
+          fx_w = directed(x1, x2, Xi_w, ro_w, l, g.sx, p->hx);
+          x2 = -1. * rdiff(P_n, l, g.sx, p->hx);
+          x1 = -1. * ldiff(P_n, l, g.sx, p->hx);
+          fx_n = directed(x1, x2, Xi_n, ro_n, l, g.sx, p->hx);
+        }
+        x2 = -1. * rdiff(P_w, l, g.sy, p->hy) + p->g_const * (ro_w[l]);
+        x1 = -1. * ldiff(P_w, l, g.sy, p->hy) + p->g_const * (ro_w[l]);
+        fy_w = directed(x1, x2, Xi_w, ro_w, l, g.sy, p->hy);
+        x2 = -1. * rdiff(P_n, l, g.sy, p->hy) + p->g_const * (ro_n[l]);
+        x1 = -1. * ldiff(P_n, l, g.sy, p->hy) + p->g_const * (ro_n[l]);
+        fy_n = directed(x1, x2, Xi_n, ro_n, l, g.sy, p->hy);
+        double A1 = roS_w[l] - (p->dt / m[l]) * (-q_w + fx_w + fy_w + fz_w);
+        double A2 = roS_n[l] - (p->dt / m[l]) * (-q_n + fx_n + fy_n + fz_n);
+        roS_w_old[l] = roS_w[l];
+        roS_n_old[l] = roS_n[l];
+        roS_w[l] = A1;
+        roS_n[l] = A2;
+      }
+
+  // Newton (b-l.cpp:74-102): no capillary pressure.
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        if (!g.interior(i, j, k)) continue;
+        long l = g.at(i, j, k);
+        double Pw = P_w[l], Sn = S_n[l];
+        for (int it = 1; it <= p->newton_iterations; it++) {
+          double F1 = p->ro0_w * (1. + (p->beta_w) * (Pw - p->P_atm)) * (1. - Sn) - roS_w[l];
+          double F2 = p->ro0_n * (1. + (p->beta_n) * (Pw - p->P_atm)) * Sn - roS_n[l];
+          double F1P = p->ro0_w * (p->beta_w) * (1 - Sn);
+          double F2P = p->ro0_n * (p->beta_n) * Sn;
+          double F1S = (-1) * (p->ro0_w) * (1 + (p->beta_w) * (Pw - p->P_atm));
+          double F2S = p->ro0_n * (1 + (p->beta_n) * (Pw - p->P_atm));
+          double det = F1P * F2S - F1S * F2P;
+          double nPw = Pw - (1. / det) * (F2S * F1 - F1S * F2);
+          double nSn = Sn - (1. / det) * (F1P * F2 - F2P * F1);
+          Pw = nPw;
+          Sn = nSn;
+        }
+        P_w[l] = Pw;
+        S_n[l] = Sn;
+      }
+
+  // boundary_conditions: Border_S and Border_P (b-l.cpp:104-171) on every
+  // cell (interior cells are their own basic coordinate), then the wells'
+  // pressures.
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        long l1 = g.basic(i, j, k);
+        long l = g.at(i, j, k);
+        S_n[l] = S_n[l1];
+        if ((j != 0) && (j != g.ny - 1)) {
+          P_w[l] = P_w[l1];
+        } else {
+          double ro_g_dy = (p->ro0_n * S_n[l] + p->ro0_w * (1 - S_n[l])) * (m[l]) * (p->g_const) * (p->hy);
+          P_w[l] = P_w[l1] + ro_g_dy;
+        }
+        if (bl_injection(g, i, j)) P_w[l] = p->injwell_Pw;
+        if (bl_output(g, i, j)) P_w[l] = p->outwell_Pw;
+      }
+}
+
+// ---------------------------------------------------------------------------
 // Three-phase step (CPU physics).
 void step3(const capaz_params* p, const Grid& g, double* P_w, double* S_w, double* S_n, double* P_n,
            double* P_g, const double* m, const double* K, Work& w) {
@@ -603,7 +777,8 @@ int oracle_init(const capaz_params* p, const double* m_in, double* m, double* P_
   Grid g(p);
   if (p->phases == 2) {
     for (long l = 0; l < g.n; l++) m[l] = m_in ? m_in[l] : p->porosity;
-    init2(p, g, m, P_w, S_n);
+    if (p->model == CAPAZ_MODEL_BUCKLEY_LEVERETT) init_bl(p, g, m, P_w, S_n);
+    else init2(p, g, m, P_w, S_n);
   } else {
     for (long l = 0; l < g.n; l++) {
       m[l] = m_in ? m_in[l] : p->porosity;
@@ -657,7 +832,8 @@ int oracle_step(const capaz_params* p, int nsteps, double* P_w, double* S_w, dou
       Pw0.assign(P_w, P_w + n);
       w.keep_u_pressures = (p->phases == 3);
     }
-    if (p->phases == 2) step2(p, g, P_w, S_n, m, K, w);
+    if (p->model == CAPAZ_MODEL_BUCKLEY_LEVERETT) step_bl(p, g, P_w, S_n, m, K, w);
+    else if (p->phases == 2) step2(p, g, P_w, S_n, m, K, w);
     else step3(p, g, P_w, S_w, S_n, P_n, P_g, m, K, w);
   }
   if (derived && nsteps > 0) {
@@ -716,7 +892,8 @@ int oracle_step(const capaz_params* p, int nsteps, double* P_w, double* S_w, dou
           double rw = p->ro0_w * (1. + (p->beta_w) * (Pw - p->P_atm));
           if (p->phases == 2) {
             double S_e = (1 - Sn - p->S_wr) / (1 - p->S_wr);
-            double Pk = (p->P_d != 0.) ? p->P_d * pow(S_e, (-1.) / p->lambda) : 0.;
+            double Pk = (p->P_d != 0. && p->model != CAPAZ_MODEL_BUCKLEY_LEVERETT)
+                            ? p->P_d * pow(S_e, (-1.) / p->lambda) : 0.;
             double rn = p->ro0_n * (1. + (p->beta_n) * (Pw + Pk - p->P_atm));
             double F1 = rw * (1. - Sn) - w.roS_w[l];
             double F2 = rn * Sn - w.roS_n[l];

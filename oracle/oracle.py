@@ -144,6 +144,9 @@ def ref_ini_text(p: Params) -> str:
         "S_N_GR": p.S_n_gr, "S_W_GR": p.S_w_gr, "S_W_INIT": p.S_w_init, "S_N_INIT": p.S_n_init,
         "SOURCE": p.source, "ITERATIONS": p.newton_iterations, "TIMEX": p.timeX,
         "SAVE_PLOTS": 1000000, "PRINT_SCREEN": 1000000,
+        "Q": p.Q, "BACKGROUND_Pw": p.background_Pw, "BACKGROUND_Sn": p.background_Sn,
+        "INJECTION_WELL_Pw": p.injwell_Pw, "INJECTION_WELL_Sn": 0.0,
+        "OUTPUT_WELL_Pw": p.outwell_Pw, "OUTPUT_WELL_Sn": 0.0,
     }
     lines = ["# defines.ini for the reference harness"]
     for k, v in vals.items():
@@ -151,7 +154,9 @@ def ref_ini_text(p: Params) -> str:
     return "\n".join(lines) + "\n"
 
 
-def ref_binary(phases: int) -> str:
+def ref_binary(phases: int, model: int = 0) -> str:
+    if model == 1:
+        return os.path.join(REF_DIR, "capaz_ref_bl")
     return os.path.join(REF_DIR, "capaz_ref_2ph" if phases == 2 else "capaz_ref_3ph")
 
 
@@ -165,18 +170,25 @@ REF_DERIVED_3PH = REF_DERIVED_2PH + ["S_g", "ro_g", "ux_g", "uy_g", "uz_g", "Xi_
 
 
 def ref_run(p: Params, nsteps: int, state: dict | None = None, m: np.ndarray | None = None,
-            binary: str | None = None, env: dict | None = None, derived: bool = False) -> dict:
+            binary: str | None = None, env: dict | None = None, derived: bool = False,
+            noise: str | None = None) -> dict:
     """Runs the reference's own CPU time step (or, with `binary`, the same
     harness linked to another backend) for nsteps from `state` (None: the
-    reference's data_initialization).  Returns the final state and timing."""
-    if p.P_top_offset != 0.0 or (p.phases == 2 and p.S_n_background != 0.0) or (p.flags & 1):
+    reference's data_initialization).  Returns the final state and timing.
+    The Buckley-Leverett build reads its permeability from `noise` (a file in
+    load_permeability's format; K_0 everywhere without one)."""
+    bl = p.model == 1
+    if p.P_top_offset != 0.0 or (p.phases == 2 and p.S_n_background != 0.0) or ((p.flags & 1) and not bl):
         raise ValueError("the reference has no P_top_offset / S_n_background / per-cell K")
-    exe = binary or ref_binary(p.phases)
+    exe = binary or ref_binary(p.phases, p.model)
     sh = _shape(p)
     n = p.nx * p.ny * p.nz
     with tempfile.TemporaryDirectory() as wd:
         with open(os.path.join(wd, "defines.ini"), "w") as f:
             f.write(ref_ini_text(p))
+        if noise is not None:
+            with open(noise, "rb") as src, open(os.path.join(wd, "noise.dat"), "wb") as dst:
+                dst.write(src.read())
         in_path = "-"
         if state is not None:
             in_path = os.path.join(wd, "in.bin")

@@ -37,6 +37,7 @@ def load_golden(name: str):
 GOLDEN_2PH = ["g2_default_15x15x1", "g2_3d_pd0_12x10x7", "g2_3d_pd_12x10x7", "g2_planar_17x13x1",
               "g2_min_3x3x3"]
 GOLDEN_3PH = ["g3_column_1x15x1", "g3_3d_9x8x6"]
+GOLDEN_BL = ["gbl_planar_20x15x1", "gbl_3d_gravity_12x10x6"]
 
 
 def interior(a: np.ndarray) -> np.ndarray:

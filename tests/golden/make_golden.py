@@ -1,6 +1,7 @@
 """Generates tests/golden/*.npz from the reference's own CPU implementation.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py        # every fixture
+    python tests/golden/make_golden.py bl     # the Buckley-Leverett ones only
 
 Each fixture holds the parameter set, the input state (or none: the
 reference's data_initialization), and the reference's outputs after N steps:
@@ -102,5 +103,46 @@ def main():
     save("g3_3d_9x8x6", p3, 30, state, m, True)
 
 
+def bl_params(nx, ny, nz, g, dt):
+    """The reference's Backley-Leverett/defines.ini fluids and wells."""
+    return default_params(nx=nx, ny=ny, nz=nz, dt=dt, model=1, Q=3.5e-6, background_Pw=3e5,
+                          background_Sn=0.7, injwell_Pw=2e5, outwell_Pw=0.9e5, beta_w=4.35e-5, beta_n=1e-5,
+                          mu_w=1.2e-3, mu_n=6e-3, ro0_n=848.978559, porosity=0.2, K0=6.64e-11, g_const=g,
+                          hx=15.0, hy=15.0, hz=10.0, newton_iterations=10, source=0, P_d=755.0, lambda_=2.7)
+
+
+def save_bl(name, p, nsteps, seed):
+    """A Buckley-Leverett case from the reference's data_initialization with
+    K from a permeability file written here (K itself as the reference's
+    loader reads it, through oracle/_ref/capaz_ref_loadk)."""
+    import tempfile
+    import make_media_golden as mg
+    with tempfile.TemporaryDirectory() as d:
+        noise = os.path.join(d, "noise.dat")
+        vals = np.random.default_rng(seed).normal(-1.5, 0.6, size=(p.ny, p.nx))
+        mg.write_noise(noise, vals)
+        if p.nz > 1:
+            text = open(noise, "rb").read().split(b"\r\n", 1)
+            open(noise, "wb").write(f"{p.nx} {p.ny} {p.nz}".encode() + b"\r\n" + text[1])
+        K = mg.reference_K(noise, p.nx, p.ny, p.nz)
+        r = O.ref_run(p, nsteps, noise=noise)
+    out = {"params": np.array(json.dumps(p.as_dict())), "nsteps": np.array(nsteps), "K": K,
+           "out_P_w": r["P_w"], "out_S_n": r["S_n"]}
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **out)
+    print(f"{path}: {os.path.getsize(path)} bytes, ref {r['info']}")
+
+
+def main_bl():
+    if not os.path.exists(O.ref_binary(2, 1)):
+        raise SystemExit("build the reference binaries first: make -C oracle ref")
+    save_bl("gbl_planar_20x15x1", bl_params(20, 15, 1, 0.0, 2000.0), 40, 20)
+    save_bl("gbl_3d_gravity_12x10x6", bl_params(12, 10, 6, 9.81, 200.0), 30, 12)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["bl"]:
+        main_bl()
+    else:
+        main()
+        main_bl()

@@ -32,7 +32,7 @@ def test_struct_layouts():
     lib = native.load()
     assert lib.capaz_params_size() == C.sizeof(native.Params)
     assert lib.capaz_diag_size() == C.sizeof(native.Diag)
-    assert lib.capaz_abi_version() == 2
+    assert lib.capaz_abi_version() == 3
 
 
 def test_defaults_are_reference_two_phase_ini():
@@ -70,6 +70,31 @@ def test_validate_rejects_unsupported_grids():
     assert lib.capaz_params_validate(C.byref(p)) == native.OK
     p = default_params(dt=0.0)
     assert lib.capaz_params_validate(C.byref(p)) == native.ERR_INVALID_ARGUMENT
+
+
+def test_validate_buckley_leverett_model():
+    """The B-L task is the two-phase FP64 step with its own wells and
+    boundary; its well blocks need nx, ny >= 4."""
+    lib = native.load()
+    ok = dict(model=native.MODEL_BUCKLEY_LEVERETT, nx=8, ny=6, nz=1)
+    assert lib.capaz_params_validate(C.byref(default_params(**ok))) == native.OK
+    assert lib.capaz_params_validate(C.byref(default_params(**dict(ok, nz=5)))) == native.OK
+    for bad, code in [(dict(nx=3), native.ERR_UNSUPPORTED_GRID), (dict(ny=3), native.ERR_UNSUPPORTED_GRID),
+                      (dict(phases=3), native.ERR_UNSUPPORTED), (dict(form=native.FORM_FP32C), native.ERR_UNSUPPORTED),
+                      (dict(flags=native.FLAG_DIAGNOSTICS), native.ERR_UNSUPPORTED),
+                      (dict(model=7), native.ERR_INVALID_ARGUMENT)]:
+        p = default_params(**dict(ok, **bad))
+        assert lib.capaz_params_validate(C.byref(p)) == code, bad
+
+
+def test_ini_round_trip_buckley_leverett(tmp_path):
+    p = default_params(nx=20, ny=15, model=native.MODEL_BUCKLEY_LEVERETT, Q=3.5e-6, background_Pw=3e5,
+                       background_Sn=0.7, injwell_Pw=2e5, outwell_Pw=0.9e5)
+    path = str(tmp_path / "defines.ini")
+    write_ini(p, path)
+    q = params_from_ini(path, base=default_params())
+    for k, v in p.as_dict().items():
+        assert getattr(q, k) == v, k
 
 
 def test_missing_ini_is_an_error():

@@ -10,13 +10,14 @@ import pytest
 
 from conftest import ROOT
 from capaz_b200 import Simulation, native
-from capaz_b200.simulation import default_params
+from capaz_b200.simulation import buckley_leverett_params, default_params
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
 MAIN_REF = {2: os.path.join(ROOT, "oracle", "_ref", "capaz_ref_main_2ph"),
-            3: os.path.join(ROOT, "oracle", "_ref", "capaz_ref_main_3ph")}
+            3: os.path.join(ROOT, "oracle", "_ref", "capaz_ref_main_3ph"),
+            "bl": os.path.join(ROOT, "oracle", "_ref", "capaz_ref_main_bl")}
 
 
 def params3(**kw):
@@ -28,25 +29,30 @@ def params3(**kw):
     return default_params(**base)
 
 
-def reference_plots(p, tmp_path, save_every):
+def reference_plots(p, tmp_path, save_every, noise=None):
     """Runs the reference's whole program (its own main and CPU backend) and
-    returns its plot files."""
-    exe = MAIN_REF[p.phases]
+    returns its plot files.  `noise`: the permeability file of the B_L build
+    (read from ../noise.dat)."""
+    exe = MAIN_REF["bl" if p.model == native.MODEL_BUCKLEY_LEVERETT else p.phases]
     if not os.path.exists(exe):
         pytest.skip("reference whole-program binaries not built (make -C oracle ref)")
     ini = O.ref_ini_text(p).replace("SAVE_PLOTS=1000000", f"SAVE_PLOTS={save_every}")
     wd = tmp_path / "ref"
     (wd / "run").mkdir(parents=True)
     (wd / "defines.ini").write_text(ini)
+    if noise is not None:
+        (wd / "noise.dat").write_bytes(open(noise, "rb").read())
     res = subprocess.run([exe], cwd=wd / "run", capture_output=True, text=True, timeout=600)
     assert res.returncode == 0, res.stdout[-2000:] + res.stderr[-2000:]
     d = wd / "run" / "plots"
     return {f: (d / f).read_text().splitlines() for f in sorted(os.listdir(d))}
 
 
-def our_plots(p, tmp_path, save_every, nsave):
+def our_plots(p, tmp_path, save_every, nsave, noise=None):
     d = tmp_path / "ours"
     with Simulation(p) as s:
+        if noise is not None:
+            s.load_permeability(noise)
         s.init_state()
         s.write_plot(str(d), 0.0)
         for q in range(1, nsave + 1):
@@ -86,6 +92,27 @@ def test_plot_file_matches_reference_program_three_phase(tmp_path, shape):
     nx, ny, nz = shape
     p = params3(nx=nx, ny=ny, nz=nz, dt=1e-3, timeX=0.06)
     compare(reference_plots(p, tmp_path, 30), our_plots(p, tmp_path, 30, 2))
+
+
+@pytest.mark.parametrize("shape,g,dt", [((20, 15, 1), 0.0, 2000.0), ((12, 10, 6), 9.81, 200.0)])
+def test_plot_file_matches_reference_program_buckley_leverett(tmp_path, shape, g, dt):
+    """The B_L build's plot rows (S_w, P_w, u, K) with K from a noise.dat."""
+    nx, ny, nz = shape
+    p = buckley_leverett_params(nx=nx, ny=ny, nz=nz, g_const=g, dt=dt, timeX=40 * dt)
+    noise = str(tmp_path / "noise.dat")
+    write_noise(noise, np.random.default_rng(nx).normal(-1.5, 0.6, size=(ny, nx)), nz)
+    compare(reference_plots(p, tmp_path, 20, noise), our_plots(p, tmp_path, 20, 2, noise))
+
+
+def write_noise(path, values, nz=1):
+    """A permeability file: header "Nx Ny" (or "Nx Ny Nz"), then Ny rows of
+    values, CRLF line ends as the reference's sample file has them."""
+    ny, nx = values.shape
+    head = f"{nx} {ny}" if nz < 2 else f"{nx} {ny} {nz}"
+    with open(path, "wb") as f:
+        f.write((head + "\r\n").encode())
+        for row in values:
+            f.write(("".join(f"{v:.6f} " for v in row) + "\r\n").encode())
 
 
 def _state(s, phases):

@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_2PH, GOLDEN_3PH, interior, load_golden
+from conftest import GOLDEN_2PH, GOLDEN_3PH, GOLDEN_BL, interior, load_golden
 from oracle import oracle as O
 
 
@@ -32,6 +32,21 @@ def test_oracle_matches_reference_bitwise(name):
             assert np.array_equal(interior(out["derived"][f]), interior(g[key])), f
         else:
             assert np.array_equal(out["derived"][f], g[key]), f
+
+
+@pytest.mark.parametrize("name", GOLDEN_BL)
+def test_oracle_buckley_leverett_matches_reference_bitwise(name):
+    """The Buckley-Leverett task (B_L build of the reference: b-l.cpp with
+    cpu.cpp): data_initialization, then the steps, with K as the reference's
+    permeability-file loader produced it."""
+    from capaz_b200 import native
+    p, g = load_golden(name)
+    q = p.copy()
+    q.flags |= native.FLAG_PERCELL_K
+    st = O.init(q)
+    out = O.step(q, {"P_w": st["P_w"], "S_n": st["S_n"]}, int(g["nsteps"]), st["m"], g["K"])
+    assert np.array_equal(out["P_w"], g["out_P_w"])
+    assert np.array_equal(out["S_n"], g["out_S_n"])
 
 
 def test_oracle_init_matches_reference():
