@@ -94,7 +94,7 @@ def test_plot_file_matches_reference_program_three_phase(tmp_path, shape):
     compare(reference_plots(p, tmp_path, 30), our_plots(p, tmp_path, 30, 2))
 
 
-@pytest.mark.parametrize("shape,g,dt", [((20, 15, 1), 0.0, 2000.0), ((12, 10, 6), 9.81, 200.0)])
+@pytest.mark.parametrize("shape,g,dt", [((20, 15, 1), 0.0, 2000.0), ((12, 10, 6), 9.81, 50.0)])
 def test_plot_file_matches_reference_program_buckley_leverett(tmp_path, shape, g, dt):
     """The B_L build's plot rows (S_w, P_w, u, K) with K from a noise.dat."""
     nx, ny, nz = shape
