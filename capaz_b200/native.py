@@ -30,6 +30,7 @@ NOALLOC_MAX_ROWS = 131072
 
 MODEL_DEFAULT = 0
 MODEL_BUCKLEY_LEVERETT = 1
+MODEL_ENERGY = 2
 
 FORM_FP64 = 0
 FORM_FP32C = 1
@@ -47,8 +48,10 @@ FIELDS = {
     "ux_w": 14, "uy_w": 15, "uz_w": 16, "ux_n": 17, "uy_n": 18, "uz_n": 19,
     "ux_g": 20, "uy_g": 21, "uz_g": 22, "roS_w": 23, "roS_n": 24, "roS_g": 25,
     "roS_w_old": 26, "roS_n_old": 27, "roS_g_old": 28,
+    "T": 29, "H_w": 30, "H_n": 31, "H_g": 32, "H_r": 33, "E": 34, "E_new": 35,
 }
-FIELD_COUNT = 29
+FIELD_COUNT = 36
+ENERGY_FIELDS = ("T", "H_w", "H_n", "H_g", "H_r", "E", "E_new")
 
 
 class Params(C.Structure):

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define CAPAZ_ABI_VERSION 3
+#define CAPAZ_ABI_VERSION 4
 
 /* ---- status codes ------------------------------------------------------ */
 enum capaz_status {
@@ -125,7 +125,12 @@ enum capaz_model {
   /* Buckley-Leverett task (Backley-Leverett/b-l.cpp): two phases, piecewise
    * relative permeabilities, per-cell K, an injection and a production well
    * in opposite corners of every z-plane; FP64 form only. */
-  CAPAZ_MODEL_BUCKLEY_LEVERETT = 1
+  CAPAZ_MODEL_BUCKLEY_LEVERETT = 1,
+  /* Three-phase with the energy equation (THREE_PHASE + ENERGY build:
+   * energy.cpp): temperature as a fifth unknown of a 5x5 Newton per cell,
+   * temperature-dependent densities and viscosities, heat conduction and
+   * advected enthalpy; FP64 form only. */
+  CAPAZ_MODEL_ENERGY = 2
 };
 
 /* Field identifiers for capaz_set_field / capaz_get_field. */
@@ -156,7 +161,15 @@ enum capaz_field {
   CAPAZ_FIELD_ROS_W_OLD = 26, /* rho*S at the start of the step (interior)  */
   CAPAZ_FIELD_ROS_N_OLD = 27,
   CAPAZ_FIELD_ROS_G_OLD = 28,
-  CAPAZ_FIELD_COUNT = 29
+  /* energy model (CAPAZ_MODEL_ENERGY) */
+  CAPAZ_FIELD_T = 29,      /* temperature (state)                          */
+  CAPAZ_FIELD_H_W = 30,    /* enthalpies of the phases and of the rock     */
+  CAPAZ_FIELD_H_N = 31,
+  CAPAZ_FIELD_H_G = 32,
+  CAPAZ_FIELD_H_R = 33,
+  CAPAZ_FIELD_E = 34,      /* internal energy per unit volume              */
+  CAPAZ_FIELD_E_NEW = 35,  /* energy balance of the step (interior)        */
+  CAPAZ_FIELD_COUNT = 36
 };
 
 /* Per-step diagnostics (CAPAZ_FLAG_DIAGNOSTICS), reduced on the device with

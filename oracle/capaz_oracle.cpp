@@ -511,51 +511,15 @@ void step_bl(const capaz_params* p, const Grid& g, double* P_w, double* S_n, con
       }
 }
 
-// ---------------------------------------------------------------------------
-// Three-phase step (CPU physics).
-void step3(const capaz_params* p, const Grid& g, double* P_w, double* S_w, double* S_n, double* P_n,
-           double* P_g, const double* m, const double* K, Work& w) {
-  const double A = p->lambda;
-  const double den = 1. - p->S_wr - p->S_nr - p->S_gr;
-  double *S_g = w.S_g.data(), *ro_w = w.ro_w.data(), *ro_n = w.ro_n.data(), *ro_g = w.ro_g.data();
+// roS_calculation of the three-phase task, NR form (cpu.cpp:619-731 with
+// wells_q three-phase.cpp:529-550, all rates zero): the conserved updates
+// roS_p and roS_p_old on interior cells from the ro_P_Xi arrays.
+void roS3(const capaz_params* p, const Grid& g, const double* P_w, const double* S_w, const double* S_n,
+          const double* P_n, const double* P_g, const double* m, Work& w) {
+  double *ro_w = w.ro_w.data(), *ro_n = w.ro_n.data(), *ro_g = w.ro_g.data();
   double *Xi_w = w.Xi_w.data(), *Xi_n = w.Xi_n.data(), *Xi_g = w.Xi_g.data();
   double *roS_w = w.roS_w.data(), *roS_n = w.roS_n.data(), *roS_g = w.roS_g.data();
   double *roS_w_old = w.roS_w_old.data(), *roS_n_old = w.roS_n_old.data(), *roS_g_old = w.roS_g_old.data();
-
-  // S_calculation (all cells).
-#pragma omp parallel for schedule(static)
-  for (long l = 0; l < g.n; l++) S_g[l] = 1. - S_w[l] - S_n[l];
-
-  // ro_P_Xi_calculation: Xi and rho on all cells, P_n and P_g on interior
-  // cells only (three-phase.cpp:225-235).
-#pragma omp parallel for schedule(static)
-  for (int k = 0; k < g.nz; k++)
-    for (int j = 0; j < g.ny; j++)
-      for (int i = 0; i < g.nx; i++) {
-        long l = g.at(i, j, k);
-        double S_w_e = (S_w[l] - p->S_wr) / den;
-        double S_n_e = (S_n[l] - p->S_nr) / den;
-        double S_g_e = 1. - S_w_e - S_n_e;
-        double k_w = k_w3(S_w_e, A), k_g = k_g3(S_g_e, A), k_n = k_n3(S_w_e, S_n_e, A);
-        double Kl = Kc(p, K, l);
-        Xi_w[l] = (-1.) * Kl * k_w / p->mu_w;
-        Xi_n[l] = (-1.) * Kl * k_n / p->mu_n;
-        Xi_g[l] = (-1.) * Kl * k_g / p->mu_g;
-        if (g.interior(i, j, k)) {
-          const double Pk_nw = 0, Pk_gn = 0;
-          P_n[l] = P_w[l] + Pk_nw;
-          P_g[l] = P_w[l] + Pk_nw + Pk_gn;
-        }
-        ro_w[l] = p->ro0_w * (1. + (p->beta_w) * (P_w[l] - p->P_atm));
-        ro_n[l] = p->ro0_n * (1. + (p->beta_n) * (P_n[l] - p->P_atm));
-        ro_g[l] = p->ro0_g * P_g[l] / p->P_atm;
-      }
-  if (w.keep_u_pressures) {
-    w.Pn_u.assign(P_n, P_n + g.n);
-    w.Pg_u.assign(P_g, P_g + g.n);
-  }
-
-  // roS_calculation, NR form.
 #pragma omp parallel for schedule(static)
   for (int k = 0; k < g.nz; k++)
     for (int j = 0; j < g.ny; j++)
@@ -614,6 +578,77 @@ void step3(const capaz_params* p, const Grid& g, double* P_w, double* S_w, doubl
         roS_g[l] = A3;
       }
 
+}
+
+// Border_P of the three-phase task (three-phase.cpp:362-427) for boundary cell
+// l with basic coordinate l1, capillary pressures zero.
+void border_P3(const capaz_params* p, int j, int ny, double* P_w, double* P_n, double* P_g, long l, long l1) {
+  const double Pk_nw = 0, Pk_gn = 0;
+  if ((j != 0) && (j != ny - 1)) {
+    P_w[l] = P_w[l1];
+    P_n[l] = P_w[l1] + Pk_nw;
+    P_g[l] = P_w[l1] + Pk_nw + Pk_gn;
+  } else if (j == 0) {
+    P_w[l] = (P_w[l1] - (p->ro0_w) * (p->g_const) * (p->hy) * (1. - (p->beta_w) * (p->P_atm))) /
+             (1. + (p->beta_w) * (p->ro0_w) * (p->g_const) * (p->hy));
+    P_n[l] = (P_w[l1] + Pk_nw - (p->ro0_n) * (p->g_const) * (p->hy) * (1. - (p->beta_n) * (p->P_atm))) /
+             (1. + (p->beta_n) * (p->ro0_n) * (p->g_const) * (p->hy));
+    P_g[l] = (P_w[l1] + Pk_nw + Pk_gn) / (1. + (p->ro0_g) * (p->g_const) * (p->hy) / (p->P_atm));
+  } else {
+    P_w[l] = (P_w[l1] + (p->ro0_w) * (p->g_const) * (p->hy) * (1. - (p->beta_w) * (p->P_atm))) /
+             (1. - (p->beta_w) * (p->ro0_w) * (p->g_const) * (p->hy));
+    P_n[l] = (P_w[l1] + Pk_nw + (p->ro0_n) * (p->g_const) * (p->hy) * (1. - (p->beta_n) * (p->P_atm))) /
+             (1. - (p->beta_n) * (p->ro0_n) * (p->g_const) * (p->hy));
+    P_g[l] = (P_w[l1] + Pk_nw + Pk_gn) / (1. - (p->ro0_g) * (p->g_const) * (p->hy) / (p->P_atm));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Three-phase step (CPU physics).
+void step3(const capaz_params* p, const Grid& g, double* P_w, double* S_w, double* S_n, double* P_n,
+           double* P_g, const double* m, const double* K, Work& w) {
+  const double A = p->lambda;
+  const double den = 1. - p->S_wr - p->S_nr - p->S_gr;
+  double *S_g = w.S_g.data(), *ro_w = w.ro_w.data(), *ro_n = w.ro_n.data(), *ro_g = w.ro_g.data();
+  double *Xi_w = w.Xi_w.data(), *Xi_n = w.Xi_n.data(), *Xi_g = w.Xi_g.data();
+  double *roS_w = w.roS_w.data(), *roS_n = w.roS_n.data(), *roS_g = w.roS_g.data();
+  double *roS_w_old = w.roS_w_old.data(), *roS_n_old = w.roS_n_old.data(), *roS_g_old = w.roS_g_old.data();
+
+  // S_calculation (all cells).
+#pragma omp parallel for schedule(static)
+  for (long l = 0; l < g.n; l++) S_g[l] = 1. - S_w[l] - S_n[l];
+
+  // ro_P_Xi_calculation: Xi and rho on all cells, P_n and P_g on interior
+  // cells only (three-phase.cpp:225-235).
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        long l = g.at(i, j, k);
+        double S_w_e = (S_w[l] - p->S_wr) / den;
+        double S_n_e = (S_n[l] - p->S_nr) / den;
+        double S_g_e = 1. - S_w_e - S_n_e;
+        double k_w = k_w3(S_w_e, A), k_g = k_g3(S_g_e, A), k_n = k_n3(S_w_e, S_n_e, A);
+        double Kl = Kc(p, K, l);
+        Xi_w[l] = (-1.) * Kl * k_w / p->mu_w;
+        Xi_n[l] = (-1.) * Kl * k_n / p->mu_n;
+        Xi_g[l] = (-1.) * Kl * k_g / p->mu_g;
+        if (g.interior(i, j, k)) {
+          const double Pk_nw = 0, Pk_gn = 0;
+          P_n[l] = P_w[l] + Pk_nw;
+          P_g[l] = P_w[l] + Pk_nw + Pk_gn;
+        }
+        ro_w[l] = p->ro0_w * (1. + (p->beta_w) * (P_w[l] - p->P_atm));
+        ro_n[l] = p->ro0_n * (1. + (p->beta_n) * (P_n[l] - p->P_atm));
+        ro_g[l] = p->ro0_g * P_g[l] / p->P_atm;
+      }
+  if (w.keep_u_pressures) {
+    w.Pn_u.assign(P_n, P_n + g.n);
+    w.Pg_u.assign(P_g, P_g + g.n);
+  }
+
+  roS3(p, g, P_w, S_w, S_n, P_n, P_g, m, w);
+
   // P_S_calculation: 3x3 Newton (three-phase.cpp:286-339).
 #pragma omp parallel for schedule(static)
   for (int k = 0; k < g.nz; k++)
@@ -652,7 +687,6 @@ void step3(const capaz_params* p, const Grid& g, double* P_w, double* S_w, doubl
       }
 
   // boundary_conditions (three-phase.cpp:345-427).
-  const double gh = p->g_const * p->hy;
 #pragma omp parallel for schedule(static)
   for (int k = 0; k < g.nz; k++)
     for (int j = 0; j < g.ny; j++)
@@ -673,25 +707,252 @@ void step3(const capaz_params* p, const Grid& g, double* P_w, double* S_w, doubl
           S_w[l] = p->S_w_gr;
           S_n[l] = p->S_n_gr;
         }
-        const double Pk_nw = 0, Pk_gn = 0;
-        (void)gh;
-        if ((j != 0) && (j != g.ny - 1)) {
-          P_w[l] = P_w[l1];
-          P_n[l] = P_w[l1] + Pk_nw;
-          P_g[l] = P_w[l1] + Pk_nw + Pk_gn;
-        } else if (j == 0) {
-          P_w[l] = (P_w[l1] - (p->ro0_w) * (p->g_const) * (p->hy) * (1. - (p->beta_w) * (p->P_atm))) /
-                   (1. + (p->beta_w) * (p->ro0_w) * (p->g_const) * (p->hy));
-          P_n[l] = (P_w[l1] + Pk_nw - (p->ro0_n) * (p->g_const) * (p->hy) * (1. - (p->beta_n) * (p->P_atm))) /
-                   (1. + (p->beta_n) * (p->ro0_n) * (p->g_const) * (p->hy));
-          P_g[l] = (P_w[l1] + Pk_nw + Pk_gn) / (1. + (p->ro0_g) * (p->g_const) * (p->hy) / (p->P_atm));
-        } else {
-          P_w[l] = (P_w[l1] + (p->ro0_w) * (p->g_const) * (p->hy) * (1. - (p->beta_w) * (p->P_atm))) /
-                   (1. - (p->beta_w) * (p->ro0_w) * (p->g_const) * (p->hy));
-          P_n[l] = (P_w[l1] + Pk_nw + (p->ro0_n) * (p->g_const) * (p->hy) * (1. - (p->beta_n) * (p->P_atm))) /
-                   (1. - (p->beta_n) * (p->ro0_n) * (p->g_const) * (p->hy));
-          P_g[l] = (P_w[l1] + Pk_nw + Pk_gn) / (1. - (p->ro0_g) * (p->g_const) * (p->hy) / (p->P_atm));
+        border_P3(p, j, g.ny, P_w, P_n, P_g, l, l1);
+      }
+}
+
+// ---------------------------------------------------------------------------
+// Three-phase step with the energy equation (THREE_PHASE + ENERGY build).
+// Constants are energy.cpp:1-30's globals (T_0 also assign_ro's local,
+// cpu.cpp:120-123); temperatures of the initial state and of the top and
+// bottom rows are three-phase.cpp:487 and energy.cpp:404-411.
+namespace en {
+const double T_0 = 273., ro_r = 2000.;
+const double lambda0_w = 0.553, lambda0_n = 0.14, lambda0_g = 0.0237, lambda0_r = 1.;
+const double lambdaA_w = 3E-3, lambdaA_n = 1E-3, lambdaA_g = 0.82;
+const double c0_w = 4.194E3, c0_n = 1.7E3, c0_g = 1E3, c0_r = 0.8E3;
+const double C_w = 1.15, C_w2 = 0.015, C_n = 3.4, C_g = 0.119, C_r = 0.75;
+const double alfa_w = 1.32E-7, alfa_n = 9.2E-7;
+const double T_init = 285., T_top = 400., T_bottom = 273.;
+
+// Specific heats (energy.cpp:33-51) and enthalpies (energy.cpp:84-140).
+inline double c_w(double T) { return c0_w - C_w * (T - T_0) + C_w2 * (T - T_0) * (T - T_0); }
+inline double c_n(double T) { return c0_n + C_n * (T - T_0); }
+inline double c_g(double T) { return c0_g + C_g * (T - T_0); }
+inline double c_r(double T) { return c0_r + C_r * (T - T_0); }
+inline double H_w(const capaz_params* p, double T) {
+  return (p->P_atm / p->ro0_w) + (T - T_0) * (c0_w - (T - T_0) * (C_w / 2 + C_w2 * (T - T_0) / 3));
+}
+inline double H_n(const capaz_params* p, double T) { return (p->P_atm / p->ro0_n) + (T - T_0) * (c0_n + C_n * (T - T_0) / 2); }
+inline double H_g(const capaz_params* p, double T) { return (p->P_atm / p->ro0_g) + (T - T_0) * (c0_g + C_g * (T - T_0) / 2); }
+inline double H_r(const capaz_params* p, double T) { return (p->P_atm / ro_r) + (T - T_0) * (c0_r + C_r * (T - T_0) / 2); }
+// Effective heat conductivity (energy.cpp:54-81).
+inline double lam_eff(double m, double Sw, double Sn, double Sg, double T) {
+  return m * (Sw * (lambda0_w * (1 - lambdaA_w * (T - T_0))) + Sn * (lambda0_n * (1 - lambdaA_n * (T - T_0))) +
+              Sg * (lambda0_g * pow((T / T_0), lambdaA_g))) +
+         (1. - m) * lambda0_r;
+}
+// Densities of (P, T) and their derivatives (energy.cpp:143-228).
+inline double ro_w(const capaz_params* p, double P, double T) {
+  return p->ro0_w * (1. + (p->beta_w) * (P - p->P_atm) - alfa_w * (T - T_0));
+}
+inline double ro_n(const capaz_params* p, double P, double T) {
+  return p->ro0_n * (1. + (p->beta_n) * (P - p->P_atm) - alfa_n * (T - T_0));
+}
+inline double ro_g(const capaz_params* p, double P, double T) { return p->ro0_g * (P / p->P_atm) * (T_0 / T); }
+}  // namespace en
+
+void velocities(const capaz_params* p, const Grid& g, const double* P, const double* Xi, const double* ro,
+                double* ux, double* uy, double* uz);
+
+struct WorkE {
+  std::vector<double> H_w, H_n, H_g, H_r, E, E_new, lam;
+  std::vector<double> ux_w, uy_w, uz_w, ux_n, uy_n, uz_n, ux_g, uy_g, uz_g;
+};
+
+// One step of the energy build's time_step_function (main.cpp:93-108):
+// S, ro/P/Xi (temperature-dependent viscosities three-phase.cpp:210-215 and
+// densities cpu.cpp:118-127), u, roS (as three-phase), H and E at the current
+// state (cpu.cpp:38-49), E_new (cpu.cpp:67-77, energy.cpp:232-343), the 5x5
+// Newton in (S_w, S_n, S_g, P_w, T) (energy.cpp:348-462) and the boundary
+// rules (three-phase.cpp:345-427, energy.cpp:396-418).
+void step3e(const capaz_params* p, const Grid& g, double* P_w, double* S_w, double* S_n, double* P_n, double* P_g,
+            double* T, const double* m, const double* K, Work& w, WorkE& e) {
+  using namespace en;
+  const double A = p->lambda;
+  const double den = 1. - p->S_wr - p->S_nr - p->S_gr;
+  double *S_g = w.S_g.data(), *rw = w.ro_w.data(), *rn = w.ro_n.data(), *rg = w.ro_g.data();
+  double *Xi_w = w.Xi_w.data(), *Xi_n = w.Xi_n.data(), *Xi_g = w.Xi_g.data();
+  double *roS_w = w.roS_w.data(), *roS_n = w.roS_n.data(), *roS_g = w.roS_g.data();
+
+#pragma omp parallel for schedule(static)
+  for (long l = 0; l < g.n; l++) S_g[l] = 1. - S_w[l] - S_n[l];
+
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        long l = g.at(i, j, k);
+        double S_w_e = (S_w[l] - p->S_wr) / den;
+        double S_n_e = (S_n[l] - p->S_nr) / den;
+        double S_g_e = 1. - S_w_e - S_n_e;
+        double k_w = k_w3(S_w_e, A), k_g = k_g3(S_g_e, A), k_n = k_n3(S_w_e, S_n_e, A);
+        double mu_w = 1. / (29.21 * T[l] - 7506.64);
+        double mu_n = 7.256E-10 * exp(4141.9 / T[l]);
+        double mu_g = 1.717E-5 * pow((T[l] / 273.), 0.683);
+        double Kl = Kc(p, K, l);
+        Xi_w[l] = (-1.) * Kl * k_w / mu_w;
+        Xi_n[l] = (-1.) * Kl * k_n / mu_n;
+        Xi_g[l] = (-1.) * Kl * k_g / mu_g;
+        if (g.interior(i, j, k)) {
+          const double Pk_nw = 0, Pk_gn = 0;
+          P_n[l] = P_w[l] + Pk_nw;
+          P_g[l] = P_w[l] + Pk_nw + Pk_gn;
         }
+        rw[l] = ro_w(p, P_w[l], T[l]);
+        rn[l] = ro_n(p, P_n[l], T[l]);
+        rg[l] = ro_g(p, P_g[l], T[l]);
+      }
+
+  velocities(p, g, P_w, Xi_w, rw, e.ux_w.data(), e.uy_w.data(), e.uz_w.data());
+  velocities(p, g, P_n, Xi_n, rn, e.ux_n.data(), e.uy_n.data(), e.uz_n.data());
+  velocities(p, g, P_g, Xi_g, rg, e.ux_g.data(), e.uy_g.data(), e.uz_g.data());
+
+  roS3(p, g, P_w, S_w, S_n, P_n, P_g, m, w);
+
+  // H_E_current_calculation (all cells).
+  double *Hw = e.H_w.data(), *Hn = e.H_n.data(), *Hg = e.H_g.data(), *Hr = e.H_r.data();
+  double *E = e.E.data(), *E_new = e.E_new.data(), *lam = e.lam.data();
+#pragma omp parallel for schedule(static)
+  for (long l = 0; l < g.n; l++) {
+    Hw[l] = H_w(p, T[l]);
+    Hn[l] = H_n(p, T[l]);
+    Hg[l] = H_g(p, T[l]);
+    Hr[l] = H_r(p, T[l]);
+    E[l] = (m[l] * (S_w[l] * (rw[l] * Hw[l] - P_w[l]) + S_n[l] * (rn[l] * Hn[l] - P_n[l]) +
+                    S_g[l] * (rg[l] * Hg[l] - P_g[l])) +
+            (1. - m[l]) * (ro_r * Hr[l] - P_w[l]));
+    lam[l] = lam_eff(m[l], S_w[l], S_n[l], S_g[l], T[l]);
+  }
+
+  // E_calculation: E_new = E + dt (T_flow + Q_hw + Q_hr - E_flow) on
+  // interior cells; the z term of T_flow replaces the sum, the z term of
+  // E_flow takes the y velocities (energy.cpp:256-261, 302-311, as written).
+  const double *uxw = e.ux_w.data(), *uyw = e.uy_w.data(), *uxn = e.ux_n.data(), *uyn = e.uy_n.data();
+  const double *uxg = e.ux_g.data(), *uyg = e.uy_g.data();
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        if (!g.interior(i, j, k)) continue;
+        long l = g.at(i, j, k);
+        double Tf = 0;
+        if (g.nx > 2)
+          Tf += (lam[l + 1] * T[l + 1] - 2 * lam[l] * T[l] + lam[l - 1] * T[l - 1]) / ((p->hx) * (p->hx));
+        if (g.ny > 2)
+          Tf += (lam[l + g.sy] * T[l + g.sy] - 2 * lam[l] * T[l] + lam[l - g.sy] * T[l - g.sy]) / ((p->hy) * (p->hy));
+        if (g.nz > 2)
+          Tf = (lam[l + g.sz] * T[l + g.sz] - 2 * lam[l] * T[l] + lam[l - g.sz] * T[l - g.sz]) / ((p->hz) * (p->hz));
+        auto flux = [&](long s, const double* uw, const double* un, const double* ug, double h) {
+          return (rw[l + s] * Hw[l + s] * uw[l + s] - rw[l - s] * Hw[l - s] * uw[l - s] +
+                  rn[l + s] * Hn[l + s] * un[l + s] - rn[l - s] * Hn[l - s] * un[l - s] +
+                  rg[l + s] * Hg[l + s] * ug[l + s] - rg[l - s] * Hg[l - s] * ug[l - s]) /
+                 (2. * h);
+        };
+        double Ef = 0;
+        if (g.nx > 2) Ef += flux(g.sx, uxw, uxn, uxg, p->hx);
+        if (g.ny > 2) Ef += flux(g.sy, uyw, uyn, uyg, p->hy);
+        if (g.nz > 2) Ef += flux(g.sz, uyw, uyn, uyg, p->hz);
+        const double Q_hw = 0, Q_hr = 0;
+        E_new[l] = E[l] + (p->dt) * (Tf + Q_hw + Q_hr - Ef);
+      }
+
+  // P_S_calculation: the 5x5 Newton with reverse_matrix and
+  // mult_matrix_vector (gauss.cpp:6-104); rows F0..F4, columns
+  // d/d(S_w, S_n, S_g, P, T).  reverse_matrix leaves dF as it is when it
+  // finds no pivot, and the reference uses dF all the same.
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        if (!g.interior(i, j, k)) continue;
+        long l = g.at(i, j, k);
+        const int n = 5;
+        const double ml = m[l];
+        for (int it = 1; it <= p->newton_iterations; it++) {
+          const double P = P_w[l], Tl = T[l], Sw = S_w[l], Sn = S_n[l], Sg = S_g[l];
+          double F[5], dF[25], c[5];
+          F[0] = Sg + Sw + Sn - 1.;
+          F[1] = ro_w(p, P, Tl) * Sw - roS_w[l];
+          F[2] = ro_n(p, P, Tl) * Sn - roS_n[l];
+          F[3] = ro_g(p, P, Tl) * Sg - roS_g[l];
+          F[4] = ml * (Sw * (ro_w(p, P, Tl) * Hw[l] - P) + Sn * (ro_n(p, P, Tl) * Hn[l] - P) +
+                       Sg * (ro_g(p, P, Tl) * Hg[l] - P)) +
+                 (1. - ml) * (ro_r * Hr[l] - P) - E_new[l];
+          const double dwP = p->ro0_w * (p->beta_w), dwT = (-1) * p->ro0_w * alfa_w;
+          const double dnP = p->ro0_n * (p->beta_n), dnT = (-1) * p->ro0_n * alfa_n;
+          const double dgP = (p->ro0_g / p->P_atm) * (T_0 / Tl);
+          const double dgT = p->ro0_g * (P / p->P_atm) * (-1) * (T_0 / Tl) / Tl;
+          dF[0] = 1.;
+          dF[1] = 1.;
+          dF[2] = 1.;
+          dF[3] = 0.;
+          dF[4] = 0.;
+          dF[0 + n] = ro_w(p, P, Tl);
+          dF[1 + n] = 0.;
+          dF[2 + n] = 0.;
+          dF[3 + n] = dwP * Sw;
+          dF[4 + n] = dwT * Sw;
+          dF[0 + n * 2] = 0.;
+          dF[1 + n * 2] = ro_n(p, P, Tl);
+          dF[2 + n * 2] = 0.;
+          dF[3 + n * 2] = dnP * Sn;
+          dF[4 + n * 2] = dnT * Sn;
+          dF[0 + n * 3] = 0.;
+          dF[1 + n * 3] = 0.;
+          dF[2 + n * 3] = ro_g(p, P, Tl);
+          dF[3 + n * 3] = dgP * Sg;
+          dF[4 + n * 3] = dgT * Sg;
+          dF[0 + n * 4] = ml * (ro_w(p, P, Tl) * Hw[l] - P);
+          dF[1 + n * 4] = ml * (ro_n(p, P, Tl) * Hn[l] - P);
+          dF[2 + n * 4] = ml * (ro_g(p, P, Tl) * Hg[l] - P);
+          dF[3 + n * 4] = ml * (Sw * (dwP * Hw[l] - 1.) + Sn * (dnP * Hn[l] - 1.) + Sg * (dgP * Hg[l] - 1.)) +
+                          (1. - ml) * (-1);
+          dF[4 + n * 4] = ml * (Sw * (dwT * Hw[l] + ro_w(p, P, Tl) * c_w(Tl)) +
+                                Sn * (dnT * Hn[l] + ro_n(p, P, Tl) * c_n(Tl)) +
+                                Sg * (dgT * Hg[l] + ro_g(p, P, Tl) * c_g(Tl))) +
+                          (1. - ml) * ro_r * c_r(Tl);
+          reverse_matrix(dF, n);
+          for (int a = 0; a < n; a++) {
+            c[a] = 0;
+            for (int b = 0; b < n; b++) c[a] += dF[b + n * a] * F[b];
+          }
+          S_w[l] = Sw - c[0];
+          S_n[l] = Sn - c[1];
+          S_g[l] = Sg - c[2];
+          P_w[l] = P - c[3];
+          T[l] = Tl - c[4];
+          Hw[l] = H_w(p, T[l]);
+          Hn[l] = H_n(p, T[l]);
+          Hg[l] = H_g(p, T[l]);
+          Hr[l] = H_r(p, T[l]);
+        }
+        E[l] = E_new[l];
+      }
+
+  // boundary_conditions: Border_S, Border_P (three-phase), Border_T.
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < g.nz; k++)
+    for (int j = 0; j < g.ny; j++)
+      for (int i = 0; i < g.nx; i++) {
+        bool bnd = (((i == 0) || (i == g.nx - 1)) && (g.nx >= 2)) || (j == 0) || (j == g.ny - 1) ||
+                   (((k == 0) || (k == g.nz - 1)) && (g.nz >= 2));
+        if (!bnd) continue;
+        long l1 = g.basic(i, j, k);
+        long l = g.at(i, j, k);
+        const bool src = (j == 0) && (p->source > 0) &&
+                         (!(p->flags & CAPAZ_FLAG_SOURCE_WINDOW) || in_window(p, i, k));
+        if (!src) {
+          S_w[l] = S_w[l1];
+          S_n[l] = S_n[l1];
+        } else {
+          S_w[l] = p->S_w_gr;
+          S_n[l] = p->S_n_gr;
+        }
+        border_P3(p, j, g.ny, P_w, P_n, P_g, l, l1);
+        if (j == 0) T[l] = T_top;
+        else if (j == g.ny - 1) T[l] = T_bottom;
+        else T[l] = T[l1];
       }
 }
 
@@ -930,6 +1191,72 @@ int oracle_step(const capaz_params* p, int nsteps, double* P_w, double* S_w, dou
       if (!(pr[k] <= diag->max_residual)) diag->max_residual = pr[k];
       diag->nonfinite_cells += pnf[k];
     }
+  }
+  return CAPAZ_OK;
+}
+
+// Energy model (CAPAZ_MODEL_ENERGY): the initial temperature of
+// data_initialization (three-phase.cpp:485-490) on every cell.
+int oracle_init_temperature(const capaz_params* p, double* T) {
+  int rc = check_grid(p);
+  if (rc) return rc;
+  Grid g(p);
+  for (long l = 0; l < g.n; l++) T[l] = en::T_init;
+  return CAPAZ_OK;
+}
+
+// Energy model: advances nsteps; P_w, S_w, S_n, P_n, P_g, T in/out.
+// `derived` as for oracle_step: the reference's other arrays after the last
+// step (S_g, rho, Xi, u, roS, roS_old, H, E, E_new).
+int oracle_step_energy(const capaz_params* p, int nsteps, double* P_w, double* S_w, double* S_n, double* P_n,
+                       double* P_g, double* T, const double* m, const double* K, double** derived, int nthreads) {
+  int rc = check_grid(p);
+  if (rc) return rc;
+  if (p->phases != 3) return CAPAZ_ERR_INVALID_ARGUMENT;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  Grid g(p);
+  const long n = g.n;
+  Work w;
+  WorkE e;
+  for (auto* v : {&w.S_g, &w.ro_w, &w.ro_n, &w.ro_g, &w.Xi_w, &w.Xi_n, &w.Xi_g, &w.roS_w, &w.roS_n, &w.roS_g,
+                  &w.roS_w_old, &w.roS_n_old, &w.roS_g_old})
+    v->assign(n, 0.);
+  for (auto* v : {&e.H_w, &e.H_n, &e.H_g, &e.H_r, &e.E, &e.E_new, &e.lam, &e.ux_w, &e.uy_w, &e.uz_w, &e.ux_n,
+                  &e.uy_n, &e.uz_n, &e.ux_g, &e.uy_g, &e.uz_g})
+    v->assign(n, 0.);
+  for (int s = 0; s < nsteps; s++) step3e(p, g, P_w, S_w, S_n, P_n, P_g, T, m, K, w, e);
+  if (derived && nsteps > 0) {
+    auto put = [&](int f, const std::vector<double>& v) {
+      if (derived[f]) memcpy(derived[f], v.data(), sizeof(double) * n);
+    };
+    put(CAPAZ_FIELD_S_G, w.S_g);
+    put(CAPAZ_FIELD_RO_W, w.ro_w);
+    put(CAPAZ_FIELD_RO_N, w.ro_n);
+    put(CAPAZ_FIELD_RO_G, w.ro_g);
+    put(CAPAZ_FIELD_XI_W, w.Xi_w);
+    put(CAPAZ_FIELD_XI_N, w.Xi_n);
+    put(CAPAZ_FIELD_XI_G, w.Xi_g);
+    put(CAPAZ_FIELD_UX_W, e.ux_w);
+    put(CAPAZ_FIELD_UY_W, e.uy_w);
+    put(CAPAZ_FIELD_UZ_W, e.uz_w);
+    put(CAPAZ_FIELD_UX_N, e.ux_n);
+    put(CAPAZ_FIELD_UY_N, e.uy_n);
+    put(CAPAZ_FIELD_UZ_N, e.uz_n);
+    put(CAPAZ_FIELD_UX_G, e.ux_g);
+    put(CAPAZ_FIELD_UY_G, e.uy_g);
+    put(CAPAZ_FIELD_UZ_G, e.uz_g);
+    put(CAPAZ_FIELD_ROS_W, w.roS_w);
+    put(CAPAZ_FIELD_ROS_N, w.roS_n);
+    put(CAPAZ_FIELD_ROS_G, w.roS_g);
+    put(CAPAZ_FIELD_ROS_W_OLD, w.roS_w_old);
+    put(CAPAZ_FIELD_ROS_N_OLD, w.roS_n_old);
+    put(CAPAZ_FIELD_ROS_G_OLD, w.roS_g_old);
+    put(CAPAZ_FIELD_H_W, e.H_w);
+    put(CAPAZ_FIELD_H_N, e.H_n);
+    put(CAPAZ_FIELD_H_G, e.H_g);
+    put(CAPAZ_FIELD_H_R, e.H_r);
+    put(CAPAZ_FIELD_E, e.E);
+    put(CAPAZ_FIELD_E_NEW, e.E_new);
   }
   return CAPAZ_OK;
 }

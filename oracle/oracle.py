@@ -42,6 +42,11 @@ def load() -> C.CDLL:
                                     C.POINTER(P), C.POINTER(Diag), C.c_int]
         lib.oracle_step.restype = C.c_int
         lib.oracle_max_threads.restype = C.c_int
+        lib.oracle_init_temperature.argtypes = [C.POINTER(Params), P]
+        lib.oracle_init_temperature.restype = C.c_int
+        lib.oracle_step_energy.argtypes = [C.POINTER(Params), C.c_int, P, P, P, P, P, P, P, P, C.POINTER(P),
+                                           C.c_int]
+        lib.oracle_step_energy.restype = C.c_int
         lib.oracle_tangent.argtypes = [C.POINTER(Params), C.c_int, P, P, P, P, C.c_int, P, P,
                                        C.POINTER(C.c_long), C.c_int, C.c_int, P, P, P, C.c_int]
         lib.oracle_tangent.restype = C.c_int
@@ -75,6 +80,11 @@ def init(p: Params, m: np.ndarray | None = None) -> dict:
     if p.phases == 2:
         for k in ("S_w", "P_n", "P_g"):
             out.pop(k)
+    if p.model == 2:
+        out["T"] = np.zeros(sh)
+        rc = load().oracle_init_temperature(C.byref(p), _ptr(out["T"]))
+        if rc:
+            raise RuntimeError(f"oracle_init_temperature failed: {rc}")
     return out
 
 
@@ -93,15 +103,28 @@ def step(p: Params, state: dict, nsteps: int, m: np.ndarray, K: np.ndarray | Non
     dout = {}
     if derived:
         arr = (C.POINTER(C.c_double) * FIELD_COUNT)()
-        from capaz_b200.native import FIELDS
+        from capaz_b200.native import ENERGY_FIELDS, FIELDS
         for name, idx in FIELDS.items():
             if name in ("P_w", "S_n", "m", "K") or (p.phases == 3 and name in ("S_w", "P_n", "P_g")):
+                continue
+            if name in ENERGY_FIELDS and (p.model != 2 or name == "T"):
                 continue
             if p.phases == 2 and name.endswith("_g") or name == "P_g":
                 continue
             dout[name] = np.zeros(sh)
             arr[idx] = _ptr(dout[name])
         dptrs = arr
+    if p.model == 2:
+        if "T" not in st:
+            raise ValueError("the energy model's state needs T")
+        rc = load().oracle_step_energy(C.byref(p), int(nsteps), _ptr(st["P_w"]), _ptr(st["S_w"]), _ptr(st["S_n"]),
+                                       _ptr(st["P_n"]), _ptr(st["P_g"]), _ptr(st["T"]), _ptr(m), _ptr(K), dptrs,
+                                       int(nthreads))
+        if rc:
+            raise RuntimeError(f"oracle_step_energy failed: {rc}")
+        if derived:
+            st["derived"] = dout
+        return st
     d = Diag()
     rc = load().oracle_step(C.byref(p), int(nsteps), _ptr(st["P_w"]), _ptr(st.get("S_w")), _ptr(st["S_n"]),
                             _ptr(st.get("P_n")), _ptr(st.get("P_g")), _ptr(m), _ptr(K), dptrs,
@@ -157,6 +180,8 @@ def ref_ini_text(p: Params) -> str:
 def ref_binary(phases: int, model: int = 0) -> str:
     if model == 1:
         return os.path.join(REF_DIR, "capaz_ref_bl")
+    if model == 2:
+        return os.path.join(REF_DIR, "capaz_ref_3phe")
     return os.path.join(REF_DIR, "capaz_ref_2ph" if phases == 2 else "capaz_ref_3ph")
 
 
@@ -167,6 +192,7 @@ def ref_available(phases: int = 2) -> bool:
 REF_DERIVED_2PH = ["S_w", "P_n", "ro_w", "ro_n", "ux_w", "uy_w", "uz_w", "ux_n", "uy_n", "uz_n",
                    "Xi_w", "Xi_n", "roS_w", "roS_w_old", "roS_n", "roS_n_old"]
 REF_DERIVED_3PH = REF_DERIVED_2PH + ["S_g", "ro_g", "ux_g", "uy_g", "uz_g", "Xi_g", "roS_g", "roS_g_old"]
+REF_DERIVED_3PHE = REF_DERIVED_3PH + ["H_w", "H_n", "H_g", "H_r", "E", "E_new"]
 
 
 def ref_run(p: Params, nsteps: int, state: dict | None = None, m: np.ndarray | None = None,
@@ -196,6 +222,8 @@ def ref_run(p: Params, nsteps: int, state: dict | None = None, m: np.ndarray | N
                 fields = [state["P_w"], state["S_n"], m]
             else:
                 fields = [state["P_w"], state["S_w"], state["S_n"], state["P_n"], state["P_g"], m]
+                if p.model == 2:
+                    fields.append(state["T"])
             np.concatenate([np.ascontiguousarray(a, dtype=np.float64).ravel() for a in fields]).tofile(in_path)
         out_path = os.path.join(wd, "out.bin")
         cmd = [exe, wd, str(nsteps), in_path, out_path]
@@ -210,10 +238,12 @@ def ref_run(p: Params, nsteps: int, state: dict | None = None, m: np.ndarray | N
         raw = np.fromfile(out_path, dtype=np.float64)
         draw = np.fromfile(der_path, dtype=np.float64) if derived else None
     names = ["P_w", "S_n"] if p.phases == 2 else ["P_w", "S_w", "S_n", "P_n", "P_g"]
+    if p.model == 2:
+        names.append("T")
     out = {k: raw[a * n:(a + 1) * n].reshape(sh) for a, k in enumerate(names)}
     out["info"] = info
     if derived:
-        dn = REF_DERIVED_2PH if p.phases == 2 else REF_DERIVED_3PH
+        dn = REF_DERIVED_2PH if p.phases == 2 else REF_DERIVED_3PHE if p.model == 2 else REF_DERIVED_3PH
         out["derived"] = {k: draw[a * n:(a + 1) * n].reshape(sh) for a, k in enumerate(dn)}
     return out
 

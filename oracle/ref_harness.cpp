@@ -20,12 +20,14 @@
 // values each, x fastest (index i + j*Nx + k*Nx*Ny, main.cpp:695):
 //   two-phase   in:  P_w, S_n, m               out: P_w, S_n
 //   three-phase in:  P_w, S_w, S_n, P_n, P_g, m out: P_w, S_w, S_n, P_n, P_g
+//   three-phase with ENERGY: T appended to both (in after m)
 // With "-" as <state_in.bin> the reference's own data_initialization is used.
 // <derived_out.bin> receives the reference's other per-cell arrays as they
 // stand after the last step, in this order:
 //   two-phase   S_w P_n ro_w ro_n ux_w uy_w uz_w ux_n uy_n uz_n Xi_w Xi_n
 //               roS_w roS_w_old roS_n roS_n_old
 //   three-phase the same, then S_g ro_g ux_g uy_g uz_g Xi_g roS_g roS_g_old
+//   with ENERGY then H_w H_n H_g H_r E E_new
 //
 // On success one line "RESULT {json}" is printed with the cell count, the step
 // count and the wall time of the step loop alone (CLOCK_MONOTONIC).
@@ -102,7 +104,13 @@ int main(int argc, char* argv[]) {
   initialization(&H, &D, &time_counter, fake_argc, fake_argv, &def);
 
   long n = (long)def.locNx * def.locNy * def.locNz;
-#ifdef THREE_PHASE
+#if defined(THREE_PHASE) && defined(ENERGY)
+  double* in_f[] = {H.P_w, H.S_w, H.S_n, H.P_n, H.P_g, H.m, H.T};
+  double* dev_in[] = {D.P_w, D.S_w, D.S_n, D.P_n, D.P_g, D.m, D.T};
+  double* out_f[] = {H.P_w, H.S_w, H.S_n, H.P_n, H.P_g, H.T};
+  double* dev_out[] = {D.P_w, D.S_w, D.S_n, D.P_n, D.P_g, D.T};
+  const int nin = 7, nout = 6;
+#elif defined(THREE_PHASE)
   double* in_f[] = {H.P_w, H.S_w, H.S_n, H.P_n, H.P_g, H.m};
   double* dev_in[] = {D.P_w, D.S_w, D.S_n, D.P_n, D.P_g, D.m};
   double* out_f[] = {H.P_w, H.S_w, H.S_n, H.P_n, H.P_g};
@@ -145,11 +153,17 @@ int main(int argc, char* argv[]) {
 #ifdef THREE_PHASE
                      , H.S_g, H.ro_g, H.ux_g, H.uy_g, H.uz_g, H.Xi_g, H.roS_g, H.roS_g_old
 #endif
+#ifdef ENERGY
+                     , H.H_w, H.H_n, H.H_g, H.H_r, H.E, H.E_new
+#endif
     };
     double* dder[] = {D.S_w, D.P_n, D.ro_w, D.ro_n, D.ux_w, D.uy_w, D.uz_w, D.ux_n, D.uy_n, D.uz_n,
                       D.Xi_w, D.Xi_n, D.roS_w, D.roS_w_old, D.roS_n, D.roS_n_old
 #ifdef THREE_PHASE
                       , D.S_g, D.ro_g, D.ux_g, D.uy_g, D.uz_g, D.Xi_g, D.roS_g, D.roS_g_old
+#endif
+#ifdef ENERGY
+                      , D.H_w, D.H_n, D.H_g, D.H_r, D.E, D.E_new
 #endif
     };
     const int nd = (int)(sizeof der / sizeof der[0]);

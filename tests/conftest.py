@@ -38,6 +38,8 @@ GOLDEN_2PH = ["g2_default_15x15x1", "g2_3d_pd0_12x10x7", "g2_3d_pd_12x10x7", "g2
               "g2_min_3x3x3"]
 GOLDEN_3PH = ["g3_column_1x15x1", "g3_3d_9x8x6"]
 GOLDEN_BL = ["gbl_planar_20x15x1", "gbl_3d_gravity_12x10x6"]
+GOLDEN_ENERGY = ["ge_column_1x15x1", "ge_9x8x6", "ge_11x7x1"]
+ENERGY_STATE = ["P_w", "S_w", "S_n", "P_n", "P_g", "T"]
 
 
 def interior(a: np.ndarray) -> np.ndarray:

@@ -2,6 +2,7 @@
 
     python tests/golden/make_golden.py        # every fixture
     python tests/golden/make_golden.py bl     # the Buckley-Leverett ones only
+    python tests/golden/make_golden.py energy # the energy-equation ones only
 
 Each fixture holds the parameter set, the input state (or none: the
 reference's data_initialization), and the reference's outputs after N steps:
@@ -48,7 +49,7 @@ def save(name, p, nsteps, state, m, with_derived):
         for k, v in state.items():
             out["in_" + k] = v
         out["in_m"] = m
-    for k in ("P_w", "S_w", "S_n", "P_n", "P_g"):
+    for k in ("P_w", "S_w", "S_n", "P_n", "P_g", "T"):
         if k in r:
             out["out_" + k] = r[k]
     if with_derived:
@@ -103,6 +104,38 @@ def main():
     save("g3_3d_9x8x6", p3, 30, state, m, True)
 
 
+def energy_3d_params(nx, ny, nz):
+    """Three-phase fluids of the random 3-D case, with the energy equation."""
+    return default_params(phases=3, nx=nx, ny=ny, nz=nz, newton_iterations=7, lambda_=2.0, S_wr=0.1, S_nr=0.05,
+                          S_gr=0.02, ro0_w=1000.0, ro0_n=850.0, ro0_g=1.2, mu_w=1e-3, mu_n=3e-3, mu_g=1.8e-5,
+                          beta_w=1e-9, beta_n=1e-9, beta_g=9.2e-6, S_w_gr=0.25, S_n_gr=0.7, S_w_init=0.2,
+                          S_n_init=0.3, source=1, porosity=0.3, K0=1e-12, hx=1.0, hy=1.0, hz=1.0, dt=0.01,
+                          g_const=9.81, model=2)
+
+
+def main_energy():
+    """The THREE_PHASE + ENERGY build: the reference's Three-phase/defines.ini
+    column case from its own initial state, and random 3-D states with a
+    random temperature field."""
+    if not os.path.exists(O.ref_binary(3, 2)):
+        raise SystemExit("build the reference binaries first: make -C oracle ref")
+    rng = np.random.default_rng(20261204)
+    p3 = default_params(phases=3, nx=1, ny=15, nz=1, newton_iterations=7, lambda_=3.25, S_wr=0.0,
+                        ro0_n=850.0, ro0_g=1.4, mu_n=1e-3, mu_g=1.84e-5, beta_g=9.2e-6, S_w_gr=0.4,
+                        S_n_gr=0.3, S_w_init=0.4, S_n_init=0.3, source=0, porosity=0.4, K0=6.64e-11,
+                        timeX=1000.0, model=2)
+    save("ge_column_1x15x1", p3, 200, None, None, True)
+    for shape, nsteps in (((9, 8, 6), 20), ((11, 7, 1), 25)):
+        p = energy_3d_params(*shape)
+        m = np.clip(0.3 + 0.03 * rng.standard_normal((p.nz, p.ny, p.nx)), 0.15, 0.45)
+        st = O.init(p, m)
+        st["S_w"] = np.clip(0.3 + 0.1 * rng.standard_normal(st["S_w"].shape), 0.12, 0.6)
+        st["S_n"] = np.clip(0.3 + 0.1 * rng.standard_normal(st["S_n"].shape), 0.07, 0.35)
+        st["T"] = 285 + 5 * rng.standard_normal(st["S_w"].shape)
+        state = {k: st[k] for k in ("P_w", "S_w", "S_n", "P_n", "P_g", "T")}
+        save("ge_%dx%dx%d" % shape, p, nsteps, state, m, True)
+
+
 def bl_params(nx, ny, nz, g, dt):
     """The reference's Backley-Leverett/defines.ini fluids and wells."""
     return default_params(nx=nx, ny=ny, nz=nz, dt=dt, model=1, Q=3.5e-6, background_Pw=3e5,
@@ -143,6 +176,9 @@ def main_bl():
 if __name__ == "__main__":
     if sys.argv[1:] == ["bl"]:
         main_bl()
+    elif sys.argv[1:] == ["energy"]:
+        main_energy()
     else:
         main()
         main_bl()
+        main_energy()

@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_2PH, GOLDEN_3PH, GOLDEN_BL, interior, load_golden
+from conftest import ENERGY_STATE, GOLDEN_2PH, GOLDEN_3PH, GOLDEN_BL, GOLDEN_ENERGY, interior, load_golden
 from oracle import oracle as O
 
 
@@ -47,6 +47,29 @@ def test_oracle_buckley_leverett_matches_reference_bitwise(name):
     out = O.step(q, {"P_w": st["P_w"], "S_n": st["S_n"]}, int(g["nsteps"]), st["m"], g["K"])
     assert np.array_equal(out["P_w"], g["out_P_w"])
     assert np.array_equal(out["S_n"], g["out_S_n"])
+
+
+@pytest.mark.parametrize("name", GOLDEN_ENERGY)
+def test_oracle_energy_matches_reference_bitwise(name):
+    """The energy equation (THREE_PHASE + ENERGY build: energy.cpp with the
+    three-phase module): the state with T and every array the reference
+    keeps, bit for bit (E_new and roS exist on interior cells only)."""
+    p, g = load_golden(name)
+    if "in_P_w" in g:
+        state, m = {k: g["in_" + k] for k in ENERGY_STATE}, g["in_m"]
+    else:
+        st = O.init(p)
+        state, m = {k: st[k] for k in ENERGY_STATE}, st["m"]
+    out = O.step(p, state, int(g["nsteps"]), m, derived=True)
+    for k in ENERGY_STATE:
+        assert np.array_equal(out[k], g["out_" + k]), k
+    for key in [k for k in g if k.startswith("der_")]:
+        f = key[4:]
+        a = out[f] if f in ENERGY_STATE else out["derived"][f]
+        if f.startswith("roS") or f == "E_new":
+            assert np.array_equal(interior(a), interior(g[key])), f
+        else:
+            assert np.array_equal(a, g[key]), f
 
 
 def test_oracle_init_matches_reference():
