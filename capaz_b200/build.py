@@ -36,6 +36,7 @@ CUDA_SOURCES = [
     ("step2_fp32c_tma.cu", []),
     ("step3_fp64.cu", ["-fmad=false"]),
     ("step_bl.cu", ["-fmad=false"]),
+    ("step3e.cu", ["-fmad=false"]),
     ("fields.cu", []),
     ("capaz_api.cu", []),
     ("capaz_run.cu", []),
@@ -46,7 +47,7 @@ CUDA_SOURCES = [
     ("media.cu", []),
     ("slab.cu", []),
 ]
-HEADERS = ["capaz_internal.h", "capaz_ctx.h"]
+HEADERS = ["capaz_internal.h", "capaz_ctx.h", "phys3.cuh"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -50,7 +50,14 @@ int cuda_fail(capaz_ctx* ctx, cudaError_t e, const char* what) {
 bool is_state_field(const capaz_params& p, int f) {
   if (f == CAPAZ_FIELD_P_W || f == CAPAZ_FIELD_S_N) return true;
   if (p.phases == 3 && (f == CAPAZ_FIELD_S_W || f == CAPAZ_FIELD_P_N || f == CAPAZ_FIELD_P_G)) return true;
+  if (p.model == CAPAZ_MODEL_ENERGY && f == CAPAZ_FIELD_T) return true;
   return false;
+}
+
+// State arrays of a context: P_w, S_n[, S_w, P_n, P_g[, T]].
+int state_count(const capaz_params& p) {
+  if (p.phases == 2) return 2;
+  return p.model == CAPAZ_MODEL_ENERGY ? 6 : 5;
 }
 
 }  // namespace
@@ -466,8 +473,17 @@ int capaz_params_validate(const capaz_params* p) {
   if (!(p->mu_w > 0) || !(p->mu_n > 0) || !(p->P_atm > 0) || !(p->lambda != 0))
     return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "mu, P_atm must be > 0 and lambda != 0");
   if (!(p->K0 > 0)) return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "K_0 must be > 0");
-  if (p->model != CAPAZ_MODEL_DEFAULT && p->model != CAPAZ_MODEL_BUCKLEY_LEVERETT)
+  if (p->model != CAPAZ_MODEL_DEFAULT && p->model != CAPAZ_MODEL_BUCKLEY_LEVERETT && p->model != CAPAZ_MODEL_ENERGY)
     return fail(nullptr, CAPAZ_ERR_INVALID_ARGUMENT, "unknown model %d", p->model);
+  if (p->model == CAPAZ_MODEL_ENERGY) {
+    if (p->phases != 3 || p->form != CAPAZ_FORM_FP64)
+      return fail(nullptr, CAPAZ_ERR_UNSUPPORTED, "the energy equation is three-phase, FP64 form");
+    if (p->flags & CAPAZ_FLAG_DIAGNOSTICS)
+      return fail(nullptr, CAPAZ_ERR_UNSUPPORTED, "diagnostics are not built for the energy equation");
+    // Its advected enthalpy reaches two cells: one halo plane per slab is not enough.
+    if (p->z_offset != 0 || (p->nz_global > 0 && p->nz_global != p->nz))
+      return fail(nullptr, CAPAZ_ERR_UNSUPPORTED, "the energy equation does not run on z-slabs");
+  }
   if (p->model == CAPAZ_MODEL_BUCKLEY_LEVERETT && (p->phases != 2 || p->form != CAPAZ_FORM_FP64))
     return fail(nullptr, CAPAZ_ERR_UNSUPPORTED, "the Buckley-Leverett task is two-phase, FP64 form");
   // The injection and production well blocks (2x2 corners, b-l.cpp:221-237)
@@ -598,7 +614,7 @@ int capaz_ctx::allocate() {
   CUDA_TRY(this, cudaSetDevice(device));
   n = (long long)p.nx * p.ny * p.nz;
   const size_t es = (p.form == CAPAZ_FORM_FP64) ? sizeof(double) : sizeof(float);
-  const int nstate = (p.phases == 2) ? 2 : 5;  // P_w, S_n[, S_w, P_n, P_g]
+  const int nstate = state_count(p);
   for (int b = 0; b < 2; b++)
     for (int s = 0; s < nstate; s++) CUDA_TRY(this, cudaMalloc(&state[b][s], n * es));
   CUDA_TRY(this, cudaMalloc(&m, n * es));
@@ -625,6 +641,10 @@ int capaz_ctx::allocate() {
   // Default porosity M_0 and a zero state until the caller sets one.
   for (int b = 0; b < 2; b++)
     for (int s = 0; s < nstate; s++) CUDA_TRY(this, cudaMemset(state[b][s], 0, n * es));
+  if (p.model == CAPAZ_MODEL_ENERGY) {
+    CUDA_TRY(this, cudaMalloc(&ework, sizeof(double) * EW_COUNT * n));
+    CUDA_TRY(this, cudaMemset(ework, 0, sizeof(double) * EW_COUNT * n));
+  }
   {
     // Defaults need no validation: the caller's own m and K are checked when
     // set.  A non-positive M_0 is kept as given until m is set.
@@ -645,8 +665,9 @@ int capaz_ctx::allocate() {
 void capaz_ctx::release() {
   cudaSetDevice(device);
   for (int b = 0; b < 2; b++)
-    for (int s = 0; s < 5; s++)
+    for (int s = 0; s < 6; s++)
       if (state[b][s]) cudaFree(state[b][s]);
+  if (ework) cudaFree(ework);
   if (m) cudaFree(m);
   if (K) cudaFree(K);
   if (err_flag) cudaFree(err_flag);
@@ -697,7 +718,7 @@ int capaz_ctx::set_field(int field, const void* src, bool on_device, cudaStream_
     CUDA_TRY(this, cudaMemcpyAsync(stage, src, n * sizeof(double), cudaMemcpyHostToDevice, s));
     d = stage;
   }
-  if ((field == CAPAZ_FIELD_M || field == CAPAZ_FIELD_K) && !defaults_unchecked) {
+  if ((field == CAPAZ_FIELD_M || field == CAPAZ_FIELD_K || field == CAPAZ_FIELD_T) && !defaults_unchecked) {
     const unsigned long long none = (unsigned long long)n;
     CUDA_TRY(this, cudaMemcpyAsync(first_bad, &none, sizeof none, cudaMemcpyHostToDevice, s));
     CUDA_TRY(this, launch_first_invalid(d, n, first_bad, s));
@@ -709,7 +730,7 @@ int capaz_ctx::set_field(int field, const void* src, bool on_device, cudaStream_
       double v = 0.;
       CUDA_TRY(this, cudaMemcpy(&v, d + bad, sizeof v, cudaMemcpyDeviceToHost));
       return fail(this, CAPAZ_ERR_BAD_STATE, "%s must be finite and > 0 (cell %llu: %g)",
-                  field == CAPAZ_FIELD_M ? "m" : "K", bad, v);
+                  field == CAPAZ_FIELD_M ? "m" : field == CAPAZ_FIELD_K ? "K" : "T", bad, v);
     }
   }
   if (p.form == CAPAZ_FORM_FP64) {
@@ -748,7 +769,8 @@ int capaz_ctx::get_field(int field, void* dst, bool on_device, cudaStream_t s) {
   else if (field == CAPAZ_FIELD_K) {
     if (!K) return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "no per-cell K");
     src = K;
-  } else if (p.phases == 3 && (field == CAPAZ_FIELD_P_N || field == CAPAZ_FIELD_P_G) && steps_done > 0) {
+  } else if (p.phases == 3 && p.model != CAPAZ_MODEL_ENERGY && (field == CAPAZ_FIELD_P_N || field == CAPAZ_FIELD_P_G) &&
+             steps_done > 0) {
     int st = derived(field, s);
     if (st) return st;
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
@@ -816,6 +838,11 @@ int capaz_ctx::init_state(cudaStream_t s) {
   const int nstate = p.phases == 2 ? 2 : 5;
   for (int q = 0; q < nstate; q++) {
     int st = set_field(fields[q], src[q], false, s);
+    if (st) return st;
+  }
+  if (p.model == CAPAZ_MODEL_ENERGY) {
+    std::vector<double> T(n, ENERGY_T_INIT);
+    int st = set_field(CAPAZ_FIELD_T, T.data(), false, s);
     if (st) return st;
   }
   return CAPAZ_OK;

@@ -13,10 +13,13 @@ struct capaz_ctx {
   int device = 0;
   long long n = 0;
   // State ping-pong buffers: state[buffer][slot], slots P_w, S_n, S_w, P_n,
-  // P_g (the last three for three-phase only).  `cur` holds the current
-  // state; after a step the other buffer holds the start-of-step state, from
-  // which derived fields are materialised.
-  void* state[2][5] = {{nullptr}};
+  // P_g (the last three for three-phase only), T (energy model).  `cur`
+  // holds the current state; after a step the other buffer holds the
+  // start-of-step state, from which derived fields are materialised.  The
+  // energy model steps buffer `cur` in place and keeps the reference's other
+  // arrays of the last step in `ework` (EW_COUNT fields).
+  void* state[2][6] = {{nullptr}};
+  double* ework = nullptr;
   int cur = 0;
   long long steps_done = 0;
   void* m = nullptr;
@@ -61,6 +64,7 @@ struct capaz_ctx {
       case CAPAZ_FIELD_S_W: return 2;
       case CAPAZ_FIELD_P_N: return 3;
       case CAPAZ_FIELD_P_G: return 4;
+      case CAPAZ_FIELD_T: return 5;
       default: return -1;
     }
   }

@@ -189,6 +189,22 @@ cudaError_t launch_derived2_fp64(const Step2Const& c, int field, const double* P
                                  cudaStream_t s);
 int step2_grid_blocks(const Step2Const& c);
 
+// Three-phase with the energy equation (step3e.cu).  The state is updated in
+// place; `work` holds EW_COUNT arrays of ncell doubles, the reference's other
+// per-cell arrays as they stand after the last step.
+struct EnergyState {
+  double *Pw, *Sn, *Sw, *Pn, *Pg, *T;
+};
+enum EnergyWork {
+  EW_SG, EW_RO_W, EW_RO_N, EW_RO_G, EW_XI_W, EW_XI_N, EW_XI_G,
+  EW_UX_W, EW_UY_W, EW_UZ_W, EW_UX_N, EW_UY_N, EW_UZ_N, EW_UX_G, EW_UY_G, EW_UZ_G,
+  EW_ROS_W, EW_ROS_N, EW_ROS_G, EW_ROS_W_OLD, EW_ROS_N_OLD, EW_ROS_G_OLD,
+  EW_H_W, EW_H_N, EW_H_G, EW_H_R, EW_E, EW_E_NEW, EW_LAM, EW_COUNT
+};
+constexpr double ENERGY_T_INIT = 285.;  // data_initialization, three-phase.cpp:487
+cudaError_t launch_step3_energy(const Step3Const& c, const EnergyState& st, const double* m, const double* K,
+                                double* work, unsigned int* err, cudaStream_t s);
+
 // Buckley-Leverett task (step_bl.cu): the two-phase constants plus the
 // wells' rate and pressures.
 struct BLConst {

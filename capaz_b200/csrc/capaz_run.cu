@@ -14,6 +14,19 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
   if (e != cudaSuccess) return fail_cuda(e, "cudaSetDevice");
   if (nsteps == 0) return CAPAZ_OK;
   const bool diag = (p.flags & CAPAZ_FLAG_DIAGNOSTICS) != 0;
+  if (p.model == CAPAZ_MODEL_ENERGY) {
+    const Step3Const c = make_step3_const(p);
+    const EnergyState st{(double*)state[cur][0], (double*)state[cur][1], (double*)state[cur][2],
+                         (double*)state[cur][3], (double*)state[cur][4], (double*)state[cur][5]};
+    const double* Kp = (p.flags & CAPAZ_FLAG_PERCELL_K) ? (const double*)K : nullptr;
+    for (int t = 0; t < nsteps; t++) {
+      e = launch_step3_energy(c, st, (const double*)m, Kp, ework, err_flag, s);
+      launches += 5;
+      if (e != cudaSuccess) return fail_cuda(e, "step3_energy launch");
+      steps_done++;
+    }
+    return CAPAZ_OK;
+  }
   if (p.model == CAPAZ_MODEL_BUCKLEY_LEVERETT) {
     const BLConst b = make_bl_const(p);
     const bool percell = (p.flags & CAPAZ_FLAG_PERCELL_K) != 0;
@@ -152,6 +165,44 @@ int capaz_ctx::derived(int field, cudaStream_t s, bool from_current) {
   if (st) return st;
   // Start-of-step state of the last step (the current state before any step).
   const int src = (steps_done > 0 && !from_current) ? (cur ^ 1) : cur;
+  if (p.model == CAPAZ_MODEL_ENERGY) {
+    // The reference's arrays as the last step left them (zero before the
+    // first step); P_n, P_g are state arrays of this model.
+    int slot = -1;
+    switch (field) {
+      case CAPAZ_FIELD_S_G: slot = EW_SG; break;
+      case CAPAZ_FIELD_RO_W: slot = EW_RO_W; break;
+      case CAPAZ_FIELD_RO_N: slot = EW_RO_N; break;
+      case CAPAZ_FIELD_RO_G: slot = EW_RO_G; break;
+      case CAPAZ_FIELD_XI_W: slot = EW_XI_W; break;
+      case CAPAZ_FIELD_XI_N: slot = EW_XI_N; break;
+      case CAPAZ_FIELD_XI_G: slot = EW_XI_G; break;
+      case CAPAZ_FIELD_ROS_W: slot = EW_ROS_W; break;
+      case CAPAZ_FIELD_ROS_N: slot = EW_ROS_N; break;
+      case CAPAZ_FIELD_ROS_G: slot = EW_ROS_G; break;
+      case CAPAZ_FIELD_ROS_W_OLD: slot = EW_ROS_W_OLD; break;
+      case CAPAZ_FIELD_ROS_N_OLD: slot = EW_ROS_N_OLD; break;
+      case CAPAZ_FIELD_ROS_G_OLD: slot = EW_ROS_G_OLD; break;
+      case CAPAZ_FIELD_H_W: slot = EW_H_W; break;
+      case CAPAZ_FIELD_H_N: slot = EW_H_N; break;
+      case CAPAZ_FIELD_H_G: slot = EW_H_G; break;
+      case CAPAZ_FIELD_H_R: slot = EW_H_R; break;
+      case CAPAZ_FIELD_E: slot = EW_E; break;
+      case CAPAZ_FIELD_E_NEW: slot = EW_E_NEW; break;
+      default:
+        if (field >= CAPAZ_FIELD_UX_W && field <= CAPAZ_FIELD_UZ_G) slot = EW_UX_W + (field - CAPAZ_FIELD_UX_W);
+        break;
+    }
+    const void* from = slot >= 0 ? (const void*)(ework + (size_t)slot * n)
+                                 : (field == CAPAZ_FIELD_P_N || field == CAPAZ_FIELD_P_G)
+                                       ? state[cur][state_slot(field)]
+                                       : nullptr;
+    if (!from) return fail_msg(CAPAZ_ERR_INVALID_ARGUMENT, "field not kept by the energy model");
+    cudaError_t e = cudaMemcpyAsync(scratch, from, n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return fail_cuda(e, "derived copy");
+    return CAPAZ_OK;
+  }
+  if (field >= CAPAZ_FIELD_T) return fail_msg(CAPAZ_ERR_INVALID_ARGUMENT, "energy fields exist in the energy model only");
   if (p.model == CAPAZ_MODEL_BUCKLEY_LEVERETT) {
     if (field == CAPAZ_FIELD_S_G || field == CAPAZ_FIELD_RO_G || field == CAPAZ_FIELD_XI_G ||
         field == CAPAZ_FIELD_UX_G || field == CAPAZ_FIELD_UY_G || field == CAPAZ_FIELD_UZ_G ||

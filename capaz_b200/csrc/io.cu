@@ -40,7 +40,7 @@ int fetch(capaz_ctx* ctx, int field, std::vector<double>& out) {
 }
 
 struct PlotFields {
-  std::vector<double> Pw, Sn, Sw, Sg, m, K, uxw, uyw, uzw, uxn, uyn, uzn, uxg, uyg, uzg;
+  std::vector<double> Pw, Sn, Sw, Sg, m, K, T, uxw, uyw, uzw, uxn, uyn, uzn, uxg, uyg, uzg;
 };
 
 // One row of print_plot_row for cell l = (i, j, k).
@@ -65,6 +65,21 @@ void plot_row(const capaz_params& p, const PlotFields& F, int i, int j, int k, s
     else
       n = snprintf(buf, sizeof buf, "%.2e %.2e %.2e %.3e %.3e %.3e %.3e %.3e %.3e\n", I * (p.hx), K * (p.hz),
                    J * (p.hy), F.Sn[l], F.Pw[l], F.uxn[l], F.uzn[l], (-1) * F.uyn[l], F.m[l]);
+  } else if (p.model == CAPAZ_MODEL_ENERGY) {
+    // The ENERGY branch of print_plot_row (main.cpp:707-747): T after P_w.
+    if (p.nz < 2 && p.nx < 2)
+      n = snprintf(buf, sizeof buf, "%.2e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e\n", J * (p.hy), F.Sw[l], F.Sn[l],
+                   F.Sg[l], F.Pw[l], F.T[l], (-1) * F.uyw[l], (-1) * F.uyn[l], (-1) * F.uyg[l], F.m[l]);
+    else if (p.nz < 2)
+      n = snprintf(buf, sizeof buf, "%.2e %.2e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e\n",
+                   I * (p.hx), J * (p.hy), F.Sw[l], F.Sn[l], F.Sg[l], F.Pw[l], F.T[l], F.uxw[l], (-1) * F.uyw[l],
+                   F.uxn[l], (-1) * F.uyn[l], F.uxg[l], (-1) * F.uyg[l], F.m[l]);
+    else
+      n = snprintf(buf, sizeof buf,
+                   "%.2e %.2e %.2e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e\n",
+                   I * (p.hx), K * (p.hz), J * (p.hy), F.Sw[l], F.Sn[l], F.Sg[l], F.Pw[l], F.T[l], F.uxw[l],
+                   F.uzw[l], (-1) * F.uyw[l], F.uxn[l], F.uzn[l], (-1) * F.uyn[l], F.uxg[l], F.uzg[l],
+                   (-1) * F.uyg[l], F.m[l]);
   } else if (p.nz < 2 && p.nx < 2) {
     n = snprintf(buf, sizeof buf, "%.2e %.5e %.5e %.5e %.5e %.5e %.5e %.5e %.5e\n", J * (p.hy), F.Sw[l], F.Sn[l],
                  F.Sg[l], F.Pw[l], (-1) * F.uyw[l], (-1) * F.uyn[l], (-1) * F.uyg[l], F.m[l]);
@@ -85,6 +100,22 @@ void plot_header(const capaz_params& p, double t, std::string& out) {
   char buf[512];
   snprintf(buf, sizeof buf, "TITLE =  \"Filtration in time=%5.2f\" \n", t);
   out += buf;
+  if (p.model == CAPAZ_MODEL_ENERGY) {
+    if (p.nz < 2 && p.nx < 2) {
+      out += "VARIABLES = \"Y\",\"S_w\",\"S_n\",\"S_g\",\"P_w\",\"T\",\"uw_y\",\"un_y\",\"ug_y\",\"porosity\" \n";
+      snprintf(buf, sizeof buf, "ZONE T = \"BIG ZONE\", K=%d, F = POINT\n", p.ny);
+    } else if (p.nz < 2) {
+      out += "VARIABLES = \"X\",\"Y\",\"S_w\",\"S_n\",\"S_g\",\"P_w\",\"T\",\"uw_x\",\"uw_y\",\"un_x\",\"un_y\","
+             "\"ug_x\",\"ug_y\",\"porosity\" \n";
+      snprintf(buf, sizeof buf, "ZONE T = \"BIG ZONE\", K=%d,J=%d, F = POINT\n", p.nx, p.ny);
+    } else {
+      out += "VARIABLES = \"X\",\"Y\",\"Z\",\"S_w\",\"S_n\",\"S_g\",\"P_w\",\"T\",\"uw_x\",\"uw_y\",\"uw_z\","
+             "\"un_x\",\"un_y\",\"un_z\",\"ug_x\",\"ug_y\",\"ug_z\",\"porosity\" \n";
+      snprintf(buf, sizeof buf, "ZONE T = \"BIG ZONE\", K=%d,J=%d,I=%d, F = POINT\n", p.nx, p.ny, p.nz);
+    }
+    out += buf;
+    return;
+  }
   if (p.nz < 2) {
     if (p.nx < 2) {
       out += p.phases == 3
@@ -131,6 +162,7 @@ int capaz_write_plot(capaz_ctx* ctx, const char* dir, double t) {
                          {CAPAZ_FIELD_UY_G, &F.uyg}, {CAPAZ_FIELD_UZ_G, &F.uzg}};
     want.insert(want.end(), std::begin(more), std::end(more));
   }
+  if (p.model == CAPAZ_MODEL_ENERGY) want.push_back({CAPAZ_FIELD_T, &F.T});
   if (p.model == CAPAZ_MODEL_BUCKLEY_LEVERETT) {
     if (p.flags & CAPAZ_FLAG_PERCELL_K) want.push_back({CAPAZ_FIELD_K, &F.K});
     else F.K.assign(ctx->n, p.K0);

@@ -19,36 +19,20 @@
 #include <math.h>
 
 #include "capaz_internal.h"
+#include "phys3.cuh"
 
 namespace capaz {
 namespace {
+
+using phys3::directed;
+using phys3::k_g3;
+using phys3::k_n3;
+using phys3::k_w3;
 
 struct Plane3 {
   double Pw[PC], Pn[PC], Pg[PC], ro_w[PC], ro_n[PC], ro_g[PC], Xi_w[PC], Xi_n[PC], Xi_g[PC];
 };
 constexpr size_t kSmem3 = 3 * sizeof(Plane3);
-
-// Relative permeabilities, three-phase.cpp:146-186.
-__device__ __forceinline__ double k_w3(double S_w_e, double A) {
-  double k_w = 0;
-  if (S_w_e >= 1e-3) k_w = pow(S_w_e, 0.5) * pow(1. - pow(1. - pow(S_w_e, A / (A - 1.)), (A - 1.) / A), 2.);
-  return k_w;
-}
-__device__ __forceinline__ double k_g3(double S_g_e, double A) {
-  double k_g = 0;
-  if (S_g_e >= 1e-3) k_g = pow(S_g_e, 0.5) * pow(1. - pow(1. - S_g_e, A / (A - 1.)), 2. * (A - 1.) / A);
-  return k_g;
-}
-__device__ __forceinline__ double k_n3(double S_w_e, double S_n_e, double A) {
-  double k_n = 0;
-  double S_g_e = 1. - S_w_e - S_n_e;
-  if (S_n_e >= 1e-3) {
-    double k_n_w = pow(1. - S_w_e, 0.5) * pow(1. - pow(S_w_e, A / (A - 1.)), 2. * (A - 1.) / A);
-    double k_n_g = pow(S_n_e, 0.5) * pow(1. - pow(1. - pow(S_n_e, A / (A - 1.)), (A - 1.) / A), 2.);
-    k_n = S_n_e * k_n_w * k_n_g / (1 - S_w_e) / (1 - S_g_e);
-  }
-  return k_n;
-}
 
 __device__ __forceinline__ bool interior3(const Step3Const& c, int i, int j, int k) {
   return (((i != 0) && (i != c.nx - 1)) || (c.nx < 2)) && (j != 0) && (j != c.ny - 1) &&
@@ -84,64 +68,6 @@ __device__ __forceinline__ D3 derive3(const Step3Const& c, double Pw, double Sw,
   o.ro_n = c.ro0_n * (1. + (c.beta_n) * (o.Pn - c.P_atm));
   o.ro_g = c.ro0_g * o.Pg / c.P_atm;
   return o;
-}
-
-__device__ __forceinline__ double directed(double x1, double x2, double Xc, double rc, double Xm, double rm,
-                                           double Xp, double rp, double h) {
-  return (((x2 + fabs(x2)) / 2. - (x1 - fabs(x1)) / 2.) * (-1.) * Xc * rc -
-          (x1 + fabs(x1)) / 2. * (-1.) * Xm * rm + (x2 - fabs(x2)) / 2. * (-1.) * Xp * rp) /
-         h;
-}
-
-// reverse_matrix for n = 3 (gauss.cpp:6-92): Gauss-Jordan on [a | I] that
-// looks for another pivot row only when |pivot| < 1e-8, taking the last row
-// below with entry > 1e-8.  Returns false where the reference reports a zero
-// determinant (it then leaves `a` unchanged).
-__device__ __forceinline__ bool reverse_matrix3(double* a) {
-  const double e = 1E-8;
-  double matr[3][6];
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      matr[i][j] = a[j + 3 * i];
-      matr[i][j + 3] = (j == i) ? 1 : 0;
-    }
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    double f = matr[k][k];
-    if (fabs(f) < e) {
-      int det_flag = 0;
-#pragma unroll
-      for (int i = k + 1; i < 3; i++) {
-        if (matr[i][k] > e) {
-          det_flag = 1;
-#pragma unroll
-          for (int j = 0; j < 6; j++) {
-            double row = matr[k][j];
-            matr[k][j] = matr[i][j];
-            matr[i][j] = row;
-          }
-          f = matr[k][k];
-        }
-      }
-      if (det_flag == 0) return false;
-    }
-#pragma unroll
-    for (int j = 0; j < 6; j++) matr[k][j] /= f;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-      if (i != k) {
-        double f1 = matr[i][k];
-#pragma unroll
-        for (int j = 0; j < 6; j++) matr[i][j] -= (matr[k][j] * f1);
-      }
-  }
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-#pragma unroll
-    for (int j = 0; j < 3; j++) a[j + 3 * i] = matr[i][j + 3];
-  return true;
 }
 
 __device__ __forceinline__ bool in_window3(const Step3Const& c, int i, int k) {
@@ -278,7 +204,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         dF[2] = 0;
         dF[5] = c.ro0_n * (1. + c.beta_n * (Pw + Pk_nw - c.P_atm));
         dF[8] = (-1) * c.ro0_g * (Pw + Pk_nw + Pk_gn - Sg * PkSn) / c.P_atm;
-        reverse_matrix3(dF);
+        phys3::reverse_matrix<3>(dF);
         double nPw = Pw - (dF[0] * F1 + dF[1] * F2 + dF[2] * F3);
         double nSw = Sw - (dF[3] * F1 + dF[4] * F2 + dF[5] * F3);
         double nSn = Sn - (dF[6] * F1 + dF[7] * F2 + dF[8] * F3);

@@ -87,6 +87,20 @@ def test_validate_buckley_leverett_model():
         assert lib.capaz_params_validate(C.byref(p)) == code, bad
 
 
+def test_validate_energy_model():
+    """The energy equation is the three-phase FP64 step with T; no
+    diagnostics, no z-slab placement (its stencil reaches two cells)."""
+    lib = native.load()
+    ok = dict(model=native.MODEL_ENERGY, phases=3, nx=9, ny=8, nz=6)
+    assert lib.capaz_params_validate(C.byref(default_params(**ok))) == native.OK
+    assert lib.capaz_params_validate(C.byref(default_params(**dict(ok, nx=1, nz=1)))) == native.OK
+    for bad, code in [(dict(phases=2), native.ERR_UNSUPPORTED), (dict(form=native.FORM_FP32C), native.ERR_UNSUPPORTED),
+                      (dict(flags=native.FLAG_DIAGNOSTICS), native.ERR_UNSUPPORTED),
+                      (dict(z_offset=1, nz_global=8), native.ERR_UNSUPPORTED)]:
+        p = default_params(**dict(ok, **bad))
+        assert lib.capaz_params_validate(C.byref(p)) == code, bad
+
+
 def test_ini_round_trip_buckley_leverett(tmp_path):
     p = default_params(nx=20, ny=15, model=native.MODEL_BUCKLEY_LEVERETT, Q=3.5e-6, background_Pw=3e5,
                        background_Sn=0.7, injwell_Pw=2e5, outwell_Pw=0.9e5)

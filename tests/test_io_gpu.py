@@ -17,7 +17,8 @@ pytestmark = pytest.mark.gpu
 
 MAIN_REF = {2: os.path.join(ROOT, "oracle", "_ref", "capaz_ref_main_2ph"),
             3: os.path.join(ROOT, "oracle", "_ref", "capaz_ref_main_3ph"),
-            "bl": os.path.join(ROOT, "oracle", "_ref", "capaz_ref_main_bl")}
+            "bl": os.path.join(ROOT, "oracle", "_ref", "capaz_ref_main_bl"),
+            "energy": os.path.join(ROOT, "oracle", "_ref", "capaz_ref_main_3phe")}
 
 
 def params3(**kw):
@@ -33,7 +34,7 @@ def reference_plots(p, tmp_path, save_every, noise=None):
     """Runs the reference's whole program (its own main and CPU backend) and
     returns its plot files.  `noise`: the permeability file of the B_L build
     (read from ../noise.dat)."""
-    exe = MAIN_REF["bl" if p.model == native.MODEL_BUCKLEY_LEVERETT else p.phases]
+    exe = MAIN_REF[{native.MODEL_BUCKLEY_LEVERETT: "bl", native.MODEL_ENERGY: "energy"}.get(p.model, p.phases)]
     if not os.path.exists(exe):
         pytest.skip("reference whole-program binaries not built (make -C oracle ref)")
     ini = O.ref_ini_text(p).replace("SAVE_PLOTS=1000000", f"SAVE_PLOTS={save_every}")
@@ -102,6 +103,14 @@ def test_plot_file_matches_reference_program_buckley_leverett(tmp_path, shape, g
     noise = str(tmp_path / "noise.dat")
     write_noise(noise, np.random.default_rng(nx).normal(-1.5, 0.6, size=(ny, nx)), nz)
     compare(reference_plots(p, tmp_path, 20, noise), our_plots(p, tmp_path, 20, 2, noise))
+
+
+@pytest.mark.parametrize("shape", [(9, 8, 6), (1, 15, 1), (11, 7, 1)])
+def test_plot_file_matches_reference_program_energy(tmp_path, shape):
+    """The THREE_PHASE + ENERGY build's plot rows (T after P_w)."""
+    nx, ny, nz = shape
+    p = params3(nx=nx, ny=ny, nz=nz, dt=1e-3, timeX=0.06, model=native.MODEL_ENERGY)
+    compare(reference_plots(p, tmp_path, 30), our_plots(p, tmp_path, 30, 2))
 
 
 def write_noise(path, values, nz=1):
