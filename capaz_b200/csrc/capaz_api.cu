@@ -12,6 +12,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -844,6 +845,22 @@ int capaz_ctx::init_state(cudaStream_t s) {
     std::vector<double> T(n, ENERGY_T_INIT);
     int st = set_field(CAPAZ_FIELD_T, T.data(), false, s);
     if (st) return st;
+    // The other arrays data_initialization fills (S_local_initialization and
+    // the densities, three-phase.cpp:429-434, 479-481), which the energy
+    // model's derived fields show until the first step.
+    std::vector<double> Sg(n), rw(n), rn(n), rg(n);
+    for (long long l = 0; l < n; l++) {
+      Sg[l] = 1. - p.S_w_init - p.S_n_init;
+      rw[l] = p.ro0_w * (1. + (p.beta_w) * (Pw[l] - p.P_atm));
+      rn[l] = p.ro0_n * (1. + (p.beta_n) * (Pn[l] - p.P_atm));
+      rg[l] = p.ro0_g * Pg[l] / p.P_atm;
+    }
+    const std::pair<int, const std::vector<double>*> put[4] = {{EW_SG, &Sg}, {EW_RO_W, &rw}, {EW_RO_N, &rn},
+                                                               {EW_RO_G, &rg}};
+    for (const auto& q : put)
+      CUDA_TRY(this, cudaMemcpyAsync(ework + (size_t)q.first * n, q.second->data(), n * sizeof(double),
+                                     cudaMemcpyHostToDevice, s));
+    CUDA_TRY(this, cudaStreamSynchronize(s));
   }
   return CAPAZ_OK;
 }
