@@ -72,6 +72,7 @@ def parse():
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-three-phase", action="store_true")
+    ap.add_argument("--no-physics", action="store_true", help="skip the Buckley-Leverett and energy legs")
     ap.add_argument("--decompose", action="store_true",
                     help="split the one grid into z-slabs over the N GPUs (strong scaling, NCCL halo "
                          "exchange every step) instead of one replica per GPU")
@@ -370,6 +371,99 @@ def three_phase_leg(dev, steps: int = 200, warmup: int = 5) -> dict:
                                                                   "7 Newton iterations with Gauss-Jordan)"}
 
 
+def _leg_timing(sim, dev, steps: int, warmup: int):
+    """ms per step of `sim` over `steps` steps after `warmup` (CUDA events on
+    one stream) and the launches counted inside."""
+    import torch
+    st = torch.cuda.Stream(device=dev)
+    sim.step(warmup, st.cuda_stream)
+    torch.cuda.synchronize()
+    l0 = sim.launch_count
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    sim.step(steps, st.cuda_stream)
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, sim.launch_count - l0
+
+
+def bl_leg(dev, steps: int = 200, warmup: int = 5) -> dict:
+    """Buckley-Leverett task (the reference's B_L build) on a 1000x1000 plane
+    (100 times the reference's 100x100), dt 2000 s, K = 1e-10 exp(v) with v a
+    seeded Gaussian field (mean -1.5, sd 0.6, correlation 8 cells) standing in
+    for the reference's noise.dat; the reference's fluids and wells.  GPU
+    cell-steps/s with the state in HBM; cpu_baseline: the oracle (the
+    restatement pinned to the reference) on a 200x200 sample, all host
+    threads."""
+    from capaz_b200 import Simulation
+    from capaz_b200.configs import grf
+    from capaz_b200.simulation import buckley_leverett_params
+    p = buckley_leverett_params(nx=1000, ny=1000, nz=1, dt=2000.0)
+    K = (1e-10 * np.exp(-1.5 + 0.6 * grf((p.ny, p.nx), 8.0, 7)))[None]
+    with Simulation(p, device=dev) as sim:
+        sim.set_field("K", K)
+        sim.init_state()
+        ms, launches = _leg_timing(sim, dev, steps, warmup)
+        S = sim.get_field("S_n")
+    out = {"workload": "Buckley-Leverett 1000x1000x1, dt 2000 s, lognormal K, reference wells and fluids, FP64",
+           "value": p.ncell / (ms * 1e-3), "unit": "cell-steps/s", "ms_per_step": ms, "steps": steps,
+           "launches": launches, "finite": bool(np.isfinite(S).all()),
+           "kernel": "step_bl_interior_kernel + step_bl_boundary_kernel"}
+    try:
+        from oracle import oracle as O
+        q = buckley_leverett_params(nx=200, ny=200, nz=1, dt=2000.0)
+        Kq = (1e-10 * np.exp(-1.5 + 0.6 * grf((q.ny, q.nx), 8.0, 7)))[None]
+        st = O.init(q)
+        n = 100
+        t0 = time.perf_counter()
+        O.step(q, {"P_w": st["P_w"], "S_n": st["S_n"]}, n, st["m"], Kq)
+        sec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": q.ncell * n / sec, "unit": "cell-steps/s", "cores": O.max_threads(),
+                               "kind": "port", "sample": f"200x200x1, {n} steps"}
+    except Exception as e:  # the CPU figure is optional
+        out["cpu_baseline"] = {"unavailable": str(e)}
+    return out
+
+
+def energy_leg(dev, steps: int = 100, warmup: int = 3) -> dict:
+    """Three-phase with the energy equation (the reference's THREE_PHASE +
+    ENERGY build) on the config-2 grid (192x192x96, gravity on z, lognormal
+    K, 3x3 NAPL source), T = 285 K initially with 400 K / 273 K top and
+    bottom rows.  GPU cell-steps/s; cpu_baseline: the oracle on a 32x24x32
+    sample, all host threads (the reference has this build on the CPU only)."""
+    from capaz_b200 import Simulation
+    from capaz_b200.configs import config2, heterogeneous_fields, stable_dt, three_phase_params
+    w = config2()
+    p = w.params.copy()
+    p.model = native.MODEL_ENERGY
+    with Simulation(p, device=dev) as sim:
+        sim.set_field("m", w.m)
+        sim.set_field("K", w.K)
+        sim.init_state()
+        ms, launches = _leg_timing(sim, dev, steps, warmup)
+        T = sim.get_field("T")
+    out = {"workload": f"energy equation, cfg2 grid {w.notes['workload_grid']}, FP64, dt {p.dt:.3g} s",
+           "value": p.ncell / (ms * 1e-3), "unit": "cell-steps/s", "ms_per_step": ms, "steps": steps,
+           "launches": launches, "finite": bool(np.isfinite(T).all()),
+           "kernel": "energy_{derive,velocity,balance,newton,boundary}_kernel"}
+    try:
+        from oracle import oracle as O
+        q = three_phase_params(32, 24, 32)
+        q.model = native.MODEL_ENERGY
+        mq, Kq = heterogeneous_fields((q.nz, q.ny, q.nx), 1.0, 8.0, 2)
+        q.dt = stable_dt(q, mq, Kq)
+        st = O.init(q, mq)
+        n = 50
+        t0 = time.perf_counter()
+        O.step(q, {k: st[k] for k in ("P_w", "S_w", "S_n", "P_n", "P_g", "T")}, n, mq, Kq)
+        sec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": q.ncell * n / sec, "unit": "cell-steps/s", "cores": O.max_threads(),
+                               "kind": "port", "sample": f"32x24x32, {n} steps"}
+    except Exception as e:  # the CPU figure is optional
+        out["cpu_baseline"] = {"unavailable": str(e)}
+    return out
+
+
 def adjoint_leg(dev) -> dict:
     """Differentiation form on the config-4 inverse problem (128x128x64,
     FP64, 500 steps, checkpoints every 50): time of one forward solve vs. one
@@ -557,6 +651,19 @@ def run_capaz(args) -> None:
         except Exception as e:  # reported, never fatal to the headline line
             three = {"failed": str(e)}
 
+    # ---- Buckley-Leverett task and energy equation ---------------------------
+    bl = energy = None
+    if not args.no_physics and ws == 1:
+        for name, fn in (("bl", bl_leg), ("energy", energy_leg)):
+            try:
+                r = fn(dev)
+            except Exception as e:  # reported, never fatal to the headline line
+                r = {"failed": str(e)}
+            if name == "bl":
+                bl = r
+            else:
+                energy = r
+
     # ---- differentiation form (config 4) ------------------------------------
     adj = None
     if not args.no_adjoint and ws == 1:
@@ -651,6 +758,8 @@ def run_capaz(args) -> None:
             "precision": prec,
             "adjoint": adj,
             "three_phase": three,
+            "buckley_leverett": bl,
+            "energy": energy,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": t["launches"],
         }
         print(json.dumps(line), flush=True)
