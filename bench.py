@@ -431,7 +431,7 @@ def energy_leg(dev, steps: int = 100, warmup: int = 3) -> dict:
     K, 3x3 NAPL source), T = 285 K initially with 400 K / 273 K top and
     bottom rows.  GPU cell-steps/s; cpu_baseline: the oracle on a 32x24x32
     sample, all host threads (the reference has this build on the CPU only)."""
-    from capaz_b200 import Simulation
+    from capaz_b200 import Simulation, native
     from capaz_b200.configs import config2, heterogeneous_fields, stable_dt, three_phase_params
     w = config2()
     p = w.params.copy()
