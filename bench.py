@@ -73,6 +73,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-three-phase", action="store_true")
     ap.add_argument("--no-physics", action="store_true", help="skip the Buckley-Leverett and energy legs")
+    ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--decompose", action="store_true",
                     help="split the one grid into z-slabs over the N GPUs (strong scaling, NCCL halo "
                          "exchange every step) instead of one replica per GPU")
@@ -464,6 +465,68 @@ def energy_leg(dev, steps: int = 100, warmup: int = 3) -> dict:
     return out
 
 
+def ensemble_leg(dev, steps: int = 300, warmup: int = 3) -> dict:
+    """Batching form on the config-3 ensemble (64 two-phase instances, dims
+    per axis from {32, 48, 64, 96, 128}, own lognormal K and dt each, 300
+    steps): one persistent launch per step over all instances, the step
+    pair replayed as a CUDA graph, tile z-chunk and CTAs per SM autotuned;
+    against the same 64 instances stepped one after another as separate
+    contexts (precision form, and the plain FP64 path).  GPU time by CUDA
+    events on one stream; aggregate cell-steps/s."""
+    import torch
+
+    from capaz_b200 import Ensemble, Simulation, native
+    from capaz_b200.configs import config3
+    ws = config3(form=native.FORM_FP32C)
+    cells = sum(w.params.ncell for w in ws)
+    st = torch.cuda.Stream(device=dev)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    with Ensemble([w.params for w in ws], device=dev) as ens:
+        for sim, w in zip(ens.instances, ws):
+            sim.set_field("m", w.m)
+            sim.set_field("K", w.K)
+            sim.init_state()
+        tune = ens.autotune(st.cuda_stream)
+        ens.step(warmup, st.cuda_stream)
+        torch.cuda.synchronize()
+        l0 = ens.launch_count
+        batch_ms = timed(lambda: ens.step(steps, st.cuda_stream))
+        launches = ens.launch_count - l0
+        finite = all(bool(np.isfinite(s.get_field("S_n")).all()) for s in ens.instances)
+
+    def sequential(form):
+        total = 0.0
+        for w in ws:
+            q = w.params.copy()
+            q.form = form
+            with Simulation(q, device=dev) as sim:
+                sim.set_field("m", w.m)
+                sim.set_field("K", w.K)
+                sim.init_state()
+                sim.step(warmup, st.cuda_stream)
+                torch.cuda.synchronize()
+                total += timed(lambda: sim.step(steps, st.cuda_stream))
+        return total
+
+    seq32 = sequential(native.FORM_FP32C)
+    seq64 = sequential(native.FORM_FP64)
+    rate = lambda ms: cells * steps / (ms * 1e-3)  # noqa: E731
+    return {"workload": f"cfg3 ensemble, {len(ws)} instances, {cells} cells, {steps} steps, precision form",
+            "value": rate(batch_ms), "unit": "cell-steps/s", "ms_per_step": batch_ms / steps,
+            "launches": launches, "autotune": tune, "finite": finite,
+            "sequential_fp32c": {"value": rate(seq32), "ms_per_step": seq32 / steps},
+            "sequential_fp64": {"value": rate(seq64), "ms_per_step": seq64 / steps},
+            "speedup_vs_sequential_fp32c": seq32 / batch_ms, "speedup_vs_sequential_fp64": seq64 / batch_ms}
+
+
 def adjoint_leg(dev) -> dict:
     """Differentiation form on the config-4 inverse problem (128x128x64,
     FP64, 500 steps, checkpoints every 50): time of one forward solve vs. one
@@ -664,6 +727,14 @@ def run_capaz(args) -> None:
             else:
                 energy = r
 
+    # ---- batching form (config 3) --------------------------------------------
+    ens = None
+    if not args.no_ensemble and ws == 1:
+        try:
+            ens = ensemble_leg(dev)
+        except Exception as e:  # reported, never fatal to the headline line
+            ens = {"failed": str(e)}
+
     # ---- differentiation form (config 4) ------------------------------------
     adj = None
     if not args.no_adjoint and ws == 1:
@@ -758,6 +829,7 @@ def run_capaz(args) -> None:
             "precision": prec,
             "adjoint": adj,
             "three_phase": three,
+            "ensemble": ens,
             "buckley_leverett": bl,
             "energy": energy,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": t["launches"],
