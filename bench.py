@@ -336,40 +336,61 @@ def precision_check(w, dev, steps):
 
 
 def three_phase_leg(dev, steps: int = 200, warmup: int = 5) -> dict:
-    """Three-phase FP64 step on the config-2 workload (192x192x96, gravity on
-    z, lognormal K, 3x3 NAPL source): cell-steps/s over `steps` steps with
-    the state in HBM (CUDA events), and the kernel's algorithmic HBM bytes
-    (64 B/cell-step: P_w, S_w, S_n, m, K read, P_w, S_w, S_n written)."""
+    """Three-phase step on the config-2 workload (192x192x96, gravity on z,
+    lognormal K, 3x3 NAPL source): cell-steps/s of the plain FP64 path and of
+    the precision form (FP32 storage and stencil, FP64 Newton) over `steps`
+    steps with the state in HBM (CUDA events), the kernels' algorithmic HBM
+    bytes (FP64: 64 B/cell-step, P_w, S_w, S_n, m, K read and P_w, S_w, S_n
+    written; FP32: 32 B), and the precision form's error against the FP64
+    path after the workload's 500 steps from the same initial state."""
     import torch
 
-    from capaz_b200 import Simulation
+    from capaz_b200 import Simulation, native
     from capaz_b200.configs import config2
     w = config2()
     p = w.params
-    with Simulation(p, device=dev) as sim:
-        sim.set_field("m", w.m)
-        sim.set_field("K", w.K)
-        sim.init_state()
-        st = torch.cuda.Stream(device=dev)
-        sim.step(warmup, st.cuda_stream)
-        torch.cuda.synchronize()
-        l0 = sim.launch_count
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        sim.step(steps, st.cuda_stream)
-        e1.record(st)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / steps
-        launches = sim.launch_count - l0
-        S = sim.get_field("S_n")
     peak, _ = measured_peaks()
-    gbs = 64 * p.ncell / (ms * 1e-3) / 1e9
-    return {"workload": f"cfg2 three-phase {w.notes['workload_grid']} (reference axes {w.notes['ref_grid']}), "
-                        f"FP64, dt {p.dt:.3g} s, per-cell K, 3x3 top source",
-            "value": p.ncell / (ms * 1e-3), "unit": "cell-steps/s", "ms_per_step": ms, "steps": steps,
-            "launches": launches, "algorithmic_bytes_per_cell": 64, "achieved_gbs": gbs, "hbm_frac": gbs / peak,
-            "finite": bool(np.isfinite(S).all()), "kernel": "step3_fp64_kernel (FP64-bound: 13 pow per cell, "
-                                                                  "7 Newton iterations with Gauss-Jordan)"}
+    out = {"workload": f"cfg2 three-phase {w.notes['workload_grid']} (reference axes {w.notes['ref_grid']}), "
+                       f"dt {p.dt:.3g} s, per-cell K, 3x3 top source"}
+    final = {}
+    for form, name, nbytes in ((native.FORM_FP64, "fp64", 64), (native.FORM_FP32C, "fp32c", 32)):
+        q = p.copy()
+        q.form = form
+        with Simulation(q, device=dev) as sim:
+            sim.set_field("m", w.m)
+            sim.set_field("K", w.K)
+            sim.init_state()
+            st = torch.cuda.Stream(device=dev)
+            sim.step(warmup, st.cuda_stream)
+            torch.cuda.synchronize()
+            l0 = sim.launch_count
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            sim.step(steps, st.cuda_stream)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            launches = sim.launch_count - l0
+            # the workload's run from the initial state, for the precision comparison
+            sim.init_state()
+            sim.step(w.steps, st.cuda_stream)
+            torch.cuda.synchronize()
+            final[name] = {k: sim.get_field(k) for k in ("P_w", "S_w", "S_n")}
+        gbs = nbytes * p.ncell / (ms * 1e-3) / 1e9
+        out[name] = {"value": p.ncell / (ms * 1e-3), "unit": "cell-steps/s", "ms_per_step": ms, "steps": steps,
+                     "launches": launches, "algorithmic_bytes_per_cell": nbytes, "achieved_gbs": gbs,
+                     "hbm_frac": gbs / peak, "finite": bool(np.isfinite(final[name]["S_n"]).all())}
+    out["value"], out["unit"], out["ms_per_step"] = out["fp64"]["value"], "cell-steps/s", out["fp64"]["ms_per_step"]
+    out["speedup_fp32c_vs_fp64"] = out["fp32c"]["value"] / out["fp64"]["value"]
+    prec = {"steps": w.steps, "against": "FP64 three-phase path (matches the reference CPU step to 1e-12)"}
+    for k in ("P_w", "S_w", "S_n"):
+        a, b = final["fp32c"][k], final["fp64"][k]
+        prec[k] = {"max_abs": float(np.abs(a - b).max()),
+                   "rel_l2": float(np.linalg.norm(a - b) / np.linalg.norm(b))}
+    out["precision"] = prec
+    out["kernel"] = ("step3_fp64_kernel (FP64-bound: 13 pow per cell, 7 Newton iterations with Gauss-Jordan); "
+                     "step3_fp32c_kernel (FP32 stencil, two FP64 Newton iterations, Cramer's rule)")
+    return out
 
 
 def _leg_timing(sim, dev, steps: int, warmup: int):

@@ -35,6 +35,7 @@ CUDA_SOURCES = [
     ("step2_fp32c.cu", []),
     ("step2_fp32c_tma.cu", []),
     ("step3_fp64.cu", ["-fmad=false"]),
+    ("step3_fp32c.cu", []),
     ("step_bl.cu", ["-fmad=false"]),
     ("step3e.cu", ["-fmad=false"]),
     ("fields.cu", []),

@@ -196,6 +196,66 @@ Step2FConst make_step2f_const(const capaz_params& p, double S_ref) {
   return c;
 }
 
+Step3FConst make_step3f_const(const capaz_params& p, double S_ref_w, double S_ref_n) {
+  const Step3Const d = make_step3_const(p);
+  Step3FConst c;
+  memset(&c, 0, sizeof c);
+  c.nx = d.nx;
+  c.ny = d.ny;
+  c.nz = d.nz;
+  c.source = d.source;
+  c.source_window = d.source_window;
+  c.win_k0 = d.win_k0;
+  c.win_k1 = d.win_k1;
+  c.tiles_x = d.tiles_x;
+  c.tiles_y = d.tiles_y;
+  c.zchunk = d.zchunk;
+  c.nzchunks = d.nzchunks;
+  c.i_lo = d.i_lo;
+  c.i_hi = d.i_hi;
+  c.a2 = p.lambda == 2.0 ? 1 : 0;
+  c.sy = d.sy;
+  c.sz = d.sz;
+  c.S_ref_w = S_ref_w;
+  c.S_ref_n = S_ref_n;
+  c.S_ref_w_f = (float)S_ref_w;
+  c.S_ref_n_f = (float)S_ref_n;
+  c.S_wr_f = (float)p.S_wr;
+  c.S_nr_f = (float)p.S_nr;
+  c.inv_den = (float)(1. / (1. - p.S_wr - p.S_nr - p.S_gr));
+  c.K0_f = (float)p.K0;
+  c.aw = p.ro0_w * p.beta_w;
+  c.an = p.ro0_n * p.beta_n;
+  c.bg = p.ro0_g / p.P_atm;
+  c.aw_f = (float)c.aw;
+  c.an_f = (float)c.an;
+  c.bg_f = (float)c.bg;
+  c.inv_mu_w_f = (float)(1. / p.mu_w);
+  c.inv_mu_n_f = (float)(1. / p.mu_n);
+  c.inv_mu_g_f = (float)(1. / p.mu_g);
+  c.inv_hx2_f = (float)(1. / (p.hx * p.hx));
+  c.inv_hy2_f = (float)(1. / (p.hy * p.hy));
+  c.inv_hz2_f = (float)(1. / (p.hz * p.hz));
+  c.g_inv_hy_f = (float)(p.g_const / p.hy);
+  c.dt_f = (float)p.dt;
+  const double A = p.lambda;
+  c.e1 = (float)(A / (A - 1.));
+  c.e2 = (float)((A - 1.) / A);
+  c.e3 = (float)(2. * (A - 1.) / A);
+  c.P_atm = p.P_atm;
+  c.ro0_w = p.ro0_w;
+  c.ro0_n = p.ro0_n;
+  c.ro0_g = p.ro0_g;
+  c.beta_w = p.beta_w;
+  c.beta_n = p.beta_n;
+  c.g = p.g_const;
+  c.hy = p.hy;
+  c.S_w_gr = p.S_w_gr;
+  c.S_n_gr = p.S_n_gr;
+  c.vol = p.hx * p.hy * p.hz;
+  return c;
+}
+
 PhysF make_physf(const capaz_params& p) {
   PhysF f;
   memset(&f, 0, sizeof f);
@@ -630,7 +690,8 @@ int capaz_ctx::allocate() {
     CUDA_TRY(this, cudaMemcpy(Pref, pref0.data(), sizeof(double) * p.ny, cudaMemcpyHostToDevice));
     CUDA_TRY(this, cudaMemcpy(PrelF, z.data(), sizeof(float) * p.ny, cudaMemcpyHostToDevice));
     CUDA_TRY(this, cudaMemcpy(dPrefF, z.data(), sizeof(float) * p.ny, cudaMemcpyHostToDevice));
-    CUDA_TRY(this, launch_row_tables(Pref, p.ny, make_physf(p), rowF, nullptr));
+    if (p.phases == 3) CUDA_TRY(this, launch_row_tables3(Pref, p.ny, make_step3f_const(p, 0., 0.), rowF, nullptr));
+    else CUDA_TRY(this, launch_row_tables(Pref, p.ny, make_physf(p), rowF, nullptr));
   }
   CUDA_TRY(this, cudaMalloc(&first_bad, sizeof(unsigned long long)));
   CUDA_TRY(this, cudaMalloc(&sum_parts, sizeof(double) * 1024));
@@ -687,7 +748,7 @@ void capaz_ctx::release() {
   if (S_ref_dev) cudaFree(S_ref_dev);
   if (PrelF) cudaFree(PrelF);
   if (dPrefF) cudaFree(dPrefF);
-  for (int q = 0; q < 4; q++)
+  for (int q = 0; q < 7; q++)
     if (wide[q]) cudaFree(wide[q]);
   if (host_stage) cudaFreeHost(host_stage);
 }
@@ -737,9 +798,33 @@ int capaz_ctx::set_field(int field, const void* src, bool on_device, cudaStream_
   if (p.form == CAPAZ_FORM_FP64) {
     if (d != dst) CUDA_TRY(this, cudaMemcpyAsync(dst, d, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   } else if (field == CAPAZ_FIELD_P_W) {
+    if (p.phases == 3) {
+      // P_n, P_g are deviations from the same per-row reference: decode them
+      // with the old reference, re-encode with the new one.
+      for (int q = 5; q < 7; q++)
+        if (!wide[q]) CUDA_TRY(this, cudaMalloc(&wide[q], n * sizeof(double)));
+      CUDA_TRY(this, launch_decode_pressure((const float*)state[cur][3], Pref, p.nx, p.ny, n, wide[5], s));
+      CUDA_TRY(this, launch_decode_pressure((const float*)state[cur][4], Pref, p.nx, p.ny, n, wide[6], s));
+      launches += 2;
+    }
     CUDA_TRY(this, launch_encode_pressure(d, p.nx, p.ny, p.nz, p.P_atm, Pref, PrelF, dPrefF, (float*)dst, s));
-    CUDA_TRY(this, launch_row_tables(Pref, p.ny, make_physf(p), rowF, s));
-    launches += 4;
+    launches += 3;
+    if (p.phases == 3) {
+      CUDA_TRY(this, launch_encode_pressure_rel(wide[5], Pref, p.nx, p.ny, n, (float*)state[cur][3], s));
+      CUDA_TRY(this, launch_encode_pressure_rel(wide[6], Pref, p.nx, p.ny, n, (float*)state[cur][4], s));
+      CUDA_TRY(this, launch_row_tables3(Pref, p.ny, make_step3f_const(p, S_ref_w, S_ref), rowF, s));
+      launches += 3;
+    } else {
+      CUDA_TRY(this, launch_row_tables(Pref, p.ny, make_physf(p), rowF, s));
+      launches++;
+    }
+  } else if (p.phases == 3 && (field == CAPAZ_FIELD_P_N || field == CAPAZ_FIELD_P_G)) {
+    CUDA_TRY(this, launch_encode_pressure_rel(d, Pref, p.nx, p.ny, n, (float*)dst, s));
+    launches++;
+  } else if (p.phases == 3 && field == CAPAZ_FIELD_S_W) {
+    CUDA_TRY(this, launch_encode_saturation(d, n, sum_parts, S_ref_dev, (float*)dst, s));
+    launches += 3;
+    CUDA_TRY(this, cudaMemcpyAsync(&S_ref_w, S_ref_dev, sizeof(double), cudaMemcpyDeviceToHost, s));
   } else if (field == CAPAZ_FIELD_S_N) {
     CUDA_TRY(this, launch_encode_saturation(d, n, sum_parts, S_ref_dev, (float*)dst, s));
     launches += 3;
@@ -748,7 +833,7 @@ int capaz_ctx::set_field(int field, const void* src, bool on_device, cudaStream_
     CUDA_TRY(this, launch_narrow(d, n, (float*)dst, s));
     launches++;
   } else {
-    return fail(this, CAPAZ_ERR_UNSUPPORTED, "the precision form stores P_w, S_n, m and K");
+    return fail(this, CAPAZ_ERR_UNSUPPORTED, "the precision form stores the state, m and K");
   }
   CUDA_TRY(this, cudaStreamSynchronize(s));
   return CAPAZ_OK;
@@ -785,7 +870,8 @@ int capaz_ctx::get_field(int field, void* dst, bool on_device, cudaStream_t s) {
     // Precision form: decode the FP32 deviations of the current state.
     int st = decode_all(cur, s);
     if (st) return st;
-    src = wide[field == CAPAZ_FIELD_P_W ? 0 : 1];
+    src = wide[field == CAPAZ_FIELD_P_W ? 0 : field == CAPAZ_FIELD_S_N ? 1 : field == CAPAZ_FIELD_S_W ? 4
+               : field == CAPAZ_FIELD_P_N ? 5 : 6];
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     CUDA_TRY(this, cudaMemcpyAsync(dst, src, n * sizeof(double), kind, s));
     if (on_device) return CAPAZ_OK;
@@ -882,10 +968,18 @@ int capaz_ctx::get_derived(int field, bool from_current, void* dst, bool on_devi
 }
 
 int capaz_ctx::decode_all(int b, cudaStream_t s) {
-  for (int q = 0; q < 4; q++)
+  const int nw = p.phases == 3 ? 7 : 4;
+  for (int q = 0; q < nw; q++)
     if (!wide[q]) CUDA_TRY(this, cudaMalloc(&wide[q], n * sizeof(double)));
   CUDA_TRY(this, launch_decode2((const float*)state[b][0], (const float*)state[b][1], Pref, S_ref, p.nx, p.ny, n,
                                 wide[0], wide[1], s));
+  if (p.phases == 3) {
+    // S_w, P_n, P_g (P_n, P_g hold the Border_P values on boundary cells).
+    CUDA_TRY(this, launch_decode2((const float*)state[b][3], (const float*)state[b][2], Pref, S_ref_w, p.nx, p.ny, n,
+                                  wide[5], wide[4], s));
+    CUDA_TRY(this, launch_decode_pressure((const float*)state[b][4], Pref, p.nx, p.ny, n, wide[6], s));
+    launches += 2;
+  }
   CUDA_TRY(this, launch_widen((const float*)m, n, wide[2], s));
   launches += 2;
   if (K) {

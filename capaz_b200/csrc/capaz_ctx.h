@@ -34,8 +34,10 @@ struct capaz_ctx {
   double* Pref = nullptr;    // ny
   float* PrelF = nullptr;    // ny: Pref - P_atm
   float* dPrefF = nullptr;   // ny: Pref[j+1] - Pref[j]
-  double S_ref = 0.;
-  double* wide[4] = {nullptr, nullptr, nullptr, nullptr};  // FP64 decode scratch
+  double S_ref = 0.;    // S_n reference
+  double S_ref_w = 0.;  // S_w reference (three-phase)
+  // FP64 decode scratch: P_w, S_n, m, K, then S_w, P_n, P_g (three-phase).
+  double* wide[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   // TMA path of the precision form.
   capaz::InstT* tma_inst = nullptr;  // device descriptor
   int4* tma_items = nullptr;
@@ -95,6 +97,7 @@ Step2Const make_step2_const(const capaz_params& p);
 BLConst make_bl_const(const capaz_params& p);
 Step2FConst make_step2f_const(const capaz_params& p, double S_ref);
 Step3Const make_step3_const(const capaz_params& p);
+Step3FConst make_step3f_const(const capaz_params& p, double S_ref_w, double S_ref_n);
 PhysF make_physf(const capaz_params& p);
 void reference_init_host(const capaz_params& p, const double* m, double* Pw, double* Sw, double* Sn, double* Pn,
                          double* Pg);

@@ -96,6 +96,28 @@ cudaError_t launch_derived3_fp64(const Step3Const& c, int field, const Step3Buff
 cudaError_t launch_compose3(const Step3Const& c, const double* Pw_start, const double* bnd_now, double* out,
                             cudaStream_t s);
 
+// Three-phase precision form (step3_fp32c.cu): FP32 deviations of P_w, P_n,
+// P_g from the per-row reference pressure and of S_w, S_n from their means.
+struct Step3FConst {
+  int nx, ny, nz, source, source_window, win_k0, win_k1;
+  int tiles_x, tiles_y, zchunk, nzchunks, i_lo, i_hi, a2;
+  long long sy, sz;
+  float S_ref_w_f, S_ref_n_f, S_wr_f, S_nr_f, inv_den, K0_f, aw_f, an_f, bg_f;
+  float inv_mu_w_f, inv_mu_n_f, inv_mu_g_f, inv_hx2_f, inv_hy2_f, inv_hz2_f, g_inv_hy_f, dt_f, e1, e2, e3;
+  double S_ref_w, S_ref_n, P_atm, aw, an, bg, ro0_w, ro0_n, ro0_g, beta_w, beta_n, g, hy, S_w_gr, S_n_gr, vol;
+};
+struct Step3FArgs {
+  const float *p_w, *s_w, *s_n, *p_n, *p_g;
+  float *o_pw, *o_sw, *o_sn, *o_pn, *o_pg;
+  const float *m, *K;   // K == nullptr: uniform K0
+  const float4* rowF;   // ny: rho_w, rho_n, rho_g at P_ref(j), P_ref(j+1) - P_ref(j)
+  const double* Pref;   // ny
+  double* diag;         // per-block partials or nullptr
+  unsigned int* err;
+};
+cudaError_t launch_step3_fp32c(const Step3FConst& c, const Step3FArgs& a, cudaStream_t s);
+cudaError_t launch_row_tables3(const double* Pref, int ny, const Step3FConst& c, float4* rowF, cudaStream_t s);
+
 // Batched (ensemble) steps: one persistent launch over (instance, tile,
 // z-chunk) work items.  State pointers per ping-pong parity.
 struct Inst64 {
@@ -173,6 +195,10 @@ cudaError_t launch_encode_pressure(const double* P, int nx, int ny, int nz, doub
 cudaError_t launch_encode_saturation(const double* S, long long n, double* part, double* S_ref, float* out,
                                      cudaStream_t s);
 cudaError_t launch_narrow(const double* a, long long n, float* out, cudaStream_t s);
+cudaError_t launch_encode_pressure_rel(const double* P, const double* Pref, int nx, int ny, long long n, float* out,
+                                       cudaStream_t s);
+cudaError_t launch_decode_pressure(const float* p, const double* Pref, int nx, int ny, long long n, double* out,
+                                   cudaStream_t s);
 
 // Per-block partial diagnostics: mass[3], max residual, non-finite count.
 constexpr int DIAG_STRIDE = 5;

@@ -157,6 +157,45 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
     }
     return CAPAZ_OK;
   }
+  if (p.phases == 3 && p.form == CAPAZ_FORM_FP32C) {
+    const Step3FConst c = make_step3f_const(p, S_ref_w, S_ref);
+    if (diag && !diag_partials) {
+      diag_blocks = c.tiles_x * c.tiles_y * c.nzchunks;
+      e = cudaMalloc(&diag_partials, sizeof(double) * DIAG_STRIDE * diag_blocks);
+      if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(diag)");
+    }
+    for (int t = 0; t < nsteps; t++) {
+      const int nxt = cur ^ 1;
+      Step3FArgs a;
+      a.p_w = (const float*)state[cur][0];
+      a.s_n = (const float*)state[cur][1];
+      a.s_w = (const float*)state[cur][2];
+      a.p_n = (const float*)state[cur][3];
+      a.p_g = (const float*)state[cur][4];
+      a.o_pw = (float*)state[nxt][0];
+      a.o_sn = (float*)state[nxt][1];
+      a.o_sw = (float*)state[nxt][2];
+      a.o_pn = (float*)state[nxt][3];
+      a.o_pg = (float*)state[nxt][4];
+      a.m = (const float*)m;
+      a.K = (p.flags & CAPAZ_FLAG_PERCELL_K) ? (const float*)K : nullptr;
+      a.rowF = rowF;
+      a.Pref = Pref;
+      a.diag = (diag && t == nsteps - 1) ? diag_partials : nullptr;
+      a.err = err_flag;
+      e = launch_step3_fp32c(c, a, s);
+      launches++;
+      if (e != cudaSuccess) return fail_cuda(e, "step3_fp32c launch");
+      cur = nxt;
+      steps_done++;
+    }
+    if (diag) {
+      e = launch_diag_finalize(diag_partials, diag_blocks, diag_out, s);
+      launches++;
+      if (e != cudaSuccess) return fail_cuda(e, "diag finalize launch");
+    }
+    return CAPAZ_OK;
+  }
   return fail_msg(CAPAZ_ERR_UNSUPPORTED, "this phase/form combination is not built yet");
 }
 
@@ -259,6 +298,35 @@ int capaz_ctx::derived(int field, cudaStream_t s, bool from_current) {
     if (field == CAPAZ_FIELD_S_W || field == CAPAZ_FIELD_P_W || field == CAPAZ_FIELD_S_N)
       return fail_msg(CAPAZ_ERR_INVALID_ARGUMENT, "state field");
     cudaError_t e = launch_derived3_fp64(c, field, stb, (const double*)m, Kp, scratch, s);
+    launches++;
+    if (e != cudaSuccess) return fail_cuda(e, "derived launch");
+    return CAPAZ_OK;
+  }
+  if (p.phases == 3 && p.form == CAPAZ_FORM_FP32C) {
+    // Decode to FP64 and evaluate the FP64 three-phase derived kernels.
+    const Step3Const c = make_step3_const(p);
+    if (field == CAPAZ_FIELD_P_N || field == CAPAZ_FIELD_P_G) {
+      // Start-of-step P_w on interior cells, current Border_P values elsewhere.
+      if (!stage) {
+        cudaError_t e = cudaMalloc(&stage, n * sizeof(double));
+        if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(stage)");
+      }
+      cudaError_t e = launch_decode_pressure((const float*)state[src][0], Pref, p.nx, p.ny, n, stage, s);
+      if (e != cudaSuccess) return fail_cuda(e, "decode launch");
+      st = decode_all(cur, s);
+      if (st) return st;
+      e = launch_compose3(c, stage, wide[field == CAPAZ_FIELD_P_N ? 5 : 6], scratch, s);
+      launches += 2;
+      if (e != cudaSuccess) return fail_cuda(e, "compose launch");
+      return CAPAZ_OK;
+    }
+    if (field == CAPAZ_FIELD_S_W || field == CAPAZ_FIELD_P_W || field == CAPAZ_FIELD_S_N)
+      return fail_msg(CAPAZ_ERR_INVALID_ARGUMENT, "state field");
+    st = decode_all(src, s);
+    if (st) return st;
+    const double* Kp = (p.flags & CAPAZ_FLAG_PERCELL_K) ? wide[3] : nullptr;
+    Step3Buffers stb{wide[0], wide[4], wide[1], wide[5], wide[6]};
+    cudaError_t e = launch_derived3_fp64(c, field, stb, wide[2], Kp, scratch, s);
     launches++;
     if (e != cudaSuccess) return fail_cuda(e, "derived launch");
     return CAPAZ_OK;

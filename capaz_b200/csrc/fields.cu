@@ -123,6 +123,27 @@ cudaError_t launch_encode_saturation(const double* S, long long n, double* part 
   return cudaGetLastError();
 }
 
+// Pressure deviations from an existing per-row reference (P_n, P_g of the
+// three-phase precision form) and back.
+__global__ void decode_p_kernel(const float* __restrict__ p, const double* __restrict__ Pref, int nx, int ny,
+                                long long n, double* __restrict__ P) {
+  const long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (l >= n) return;
+  P[l] = Pref[(int)((l / nx) % ny)] + (double)p[l];
+}
+
+cudaError_t launch_encode_pressure_rel(const double* P, const double* Pref, int nx, int ny, long long n, float* out,
+                                       cudaStream_t s) {
+  encode_p_kernel<<<grid_for(n, 256), 256, 0, s>>>(P, Pref, nx, ny, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_decode_pressure(const float* p, const double* Pref, int nx, int ny, long long n, double* out,
+                                   cudaStream_t s) {
+  decode_p_kernel<<<grid_for(n, 256), 256, 0, s>>>(p, Pref, nx, ny, n, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_row_tables(const double* Pref, int ny, const PhysF& f, float4* rowF, cudaStream_t s) {
   row_tables_kernel<<<(ny + 127) / 128, 128, 0, s>>>(Pref, ny, f, rowF);
   return cudaGetLastError();

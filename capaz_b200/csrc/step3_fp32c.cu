@@ -1,0 +1,355 @@
+// Three-phase precision form: FP32 storage and stencil, FP64 Newton.
+//
+// The state is stored as FP32 deviations from a reference state: pressures
+// P_w, P_n, P_g from the per-row reference pressure P_ref(j) (the row means
+// of P_w when it was set), saturations S_w, S_n from their grid means.  One
+// launch per step, tiled as the FP64 three-phase step (32 x 8 columns per
+// CTA marching along z with a 3-plane ring in shared memory):
+//   - every cell of the plane window is derived in FP32: effective
+//     saturations, the reference CPU relative permeabilities
+//     (three-phase.cpp:146-186; square roots when A = 2), densities from the
+//     per-row reference densities plus the linear pressure term, and the
+//     mobility-densities M_p = K k_p rho_p / mu_p (= -Xi_p rho_p);
+//   - the upwind flux difference of each phase (cpu.cpp:236-264 in select
+//     form) is formed per axis as out - in, the three axis terms Kahan-summed
+//     in FP32; d(rho S)_p = -dt/m div F_p goes to FP64;
+//   - two Newton iterations in FP64 solve the exact bilinear increment
+//     equations rho_p(P + dP)(S_p + dS_p) - rho_p(P) S_p = d(rho S)_p for
+//     (dP, dS_w, dS_n) (S_g = 1 - S_w - S_n), with the 3x3 Jacobian solved
+//     by Cramer's rule; the new deviations are rounded to FP32 once;
+//   - boundary cells (Border_S, Border_P of three-phase.cpp:345-427) are
+//     written by the thread of their basic-coordinate cell in FP64 from its
+//     new state, as in the FP64 step.
+// Diagnostics (mass per phase, the reference Newton functions' residual at
+// the result, non-finite cells) are evaluated in FP64.
+#include <math.h>
+
+#include "capaz_internal.h"
+
+namespace capaz {
+namespace {
+
+// Derived values of one window cell: pressure deviations of the three
+// phases and their mobility-densities.
+struct Plane3F {
+  float p[3][PC];
+  float M[3][PC];
+};
+constexpr size_t kSmem3F = 3 * sizeof(Plane3F);
+
+// Relative permeabilities (three-phase.cpp:146-186) in FP32.  A2: A = 2, so
+// the exponents A/(A-1), (A-1)/A and 2(A-1)/A are 2, 1/2 and 1.
+template <bool A2>
+__device__ __forceinline__ void relperm3f(const Step3FConst& f, float S_w_e, float S_n_e, float& k_w, float& k_n,
+                                          float& k_g) {
+  const float S_g_e = 1.f - S_w_e - S_n_e;
+  auto p1 = [&](float x) { return A2 ? x * x : powf(x, f.e1); };        // x^(A/(A-1))
+  auto p2 = [&](float x) { return A2 ? sqrtf(x) : powf(x, f.e2); };     // x^((A-1)/A)
+  auto p3 = [&](float x) { return A2 ? x : powf(x, f.e3); };            // x^(2(A-1)/A)
+  k_w = 0.f;
+  if (S_w_e >= 1e-3f) {
+    const float t = 1.f - p2(1.f - p1(S_w_e));
+    k_w = sqrtf(S_w_e) * t * t;
+  }
+  k_g = 0.f;
+  if (S_g_e >= 1e-3f) k_g = sqrtf(S_g_e) * p3(1.f - p1(1.f - S_g_e));
+  k_n = 0.f;
+  if (S_n_e >= 1e-3f) {
+    const float k_n_w = sqrtf(1.f - S_w_e) * p3(1.f - p1(S_w_e));
+    const float t = 1.f - p2(1.f - p1(S_n_e));
+    const float k_n_g = sqrtf(S_n_e) * t * t;
+    k_n = S_n_e * k_n_w * k_n_g / (1.f - S_w_e) / (1.f - S_g_e);
+  }
+}
+
+__device__ __forceinline__ bool interior3f(const Step3FConst& c, int i, int j, int k) {
+  return (((i != 0) && (i != c.nx - 1)) || (c.nx < 2)) && (j != 0) && (j != c.ny - 1) &&
+         (((k != 0) && (k != c.nz - 1)) || (c.nz < 2));
+}
+__device__ __forceinline__ bool in_window3f(const Step3FConst& c, int i, int k) {
+  return (i >= c.nx / 2 - c.source) && (i <= c.nx / 2 + c.source) && (k >= c.win_k0) && (k <= c.win_k1);
+}
+
+__device__ __forceinline__ float face(float x1, float x2, float Mc, float Mm, float Mp) {
+  return x2 * (x2 > 0.f ? Mc : Mp) - x1 * (x1 > 0.f ? Mm : Mc);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+template <bool UNIK, bool PLANAR, bool DIAG, bool A2>
+__global__ void __launch_bounds__(NTHREADS, 2)
+    step3_fp32c_kernel(const Step3FConst c, const Step3FArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Plane3F* ring = reinterpret_cast<Plane3F*>(smem_raw);
+  const int tid = threadIdx.x + TX * threadIdx.y;
+  const int tile = blockIdx.x;
+  const int ti = tile % c.tiles_x, tj = tile / c.tiles_x;
+  const int i0 = c.i_lo + ti * TX, j0 = 1 + tj * TY;
+  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  const bool active = (i <= c.i_hi) && (j <= c.ny - 2);
+  const int cidx = (threadIdx.y + 1) * PX + (threadIdx.x + 1);
+  int kb, ke;
+  if (PLANAR) {
+    kb = 0;
+    ke = 1;
+  } else {
+    kb = 1 + blockIdx.y * c.zchunk;
+    ke = min(kb + c.zchunk, c.nz - 1);
+  }
+  const float den_inv = c.inv_den;
+
+  // Derive plane k of the window into its ring slot.
+  auto fill = [&](int k) {
+    Plane3F& P = ring[k % 3];
+    for (int q = tid; q < PC; q += NTHREADS) {
+      const int gi = i0 - 1 + q % PX, gj = j0 - 1 + q / PX;
+      if (gi >= 0 && gi < c.nx && gj < c.ny) {
+        const long long l = gi + gj * c.sy + (long long)k * c.sz;
+        const float pw = a.p_w[l];
+        float pn = pw, pg = pw;  // interior: P_n = P_g = P_w (capillary pressures zero)
+        if (!interior3f(c, gi, gj, k)) {
+          pn = a.p_n[l];
+          pg = a.p_g[l];
+        }
+        const float Sw = c.S_ref_w_f + a.s_w[l], Sn = c.S_ref_n_f + a.s_n[l];
+        const float S_w_e = (Sw - c.S_wr_f) * den_inv, S_n_e = (Sn - c.S_nr_f) * den_inv;
+        float k_w, k_n, k_g;
+        relperm3f<A2>(c, S_w_e, S_n_e, k_w, k_n, k_g);
+        const float Kl = UNIK ? c.K0_f : a.K[l];
+        const float4 r = a.rowF[gj];  // rho_p(P_ref(j)) for w, n, g
+        P.p[0][q] = pw;
+        P.p[1][q] = pn;
+        P.p[2][q] = pg;
+        P.M[0][q] = Kl * k_w * fmaf(c.aw_f, pw, r.x) * c.inv_mu_w_f;
+        P.M[1][q] = Kl * k_n * fmaf(c.an_f, pn, r.y) * c.inv_mu_n_f;
+        P.M[2][q] = Kl * k_g * fmaf(c.bg_f, pg, r.z) * c.inv_mu_g_f;
+      }
+    }
+  };
+
+  double acc[3] = {0., 0., 0.}, rmax = 0., nonfinite = 0.;
+  if (!PLANAR) fill(kb - 1);
+  fill(kb);
+  for (int k = kb; k < ke; k++) {
+    if (!PLANAR) fill(k + 1);
+    __syncthreads();
+    if (active) {
+      const Plane3F& C = ring[k % 3];
+      const long long l = i + j * c.sy + (long long)k * c.sz;
+      const float mc = a.m[l];
+      const float sw0 = a.s_w[l], sn0 = a.s_n[l];
+      const float4 row = a.rowF[j];
+      const float dn = a.rowF[j - 1].w, dp = row.w;  // P_ref(j) - P_ref(j-1), P_ref(j+1) - P_ref(j)
+      const float rho_row[3] = {row.x, row.y, row.z};
+      const float slope[3] = {c.aw_f, c.an_f, c.bg_f};
+      float div[3];
+#pragma unroll
+      for (int ph = 0; ph < 3; ph++) {
+        const float pc = C.p[ph][cidx], Mc = C.M[ph][cidx];
+        // x
+        float fx = 0.f;
+        if (c.nx >= 2) {
+          const float pa = C.p[ph][cidx - 1], pb = C.p[ph][cidx + 1];
+          fx = face((pa - pc) * c.inv_hx2_f, (pc - pb) * c.inv_hx2_f, Mc, C.M[ph][cidx - 1], C.M[ph][cidx + 1]);
+        }
+        // y (vertical, gravity g rho of the centre cell)
+        const float gr = c.g_inv_hy_f * fmaf(slope[ph], pc, rho_row[ph]);
+        const float y1 = fmaf(C.p[ph][cidx - PX] - pc, c.inv_hy2_f, -dn * c.inv_hy2_f) + gr;
+        const float y2 = fmaf(pc - C.p[ph][cidx + PX], c.inv_hy2_f, -dp * c.inv_hy2_f) + gr;
+        const float fy = face(y1, y2, Mc, C.M[ph][cidx - PX], C.M[ph][cidx + PX]);
+        // Kahan sum of the axis terms
+        float s = fx + fy;
+        float comp = (s - fx) - fy;
+        if (!PLANAR) {
+          const Plane3F& Mz = ring[(k + 2) % 3];
+          const Plane3F& Qz = ring[(k + 1) % 3];
+          const float fz = face((Mz.p[ph][cidx] - pc) * c.inv_hz2_f, (pc - Qz.p[ph][cidx]) * c.inv_hz2_f, Mc,
+                                Mz.M[ph][cidx], Qz.M[ph][cidx]);
+          const float y = fz - comp;
+          const float t = s + y;
+          comp = (t - s) - y;
+          s = t;
+        }
+        div[ph] = s - comp;
+      }
+      // Conserved increments d(rho S)_p = -dt/m div F_p, then Newton in FP64.
+      const float dtm = c.dt_f / mc;
+      const double dAw = (double)(-dtm * div[0]), dAn = (double)(-dtm * div[1]), dAg = (double)(-dtm * div[2]);
+      const double prel = a.Pref[j] - c.P_atm;
+      const double pw0 = (double)C.p[0][cidx];
+      const double P = a.Pref[j] + pw0;
+      const double Sw = c.S_ref_w + (double)sw0, Sn = c.S_ref_n + (double)sn0, Sg = 1. - Sw - Sn;
+      const double rw = fma(c.aw, prel + pw0, c.ro0_w), rn = fma(c.an, prel + pw0, c.ro0_n);
+      double dP = 0., dSw = 0., dSn = 0.;
+      for (int it = 0; it < 2; it++) {
+        const double dSg = -dSw - dSn;
+        const double R1 = c.aw * dP * (Sw + dSw) + rw * dSw - dAw;
+        const double R2 = c.an * dP * (Sn + dSn) + rn * dSn - dAn;
+        const double R3 = c.bg * (dP * (Sg + dSg) + P * dSg) - dAg;
+        // Jacobian in (dP, dSw, dSn)
+        const double a11 = c.aw * (Sw + dSw), a12 = c.aw * dP + rw, a13 = 0.;
+        const double a21 = c.an * (Sn + dSn), a22 = 0., a23 = c.an * dP + rn;
+        const double a31 = c.bg * (Sg + dSg), a32 = -c.bg * (P + dP), a33 = a32;
+        const double c11 = a22 * a33 - a23 * a32, c12 = a23 * a31 - a21 * a33, c13 = a21 * a32 - a22 * a31;
+        const double det = a11 * c11 + a12 * c12 + a13 * c13;
+        const double inv = 1. / det;
+        const double x1 = (R1 * c11 + a12 * (a23 * R3 - R2 * a33) + a13 * (R2 * a32 - a22 * R3)) * inv;
+        const double x2 = (a11 * (R2 * a33 - a23 * R3) + R1 * c12 + a13 * (a21 * R3 - R2 * a31)) * inv;
+        const double x3 = (a11 * (a22 * R3 - R2 * a32) + a12 * (R2 * a31 - a21 * R3) + R1 * c13) * inv;
+        dP -= x1;
+        dSw -= x2;
+        dSn -= x3;
+      }
+      const double Pn1 = P + dP, Swn = Sw + dSw, Snn = Sn + dSn;
+      a.o_pw[l] = (float)(pw0 + dP);
+      a.o_sw[l] = (float)((double)sw0 + dSw);
+      a.o_sn[l] = (float)((double)sn0 + dSn);
+      const bool finite = isfinite(Pn1) && isfinite(Swn) && isfinite(Snn);
+      if (!finite) atomicOr(a.err, 1u);
+
+      // Border_S / Border_P for the boundary cells mapped onto (i, j, k).
+      const bool xb = c.nx >= 3;
+      const bool edge = (xb && (i == 1 || i == c.nx - 2)) || (j == 1) || (j == c.ny - 2) ||
+                        (!PLANAR && ((k == 1) || (k == c.nz - 2)));
+      if (edge) {
+        int xs[3], ys[3], zs[3], nxs = 0, nys = 0, nzs = 0;
+        xs[nxs++] = i;
+        if (xb && i == 1) xs[nxs++] = 0;
+        if (xb && i == c.nx - 2) xs[nxs++] = c.nx - 1;
+        ys[nys++] = j;
+        if (j == 1) ys[nys++] = 0;
+        if (j == c.ny - 2) ys[nys++] = c.ny - 1;
+        zs[nzs++] = k;
+        if (!PLANAR) {
+          if (k == 1) zs[nzs++] = 0;
+          if (k == c.nz - 2) zs[nzs++] = c.nz - 1;
+        }
+        for (int qa = 0; qa < nxs; qa++)
+          for (int qb = 0; qb < nys; qb++)
+            for (int qd = 0; qd < nzs; qd++) {
+              if (qa == 0 && qb == 0 && qd == 0) continue;
+              const int bj = ys[qb], bi = xs[qa], bk = zs[qd];
+              const long long lb = bi + bj * c.sy + (long long)bk * c.sz;
+              double sw = Swn, sn = Snn;
+              if ((bj == 0) && (c.source > 0) && (!c.source_window || in_window3f(c, bi, bk))) {
+                sw = c.S_w_gr;
+                sn = c.S_n_gr;
+              }
+              double pw, pn, pg;
+              if ((bj != 0) && (bj != c.ny - 1)) {
+                pw = pn = pg = Pn1;
+              } else if (bj == 0) {
+                pw = (Pn1 - (c.ro0_w) * (c.g) * (c.hy) * (1. - (c.beta_w) * (c.P_atm))) /
+                     (1. + (c.beta_w) * (c.ro0_w) * (c.g) * (c.hy));
+                pn = (Pn1 - (c.ro0_n) * (c.g) * (c.hy) * (1. - (c.beta_n) * (c.P_atm))) /
+                     (1. + (c.beta_n) * (c.ro0_n) * (c.g) * (c.hy));
+                pg = Pn1 / (1. + (c.ro0_g) * (c.g) * (c.hy) / (c.P_atm));
+              } else {
+                pw = (Pn1 + (c.ro0_w) * (c.g) * (c.hy) * (1. - (c.beta_w) * (c.P_atm))) /
+                     (1. - (c.beta_w) * (c.ro0_w) * (c.g) * (c.hy));
+                pn = (Pn1 + (c.ro0_n) * (c.g) * (c.hy) * (1. - (c.beta_n) * (c.P_atm))) /
+                     (1. - (c.beta_n) * (c.ro0_n) * (c.g) * (c.hy));
+                pg = Pn1 / (1. - (c.ro0_g) * (c.g) * (c.hy) / (c.P_atm));
+              }
+              const double pr = a.Pref[bj];
+              a.o_sw[lb] = (float)(sw - c.S_ref_w);
+              a.o_sn[lb] = (float)(sn - c.S_ref_n);
+              a.o_pw[lb] = (float)(pw - pr);
+              a.o_pn[lb] = (float)(pn - pr);
+              a.o_pg[lb] = (float)(pg - pr);
+            }
+      }
+      if (DIAG) {
+        const double Sgn = 1. - Swn - Snn;
+        const double rw1 = c.ro0_w * (1. + (c.beta_w) * (Pn1 - c.P_atm));
+        const double rn1 = c.ro0_n * (1. + (c.beta_n) * (Pn1 - c.P_atm));
+        const double rg1 = c.ro0_g * Pn1 / c.P_atm;
+        const double vm = (double)mc * c.vol;
+        acc[0] += vm * rw1 * Swn;
+        acc[1] += vm * rn1 * Snn;
+        acc[2] += vm * rg1 * Sgn;
+        // the reference's Newton functions F_p = rho_p S_p - roS_p at the result
+        const double G1 = rw1 * Swn - (rw * Sw + dAw);
+        const double G2 = rn1 * Snn - (rn * Sn + dAn);
+        const double G3 = rg1 * Sgn - (c.ro0_g * P / c.P_atm * Sg + dAg);
+        const double r = fmax(fmax(fabs(G1) / c.ro0_w, fabs(G2) / c.ro0_n), fabs(G3) / c.ro0_g);
+        if (!(r <= rmax)) rmax = r;
+        if (!finite) nonfinite += 1.;
+      }
+    }
+    __syncthreads();
+  }
+
+  if (DIAG) {
+    __shared__ double red[NTHREADS / 32][5];
+    const int lane = tid & 31, wid = tid >> 5;
+    double v[5] = {warp_sum(acc[0]), warp_sum(acc[1]), warp_sum(acc[2]), warp_max(rmax), warp_sum(nonfinite)};
+    if (lane == 0)
+      for (int q = 0; q < 5; q++) red[wid][q] = v[q];
+    __syncthreads();
+    if (tid == 0) {
+      double t[5] = {0, 0, 0, 0, 0};
+      for (int w = 0; w < NTHREADS / 32; w++) {
+        t[0] += red[w][0];
+        t[1] += red[w][1];
+        t[2] += red[w][2];
+        t[3] = fmax(t[3], red[w][3]);
+        t[4] += red[w][4];
+      }
+      double* o = a.diag + (size_t)DIAG_STRIDE * (blockIdx.x + (size_t)gridDim.x * blockIdx.y);
+      for (int q = 0; q < 5; q++) o[q] = t[q];
+    }
+  }
+}
+
+template <bool UNIK, bool PLANAR, bool DIAG, bool A2>
+cudaError_t launch_t(const Step3FConst& c, const Step3FArgs& a, cudaStream_t s) {
+  auto kern = step3_fp32c_kernel<UNIK, PLANAR, DIAG, A2>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem3F);
+  if (e != cudaSuccess) return e;
+  dim3 grid(c.tiles_x * c.tiles_y, c.nzchunks);
+  kern<<<grid, dim3(TX, TY), kSmem3F, s>>>(c, a);
+  return cudaGetLastError();
+}
+
+template <bool UNIK, bool PLANAR, bool DIAG>
+cudaError_t launch_a(const Step3FConst& c, const Step3FArgs& a, cudaStream_t s) {
+  return c.a2 ? launch_t<UNIK, PLANAR, DIAG, true>(c, a, s) : launch_t<UNIK, PLANAR, DIAG, false>(c, a, s);
+}
+
+template <bool UNIK, bool PLANAR>
+cudaError_t launch_d(const Step3FConst& c, const Step3FArgs& a, cudaStream_t s) {
+  return a.diag ? launch_a<UNIK, PLANAR, true>(c, a, s) : launch_a<UNIK, PLANAR, false>(c, a, s);
+}
+
+__global__ void row_tables3_kernel(const double* __restrict__ Pref, int ny, double P_atm, double ro0_w, double ro0_n,
+                                   double ro0_g, double aw, double an, float4* __restrict__ rowF) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ny) return;
+  const double prel = Pref[j] - P_atm;
+  const double dnext = (j + 1 < ny) ? (Pref[j + 1] - Pref[j]) : 0.;
+  rowF[j] = make_float4((float)(ro0_w + aw * prel), (float)(ro0_n + an * prel), (float)(ro0_g * Pref[j] / P_atm),
+                        (float)dnext);
+}
+
+}  // namespace
+
+cudaError_t launch_step3_fp32c(const Step3FConst& c, const Step3FArgs& a, cudaStream_t s) {
+  const bool unik = a.K == nullptr, planar = c.nz == 1;
+  if (unik) return planar ? launch_d<true, true>(c, a, s) : launch_d<true, false>(c, a, s);
+  return planar ? launch_d<false, true>(c, a, s) : launch_d<false, false>(c, a, s);
+}
+
+cudaError_t launch_row_tables3(const double* Pref, int ny, const Step3FConst& c, float4* rowF, cudaStream_t s) {
+  row_tables3_kernel<<<(ny + 127) / 128, 128, 0, s>>>(Pref, ny, c.P_atm, c.ro0_w, c.ro0_n, c.ro0_g, c.aw, c.an, rowF);
+  return cudaGetLastError();
+}
+
+}  // namespace capaz
