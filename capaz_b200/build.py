@@ -87,16 +87,18 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         _run([NVCC] + ARCH + ["-shared", "-o", lib] + objs + ["-cudart", "static"], verbose)
 
     out = {"libcapaz_b200": lib}
-    dsrc = os.path.join(CSRC, "dropin_2ph.cpp")
+    dsrc = os.path.join(CSRC, "dropin.cpp")
     if os.path.exists(dsrc):
-        dlib = os.path.join(LIB, "libcapaz_dropin_2ph.so")
         dh = [os.path.join(INCLUDE, "capaz_refabi.h"), os.path.join(INCLUDE, "capaz_b200.h")]
-        if force or _newer(dlib, [dsrc, lib] + dh):
-            cuda = os.path.dirname(os.path.dirname(NVCC))
-            _run([CXX, "-O2", "-fPIC", "-shared", "-std=c++17", "-I" + INCLUDE, "-I" + os.path.join(cuda, "include"),
-                  dsrc, "-o", dlib, "-L" + LIB, "-lcapaz_b200", "-L" + os.path.join(cuda, "lib64"),
-                  "-lcudart_static", "-ldl", "-lrt", "-lpthread", "-Wl,-rpath,$ORIGIN"], verbose)
-        out["libcapaz_dropin_2ph"] = dlib
+        cuda = os.path.dirname(os.path.dirname(NVCC))
+        for tag, defs in (("2ph", []), ("3ph", ["-DCAPAZ_REFABI_THREE_PHASE"])):
+            dlib = os.path.join(LIB, f"libcapaz_dropin_{tag}.so")
+            if force or _newer(dlib, [dsrc, lib] + dh):
+                _run([CXX, "-O2", "-fPIC", "-shared", "-std=c++17"] + defs +
+                     ["-I" + INCLUDE, "-I" + os.path.join(cuda, "include"), dsrc, "-o", dlib, "-L" + LIB,
+                      "-lcapaz_b200", "-L" + os.path.join(cuda, "lib64"), "-lcudart_static", "-ldl", "-lrt",
+                      "-lpthread", "-Wl,-rpath,$ORIGIN"], verbose)
+            out[f"libcapaz_dropin_{tag}"] = dlib
     return out
 
 

@@ -1,6 +1,8 @@
-// Link-level drop-in for the reference's two-phase GPU backend: the
-// reference's stage/memory/device call surface (include/capaz_refabi.h) on
-// top of the C ABI (include/capaz_b200.h).  Built as libcapaz_dropin_2ph.so.
+// Link-level drop-in for the reference's GPU backend: the reference's
+// stage/memory/device call surface (include/capaz_refabi.h) on top of the C
+// ABI (include/capaz_b200.h).  Built twice: libcapaz_dropin_2ph.so, and
+// libcapaz_dropin_3ph.so with CAPAZ_REFABI_THREE_PHASE defined (the
+// reference's THREE_PHASE struct layouts and the three-phase step).
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -11,8 +13,17 @@
 #include "capaz_b200.h"
 #include "capaz_refabi.h"
 
+#ifdef CAPAZ_REFABI_THREE_PHASE
+static_assert(sizeof(ptr_Arrays) == 232, "ptr_Arrays layout must match the reference (three-phase)");
+static_assert(sizeof(consts) == 488, "consts layout must match the reference (three-phase)");
+constexpr int kPhases = 3;
+#define CAPAZ_DROPIN_LIB "libcapaz_dropin_3ph"
+#else
 static_assert(sizeof(ptr_Arrays) == 160, "ptr_Arrays layout must match the reference (two-phase)");
 static_assert(sizeof(consts) == 384, "consts layout must match the reference (two-phase)");
+constexpr int kPhases = 2;
+#define CAPAZ_DROPIN_LIB "libcapaz_dropin_2ph"
+#endif
 
 namespace {
 
@@ -66,7 +77,7 @@ capaz_params params_from(const consts& def) {
   p.nx = def.locNx;
   p.ny = def.locNy;
   p.nz = def.locNz;
-  p.phases = 2;
+  p.phases = kPhases;
   p.form = CAPAZ_FORM_FP64;
   p.newton_iterations = def.newton_iterations;
   p.source = def.source;
@@ -85,7 +96,20 @@ capaz_params params_from(const consts& def) {
   p.P_atm = def.P_atm;
   p.lambda = def.lambda[0];
   p.S_wr = def.S_wr[0];
+#ifdef CAPAZ_REFABI_THREE_PHASE
+  // The CPU three-phase model has no capillary pressure (P_D_NW, P_D_GN unused).
+  p.P_d = 0.;
+  p.S_nr = def.S_nr[0];
+  p.S_gr = def.S_gr[0];
+  p.S_w_init = def.S_w_init;
+  p.S_n_init = def.S_n_init;
+  p.beta_g = def.beta_g;
+  p.mu_g = def.mu_g;
+  p.ro0_g = def.ro0_g;
+  p.S_w_gr = def.S_w_gr;
+#else
   p.P_d = def.P_d[0];
+#endif
   p.S_n_gr = def.S_n_gr;
   p.porosity = def.porosity[0];
   p.K0 = def.K[0];
@@ -97,7 +121,13 @@ capaz_params params_from(const consts& def) {
 
 void require_one_rank(const consts& def, int line) {
   if (def.size > 1 || def.sizex > 1 || def.sizey > 1 || def.sizez > 1)
-    die("libcapaz_dropin_2ph runs one rank (link no_communication.cpp)", line);
+    die(CAPAZ_DROPIN_LIB " runs one rank (link no_communication.cpp)", line);
+}
+
+// Fields the context holds as state or media (set on upload).
+bool is_state_or_media(int f) {
+  if (f == CAPAZ_FIELD_P_W || f == CAPAZ_FIELD_S_N || f == CAPAZ_FIELD_M) return true;
+  return kPhases == 3 && (f == CAPAZ_FIELD_S_W || f == CAPAZ_FIELD_P_N || f == CAPAZ_FIELD_P_G);
 }
 
 int field_of(const double* dev) {
@@ -172,9 +202,14 @@ void device_memory_allocation(ptr_Arrays* A, double** DevBuffer, consts def) {
       {&A->Xi_w, CAPAZ_FIELD_XI_W},     {&A->Xi_n, CAPAZ_FIELD_XI_N},     {&A->roS_w, CAPAZ_FIELD_ROS_W},
       {&A->roS_n, CAPAZ_FIELD_ROS_N},   {&A->roS_w_old, CAPAZ_FIELD_ROS_W_OLD},
       {&A->roS_n_old, CAPAZ_FIELD_ROS_N_OLD}, {&A->m, CAPAZ_FIELD_M},
-      // K: the two-phase physics reads K_0 (two-phase.cpp:16-17), so the K
-      // array is kept but does not reach the step, as in the reference.
+      // K: the physics reads K_0 (two-phase.cpp:16-17, three-phase.cpp:220-222),
+      // so the K array is kept but does not reach the step, as in the reference.
       {&A->K, -1},
+#ifdef CAPAZ_REFABI_THREE_PHASE
+      {&A->S_g, CAPAZ_FIELD_S_G},       {&A->P_g, CAPAZ_FIELD_P_G},       {&A->ro_g, CAPAZ_FIELD_RO_G},
+      {&A->ux_g, CAPAZ_FIELD_UX_G},     {&A->uy_g, CAPAZ_FIELD_UY_G},     {&A->uz_g, CAPAZ_FIELD_UZ_G},
+      {&A->Xi_g, CAPAZ_FIELD_XI_G},     {&A->roS_g, CAPAZ_FIELD_ROS_G},   {&A->roS_g_old, CAPAZ_FIELD_ROS_G_OLD},
+#endif
   };
   g.handles.clear();
   for (auto& s : slots) {
@@ -202,7 +237,7 @@ void load_data_to_device(double* HostArrayPtr, double* DevArrayPtr, consts def) 
   check_cuda(cudaMemcpy(DevArrayPtr, HostArrayPtr, bytes, cudaMemcpyHostToDevice), "copy double data to device",
              __LINE__);
   const int f = field_of(DevArrayPtr);
-  if (f == CAPAZ_FIELD_P_W || f == CAPAZ_FIELD_S_N || f == CAPAZ_FIELD_M)
+  if (is_state_or_media(f))
     check(capaz_set_field_device(g.ctx, f, DevArrayPtr, nullptr), "capaz_set_field_device", __LINE__);
 }
 
@@ -216,7 +251,7 @@ void load_data_to_host(double* HostArrayPtr, double* DevArrayPtr, consts def) {
   (void)def;
   const size_t bytes = (size_t)g.n * sizeof(double);
   const int f = field_of(DevArrayPtr);
-  const bool state_or_media = (f == CAPAZ_FIELD_P_W || f == CAPAZ_FIELD_S_N || f == CAPAZ_FIELD_M);
+  const bool state_or_media = is_state_or_media(f);
   // Before the first stage call the reference's derived arrays hold what
   // the allocation left there (the handles are zeroed) or what the host
   // uploaded; they are computed only once a step has begun.
@@ -234,15 +269,27 @@ void data_initialization(ptr_Arrays H, long int* time_counter, consts def) {
   require_one_rank(def, __LINE__);
   *time_counter = 0;
   capaz_params p = params_from(def);
+  const long long n = (long long)def.locNx * def.locNy * def.locNz;
+#ifdef CAPAZ_REFABI_THREE_PHASE
+  check(capaz_reference_init(&p, H.m, 0, H.P_w, H.S_w, H.S_n, H.P_n, H.P_g), "capaz_reference_init", __LINE__);
+  // S_g and the densities data_initialization also leaves in the host
+  // arrays (three-phase.cpp:429-434, 479-481).
+  for (long long l = 0; l < n; l++) {
+    H.S_g[l] = 1. - def.S_w_init - def.S_n_init;
+    H.ro_w[l] = def.ro0_w * (1. + (def.beta_w) * (H.P_w[l] - def.P_atm));
+    H.ro_n[l] = def.ro0_n * (1. + (def.beta_n) * (H.P_n[l] - def.P_atm));
+    H.ro_g[l] = def.ro0_g * H.P_g[l] / def.P_atm;
+  }
+#else
   check(capaz_reference_init(&p, H.m, 0, H.P_w, nullptr, H.S_n, nullptr, nullptr), "capaz_reference_init",
         __LINE__);
   // The densities data_initialization also leaves in the host arrays
   // (two-phase.cpp:147-150).
-  const long long n = (long long)def.locNx * def.locNy * def.locNz;
   for (long long l = 0; l < n; l++) {
     H.ro_w[l] = def.ro0_w * (1. + (def.beta_w) * (H.P_w[l] - def.P_atm));
     H.ro_n[l] = def.ro0_n * (1. + (def.beta_n) * (H.P_w[l] - def.P_atm));
   }
+#endif
 }
 
 // ---- stages ----------------------------------------------------------------

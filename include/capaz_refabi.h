@@ -1,9 +1,12 @@
 /*
- * capaz_refabi.h — link-level drop-in for the reference's two-phase GPU
- * backend (libcapaz_dropin_2ph.so).
+ * capaz_refabi.h — link-level drop-in for the reference's GPU backend:
+ * libcapaz_dropin_2ph.so for the two-phase build, libcapaz_dropin_3ph.so
+ * (this header with CAPAZ_REFABI_THREE_PHASE defined) for the three-phase
+ * build.
  *
  * The reference's host program (main.cpp + no_communication.cpp +
- * shared_test.cpp + gauss.cpp, built with -D TWO_PHASE) links one
+ * shared_test.cpp + gauss.cpp, built with -D TWO_PHASE or -D THREE_PHASE)
+ * links one
  * architecture backend: cpu.cpp or the CUDA object gpu.o (sh/run.sh:98-112,
  * 165).  This library exports, with C++ linkage and the reference's
  * signatures (defines.h:115-207), every symbol the host program takes from
@@ -11,10 +14,10 @@
  * the C ABI of include/capaz_b200.h; the whole step is one fused kernel.
  *
  * The two structs below must have the reference's member order and types
- * (defines.h:65-76 and 79-113 with TWO_PHASE defined, ENERGY undefined) so
- * that structs passed by value between the reference's objects and this
- * library agree byte for byte: sizeof(ptr_Arrays) == 160,
- * sizeof(consts) == 384 on x86-64.
+ * (defines.h:65-76 and 79-113 with TWO_PHASE or THREE_PHASE defined, ENERGY
+ * undefined) so that structs passed by value between the reference's
+ * objects and this library agree byte for byte: sizeof(ptr_Arrays) == 160,
+ * sizeof(consts) == 384 (two-phase), 232 and 488 (three-phase) on x86-64.
  *
  * Semantics, compared with the reference's gpu.cu:
  *   - device_initialization creates the context (device = rank % devices,
@@ -40,16 +43,24 @@
  */
 #ifndef CAPAZ_REFABI_H
 #define CAPAZ_REFABI_H
+/* Three-phase (libcapaz_dropin_3ph.so): the CPU model's physics, capillary
+ * pressures zero and K_0 throughout (three-phase.cpp), the whole top face a
+ * source when SOURCE > 0, as the reference's CPU backend computes it; the
+ * reference's GPU three-phase code differs from its CPU code, and the CPU
+ * code is the one followed. */
 
-/* defines.h:65-76 (TWO_PHASE). */
+/* defines.h:65-76. */
 struct ptr_Arrays_tag {
   double *S_n, *S_w, *P_w, *P_n, *ro_w, *ro_n, *ux_w, *uy_w, *uz_w, *ux_n, *uy_n, *uz_n, *Xi_w, *Xi_n, *roS_w,
       *roS_w_old, *roS_n, *roS_n_old;
   double *m, *K;
+#ifdef CAPAZ_REFABI_THREE_PHASE
+  double *S_g, *P_g, *ro_g, *ux_g, *uy_g, *uz_g, *Xi_g, *roS_g, *roS_g_old;
+#endif
 };
 typedef struct ptr_Arrays_tag ptr_Arrays;
 
-/* defines.h:79-113 (TWO_PHASE). */
+/* defines.h:79-113. */
 struct consts_tag {
   double upscale_l, upscale_t;
   double lambda[2];
@@ -61,7 +72,16 @@ struct consts_tag {
   int source, save_plots, print_screen, newton_iterations;
   double K[2];
   double Q, InjWell_Pw, InjWell_Sn, OutWell_Pw, OutWell_Sn, Background_Sn, Background_Pw;
+#ifdef CAPAZ_REFABI_THREE_PHASE
+  double S_w_init, S_n_init;
+  double S_nr[2];
+  double S_gr[2];
+  double P_d_nw[2];
+  double P_d_gn[2];
+  double c_g, beta_g, mu_g, ro0_g, S_w_gr;
+#else
   double P_d[2];
+#endif
   int locNx, locNy, locNz;
   int size, rank;
   int sizex, sizey, sizez;
@@ -91,7 +111,8 @@ void device_initialization(consts* def);
 void device_finalization(void);
 
 /* Initial state on the host arrays (defines.h:126), replacing the GPU
- * build's copy in two-phase.cu:6-65. */
+ * build's copy in two-phase.cu:6-65 (three-phase: three-phase.cpp:438-500,
+ * the CPU model's). */
 void data_initialization(ptr_Arrays HostArraysPtr, long int* time_counter, consts def);
 
 /* Halo pack/unpack for multi-rank backends (defines.h:196-207), replacing

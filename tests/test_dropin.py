@@ -1,4 +1,5 @@
-"""Link-level drop-in (include/capaz_refabi.h, libcapaz_dropin_2ph.so).
+"""Link-level drop-in (include/capaz_refabi.h, libcapaz_dropin_2ph.so and
+libcapaz_dropin_3ph.so).
 
 The reference's own host objects (main.cpp, no_communication.cpp,
 shared_test.cpp, gauss.cpp), compiled from its sources by oracle/Makefile,
@@ -12,13 +13,17 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_2PH, ROOT, interior, load_golden, rel_err
+from conftest import GOLDEN_2PH, GOLDEN_3PH, ROOT, interior, load_golden, rel_err
 from oracle import oracle as O
 
 DROPIN = os.path.join(ROOT, "capaz_b200", "lib", "libcapaz_dropin_2ph.so")
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "capaz_dropin_harness_2ph")
 MAIN_DROPIN = os.path.join(ROOT, "oracle", "_ref", "capaz_dropin_main_2ph")
 MAIN_REF = os.path.join(ROOT, "oracle", "_ref", "capaz_ref_main_2ph")
+DROPIN3 = os.path.join(ROOT, "capaz_b200", "lib", "libcapaz_dropin_3ph.so")
+HARNESS3 = os.path.join(ROOT, "oracle", "_ref", "capaz_dropin_harness_3ph")
+MAIN_DROPIN3 = os.path.join(ROOT, "oracle", "_ref", "capaz_dropin_main_3ph")
+MAIN_REF3 = os.path.join(ROOT, "oracle", "_ref", "capaz_ref_main_3ph")
 
 
 def declared_refabi_functions():
@@ -27,23 +32,26 @@ def declared_refabi_functions():
     return sorted(set(re.findall(r"^void\s+([A-Za-z_0-9]+)\s*\(", text, flags=re.M)))
 
 
-def test_dropin_exports_every_declared_function():
+@pytest.mark.parametrize("lib", [DROPIN, DROPIN3])
+def test_dropin_exports_every_declared_function(lib):
     names = declared_refabi_functions()
     assert len(names) == 27  # 6 stages, 5 memory, 2 device, init, 12 halo, checkErrors
-    out = subprocess.run(["nm", "-D", "--defined-only", "-C", DROPIN], capture_output=True, text=True,
+    out = subprocess.run(["nm", "-D", "--defined-only", "-C", lib], capture_output=True, text=True,
                          check=True).stdout
     for n in names:
         assert re.search(r"\s" + re.escape(n) + r"\(", out), n
 
 
-def test_dropin_covers_what_the_reference_host_program_needs():
+@pytest.mark.parametrize("exe,lib", [(MAIN_DROPIN, "libcapaz_dropin_2ph.so"),
+                                     (MAIN_DROPIN3, "libcapaz_dropin_3ph.so")])
+def test_dropin_covers_what_the_reference_host_program_needs(exe, lib):
     """Every symbol the reference's main.cpp takes from its arch backend is
     among those the drop-in exports (checked on the linked test binary)."""
-    if not os.path.exists(MAIN_DROPIN):
+    if not os.path.exists(exe):
         pytest.skip("drop-in link binaries not built (make -C oracle all)")
-    res = subprocess.run(["ldd", MAIN_DROPIN], capture_output=True, text=True)
+    res = subprocess.run(["ldd", exe], capture_output=True, text=True)
     assert "not found" not in res.stdout
-    assert "libcapaz_dropin_2ph.so" in res.stdout
+    assert lib in res.stdout
 
 
 def _plots(dirpath):
@@ -92,6 +100,69 @@ def test_reference_program_runs_unmodified_on_the_dropin(tmp_path):
         results[tag] = _plots(wd / "run" / "plots")
     assert results["ref"].keys() == results["dropin"].keys()
     assert len(results["ref"]) == 3  # t = 0, 0.1, 0.2
+    exact = total = 0
+    for f, lines in results["ref"].items():
+        other = results["dropin"][f]
+        assert len(lines) == len(other)
+        for a, b in zip(lines, other):
+            total += 1
+            if a == b:
+                exact += 1
+                continue
+            va = np.array([float(x) for x in a.split()])
+            vb = np.array([float(x) for x in b.split()])
+            assert np.allclose(va, vb, rtol=2e-3, atol=1e-30), (f, a, b)
+    assert exact / total > 0.999, f"{exact}/{total} plot lines identical"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", GOLDEN_3PH)
+def test_dropin3_harness_matches_reference(name):
+    """The reference's three-phase step loop driven through
+    libcapaz_dropin_3ph reproduces the reference CPU results."""
+    if not os.path.exists(HARNESS3):
+        pytest.skip("drop-in link binaries not built (make -C oracle all)")
+    p, g = load_golden(name)
+    names = ["P_w", "S_w", "S_n", "P_n", "P_g"]
+    if "in_P_w" in g:
+        state, m = {k: g["in_" + k] for k in names}, g["in_m"]
+    else:
+        state, m = None, None
+    r = O.ref_run(p, int(g["nsteps"]), state, m, binary=HARNESS3, derived=True)
+    for k in names:
+        assert rel_err(r[k], g["out_" + k]) <= 1e-12, k
+    for f, v in r["derived"].items():
+        a, b = v, g["der_" + f]
+        if f.startswith("roS"):
+            a, b = interior(a), interior(b)
+        assert rel_err(a, b) <= 1e-12, f
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(9, 8, 6), (1, 15, 1)])
+def test_reference_three_phase_program_runs_unmodified_on_the_dropin(tmp_path, shape):
+    """The reference's whole THREE_PHASE program with libcapaz_dropin_3ph in
+    place of its backend writes the plot files its CPU backend writes."""
+    from capaz_b200.simulation import default_params
+    if not os.path.exists(MAIN_DROPIN3):
+        pytest.skip("drop-in link binaries not built (make -C oracle all)")
+    nx, ny, nz = shape
+    p = default_params(phases=3, nx=nx, ny=ny, nz=nz, newton_iterations=7, lambda_=2.0, S_wr=0.1, S_nr=0.05,
+                       S_gr=0.02, ro0_w=1000.0, ro0_n=850.0, ro0_g=1.2, mu_w=1e-3, mu_n=3e-3, mu_g=1.8e-5,
+                       beta_w=1e-9, beta_n=1e-9, beta_g=9.2e-6, S_w_gr=0.25, S_n_gr=0.7, S_w_init=0.2,
+                       S_n_init=0.3, source=1, porosity=0.3, K0=1e-12, hx=1.0, hy=1.0, hz=1.0, dt=1e-3,
+                       g_const=9.81, P_d=0.0, timeX=0.06)
+    ini = O.ref_ini_text(p).replace("SAVE_PLOTS=1000000", "SAVE_PLOTS=30")
+    results = {}
+    for tag, exe in (("ref", MAIN_REF3), ("dropin", MAIN_DROPIN3)):
+        wd = tmp_path / tag
+        (wd / "run").mkdir(parents=True)
+        (wd / "defines.ini").write_text(ini)
+        res = subprocess.run([exe], cwd=wd / "run", capture_output=True, text=True, timeout=600)
+        assert res.returncode == 0, res.stdout[-2000:] + res.stderr[-2000:]
+        results[tag] = _plots(wd / "run" / "plots")
+    assert results["ref"].keys() == results["dropin"].keys()
+    assert len(results["ref"]) == 3
     exact = total = 0
     for f, lines in results["ref"].items():
         other = results["dropin"][f]
