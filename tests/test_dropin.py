@@ -142,7 +142,11 @@ def test_dropin3_harness_matches_reference(name):
 @pytest.mark.parametrize("shape", [(9, 8, 6), (1, 15, 1)])
 def test_reference_three_phase_program_runs_unmodified_on_the_dropin(tmp_path, shape):
     """The reference's whole THREE_PHASE program with libcapaz_dropin_3ph in
-    place of its backend writes the plot files its CPU backend writes."""
+    place of its backend writes the plot files its CPU backend writes, except
+    the S_g column: save_data_plots downloads S_w, S_n, P_w and the
+    velocities but not S_g (main.cpp:475-491), so with any device backend
+    (the reference's own gpu.o too) the plot shows the host copy that
+    data_initialization left, while the CPU backend updates it in place."""
     from capaz_b200.simulation import default_params
     if not os.path.exists(MAIN_DROPIN3):
         pytest.skip("drop-in link binaries not built (make -C oracle all)")
@@ -153,6 +157,7 @@ def test_reference_three_phase_program_runs_unmodified_on_the_dropin(tmp_path, s
                        S_n_init=0.3, source=1, porosity=0.3, K0=1e-12, hx=1.0, hy=1.0, hz=1.0, dt=1e-3,
                        g_const=9.81, P_d=0.0, timeX=0.06)
     ini = O.ref_ini_text(p).replace("SAVE_PLOTS=1000000", "SAVE_PLOTS=30")
+    sg_col = 3 if nx == 1 and nz == 1 else 5  # "Y",S_w,S_n,S_g... / "X","Y","Z",S_w,S_n,S_g...
     results = {}
     for tag, exe in (("ref", MAIN_REF3), ("dropin", MAIN_DROPIN3)):
         wd = tmp_path / tag
@@ -167,13 +172,18 @@ def test_reference_three_phase_program_runs_unmodified_on_the_dropin(tmp_path, s
     for f, lines in results["ref"].items():
         other = results["dropin"][f]
         assert len(lines) == len(other)
-        for a, b in zip(lines, other):
+        for q, (a, b) in enumerate(zip(lines, other)):
+            if q < 3:  # TITLE, VARIABLES, ZONE
+                assert a == b
+                continue
+            ta, tb = a.split(), b.split()
+            del ta[sg_col], tb[sg_col]
             total += 1
-            if a == b:
+            if ta == tb:
                 exact += 1
                 continue
-            va = np.array([float(x) for x in a.split()])
-            vb = np.array([float(x) for x in b.split()])
+            va = np.array([float(x) for x in ta])
+            vb = np.array([float(x) for x in tb])
             assert np.allclose(va, vb, rtol=2e-3, atol=1e-30), (f, a, b)
     assert exact / total > 0.999, f"{exact}/{total} plot lines identical"
 
