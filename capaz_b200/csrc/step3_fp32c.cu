@@ -58,7 +58,7 @@ __device__ __forceinline__ void relperm3f(const Step3FConst& f, float S_w_e, flo
     const float k_n_w = sqrtf(1.f - S_w_e) * p3(1.f - p1(S_w_e));
     const float t = 1.f - p2(1.f - p1(S_n_e));
     const float k_n_g = sqrtf(S_n_e) * t * t;
-    k_n = S_n_e * k_n_w * k_n_g / (1.f - S_w_e) / (1.f - S_g_e);
+    k_n = __fdividef(__fdividef(S_n_e * k_n_w * k_n_g, 1.f - S_w_e), 1.f - S_g_e);
   }
 }
 
@@ -104,25 +104,45 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     ke = min(kb + c.zchunk, c.nz - 1);
   }
   const float den_inv = c.inv_den;
+  static_assert(PC <= 2 * NTHREADS, "a thread derives at most two window cells per plane");
+
+  // The (at most two) window cells this thread derives in every plane:
+  // window index, grid offset in the plane, row, and whether the cell lies on
+  // the grid and on an x/y boundary (whose P_n, P_g are stored state).
+  int wq[2], wrow[2];
+  long long woff[2];
+  bool won[2], wbnd[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int q = tid + h * NTHREADS;
+    const int gi = i0 - 1 + q % PX, gj = j0 - 1 + q / PX;
+    wq[h] = q;
+    won[h] = q < PC && gi >= 0 && gi < c.nx && gj < c.ny;
+    wrow[h] = won[h] ? gj : 0;
+    woff[h] = won[h] ? gi + gj * c.sy : 0;
+    wbnd[h] = !((((gi != 0) && (gi != c.nx - 1)) || (c.nx < 2)) && (gj != 0) && (gj != c.ny - 1));
+  }
 
   // Derive plane k of the window into its ring slot.
   auto fill = [&](int k) {
     Plane3F& P = ring[k % 3];
-    for (int q = tid; q < PC; q += NTHREADS) {
-      const int gi = i0 - 1 + q % PX, gj = j0 - 1 + q / PX;
-      if (gi >= 0 && gi < c.nx && gj < c.ny) {
-        const long long l = gi + gj * c.sy + (long long)k * c.sz;
-        const float pw = a.p_w[l];
+    const bool kbnd = !(((k != 0) && (k != c.nz - 1)) || (c.nz < 2));
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (won[h]) {
+        const int q = wq[h], gj = wrow[h];
+        const long long l = woff[h] + (long long)k * c.sz;
+        const float pw = __ldg(a.p_w + l);
         float pn = pw, pg = pw;  // interior: P_n = P_g = P_w (capillary pressures zero)
-        if (!interior3f(c, gi, gj, k)) {
-          pn = a.p_n[l];
-          pg = a.p_g[l];
+        if (wbnd[h] || kbnd) {
+          pn = __ldg(a.p_n + l);
+          pg = __ldg(a.p_g + l);
         }
-        const float Sw = c.S_ref_w_f + a.s_w[l], Sn = c.S_ref_n_f + a.s_n[l];
+        const float Sw = c.S_ref_w_f + __ldg(a.s_w + l), Sn = c.S_ref_n_f + __ldg(a.s_n + l);
         const float S_w_e = (Sw - c.S_wr_f) * den_inv, S_n_e = (Sn - c.S_nr_f) * den_inv;
         float k_w, k_n, k_g;
         relperm3f<A2>(c, S_w_e, S_n_e, k_w, k_n, k_g);
-        const float Kl = UNIK ? c.K0_f : a.K[l];
+        const float Kl = UNIK ? c.K0_f : __ldg(a.K + l);
         const float4 r = a.rowF[gj];  // rho_p(P_ref(j)) for w, n, g
         P.p[0][q] = pw;
         P.p[1][q] = pn;
@@ -180,32 +200,33 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         div[ph] = s - comp;
       }
       // Conserved increments d(rho S)_p = -dt/m div F_p, then Newton in FP64.
-      const float dtm = c.dt_f / mc;
+      const float dtm = __fdividef(c.dt_f, mc);
       const double dAw = (double)(-dtm * div[0]), dAn = (double)(-dtm * div[1]), dAg = (double)(-dtm * div[2]);
       const double prel = a.Pref[j] - c.P_atm;
       const double pw0 = (double)C.p[0][cidx];
       const double P = a.Pref[j] + pw0;
       const double Sw = c.S_ref_w + (double)sw0, Sn = c.S_ref_n + (double)sn0, Sg = 1. - Sw - Sn;
       const double rw = fma(c.aw, prel + pw0, c.ro0_w), rn = fma(c.an, prel + pw0, c.ro0_n);
-      double dP = 0., dSw = 0., dSn = 0.;
-      for (int it = 0; it < 2; it++) {
-        const double dSg = -dSw - dSn;
-        const double R1 = c.aw * dP * (Sw + dSw) + rw * dSw - dAw;
-        const double R2 = c.an * dP * (Sn + dSn) + rn * dSn - dAn;
-        const double R3 = c.bg * (dP * (Sg + dSg) + P * dSg) - dAg;
-        // Jacobian in (dP, dSw, dSn)
-        const double a11 = c.aw * (Sw + dSw), a12 = c.aw * dP + rw, a13 = 0.;
-        const double a21 = c.an * (Sn + dSn), a22 = 0., a23 = c.an * dP + rn;
-        const double a31 = c.bg * (Sg + dSg), a32 = -c.bg * (P + dP), a33 = a32;
-        const double c11 = a22 * a33 - a23 * a32, c12 = a23 * a31 - a21 * a33, c13 = a21 * a32 - a22 * a31;
-        const double det = a11 * c11 + a12 * c12 + a13 * c13;
-        const double inv = 1. / det;
-        const double x1 = (R1 * c11 + a12 * (a23 * R3 - R2 * a33) + a13 * (R2 * a32 - a22 * R3)) * inv;
-        const double x2 = (a11 * (R2 * a33 - a23 * R3) + R1 * c12 + a13 * (a21 * R3 - R2 * a31)) * inv;
-        const double x3 = (a11 * (a22 * R3 - R2 * a32) + a12 * (R2 * a31 - a21 * R3) + R1 * c13) * inv;
-        dP -= x1;
-        dSw -= x2;
-        dSn -= x3;
+      // One Newton step from the stored state (zero increments): the
+      // Jacobian solve of the bilinear system, exact up to the dP dS terms
+      // (relative size |dS| / S of the increments).  Jacobian in
+      // (dP, dS_w, dS_n), with a13 = a22 = 0 and a33 = a32:
+      //   [aw Sw   rw       0  ]
+      //   [an Sn   0        rn ]
+      //   [bg Sg  -bg P   -bg P]
+      // and right-hand side (dAw, dAn, dAg).
+      double dP, dSw, dSn;
+      {
+        const double a11 = c.aw * Sw, a12 = rw;
+        const double a21 = c.an * Sn, a23 = rn;
+        const double a31 = c.bg * Sg, a32 = -c.bg * P;
+        const double c11 = -a23 * a32, c12 = a23 * a31 - a21 * a32, c13 = a21 * a32;
+        const double det = a11 * c11 + a12 * c12;
+        double inv = (double)__frcp_rn((float)det);  // FP32 seed, one Newton-Raphson step: 2^-46
+        inv = inv * fma(-det, inv, 2.0);
+        dP = (dAw * c11 + a12 * (a23 * dAg - dAn * a32)) * inv;
+        dSw = (a11 * (dAn * a32 - a23 * dAg) + dAw * c12) * inv;
+        dSn = (a12 * (dAn * a31 - a21 * dAg) + dAw * c13 - a11 * dAn * a32) * inv;
       }
       const double Pn1 = P + dP, Swn = Sw + dSw, Snn = Sn + dSn;
       a.o_pw[l] = (float)(pw0 + dP);
@@ -219,22 +240,20 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       const bool edge = (xb && (i == 1 || i == c.nx - 2)) || (j == 1) || (j == c.ny - 2) ||
                         (!PLANAR && ((k == 1) || (k == c.nz - 2)));
       if (edge) {
-        int xs[3], ys[3], zs[3], nxs = 0, nys = 0, nzs = 0;
-        xs[nxs++] = i;
-        if (xb && i == 1) xs[nxs++] = 0;
-        if (xb && i == c.nx - 2) xs[nxs++] = c.nx - 1;
-        ys[nys++] = j;
-        if (j == 1) ys[nys++] = 0;
-        if (j == c.ny - 2) ys[nys++] = c.ny - 1;
-        zs[nzs++] = k;
-        if (!PLANAR) {
-          if (k == 1) zs[nzs++] = 0;
-          if (k == c.nz - 2) zs[nzs++] = c.nz - 1;
-        }
-        for (int qa = 0; qa < nxs; qa++)
-          for (int qb = 0; qb < nys; qb++)
-            for (int qd = 0; qd < nzs; qd++) {
+        // Candidate coordinates per axis: the cell's own, then the boundary
+        // planes it is the basic coordinate of (-1: none).  Fixed-size,
+        // fully unrolled loops keep these in registers.
+        const int xs[3] = {i, (xb && i == 1) ? 0 : -1, (xb && i == c.nx - 2) ? c.nx - 1 : -1};
+        const int ys[3] = {j, (j == 1) ? 0 : -1, (j == c.ny - 2) ? c.ny - 1 : -1};
+        const int zs[3] = {k, (!PLANAR && k == 1) ? 0 : -1, (!PLANAR && k == c.nz - 2) ? c.nz - 1 : -1};
+#pragma unroll
+        for (int qa = 0; qa < 3; qa++)
+#pragma unroll
+          for (int qb = 0; qb < 3; qb++)
+#pragma unroll
+            for (int qd = 0; qd < 3; qd++) {
               if (qa == 0 && qb == 0 && qd == 0) continue;
+              if (xs[qa] < 0 || ys[qb] < 0 || zs[qd] < 0) continue;
               const int bj = ys[qb], bi = xs[qa], bk = zs[qd];
               const long long lb = bi + bj * c.sy + (long long)bk * c.sz;
               double sw = Swn, sn = Snn;
