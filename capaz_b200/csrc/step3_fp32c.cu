@@ -23,6 +23,7 @@
 // Diagnostics (mass per phase, the reference Newton functions' residual at
 // the result, non-finite cells) are evaluated in FP64.
 #include <math.h>
+#include <stdint.h>
 
 #include "capaz_internal.h"
 
@@ -35,7 +36,28 @@ struct Plane3F {
   float p[3][PC];
   float M[3][PC];
 };
-constexpr size_t kSmem3F = 3 * sizeof(Plane3F);
+// Raw state of one plane of the window, copied from global memory ahead of
+// its derive with cp.async (each thread copies and derives its own cells).
+struct Raw3F {
+  float pw[PC], sw[PC], sn[PC], K[PC], pn[PC], pg[PC];
+};
+constexpr int NRING = 4;  // derived planes: k-1, k, k+1 read while k+2 is derived
+struct Smem3F {
+  Plane3F ring[NRING];
+  Raw3F raw[2];
+};
+constexpr size_t kSmem3F = sizeof(Smem3F);
+
+__device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // Square root for the FP32 relative permeabilities: x * rsqrt(x) (a few
 // ulp, no slow path), 0 for x <= 0.
@@ -91,7 +113,8 @@ template <bool UNIK, bool PLANAR, bool DIAG, bool A2>
 __global__ void __launch_bounds__(NTHREADS, 2)
     step3_fp32c_kernel(const Step3FConst c, const Step3FArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Plane3F* ring = reinterpret_cast<Plane3F*>(smem_raw);
+  Smem3F& sm = *reinterpret_cast<Smem3F*>(smem_raw);
+  Plane3F* ring = sm.ring;
   const int tid = threadIdx.x + TX * threadIdx.y;
   const int tile = blockIdx.x;
   const int ti = tile % c.tiles_x, tj = tile / c.tiles_x;
@@ -127,26 +150,49 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     wbnd[h] = !((((gi != 0) && (gi != c.nx - 1)) || (c.nx < 2)) && (gj != 0) && (gj != c.ny - 1));
   }
 
-  // Derive plane k of the window into its ring slot.
-  auto fill = [&](int k) {
-    Plane3F& P = ring[k % 3];
-    const bool kbnd = !(((k != 0) && (k != c.nz - 1)) || (c.nz < 2));
+  auto kbnd_of = [&](int k) { return !(((k != 0) && (k != c.nz - 1)) || (c.nz < 2)); };
+  // Start copying the raw state of plane k's window cells of this thread
+  // into raw stage b (one commit group per plane).
+  auto issue = [&](int k, int b) {
+    Raw3F& R = sm.raw[b];
+    const bool kbnd = kbnd_of(k);
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (won[h]) {
+        const int q = wq[h];
+        const long long l = woff[h] + (long long)k * c.sz;
+        cp_async4(&R.pw[q], a.p_w + l);
+        cp_async4(&R.sw[q], a.s_w + l);
+        cp_async4(&R.sn[q], a.s_n + l);
+        if (!UNIK) cp_async4(&R.K[q], a.K + l);
+        if (wbnd[h] || kbnd) {
+          cp_async4(&R.pn[q], a.p_n + l);
+          cp_async4(&R.pg[q], a.p_g + l);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  // Derive plane k of the window from raw stage b into its ring slot.
+  auto fill = [&](int k, int b) {
+    Plane3F& P = ring[k % NRING];
+    const Raw3F& R = sm.raw[b];
+    const bool kbnd = kbnd_of(k);
 #pragma unroll
     for (int h = 0; h < 2; h++) {
       if (won[h]) {
         const int q = wq[h], gj = wrow[h];
-        const long long l = woff[h] + (long long)k * c.sz;
-        const float pw = __ldg(a.p_w + l);
+        const float pw = R.pw[q];
         float pn = pw, pg = pw;  // interior: P_n = P_g = P_w (capillary pressures zero)
         if (wbnd[h] || kbnd) {
-          pn = __ldg(a.p_n + l);
-          pg = __ldg(a.p_g + l);
+          pn = R.pn[q];
+          pg = R.pg[q];
         }
-        const float Sw = c.S_ref_w_f + __ldg(a.s_w + l), Sn = c.S_ref_n_f + __ldg(a.s_n + l);
+        const float Sw = c.S_ref_w_f + R.sw[q], Sn = c.S_ref_n_f + R.sn[q];
         const float S_w_e = (Sw - c.S_wr_f) * den_inv, S_n_e = (Sn - c.S_nr_f) * den_inv;
         float k_w, k_n, k_g;
         relperm3f<A2>(c, S_w_e, S_n_e, k_w, k_n, k_g);
-        const float Kl = UNIK ? c.K0_f : __ldg(a.K + l);
+        const float Kl = UNIK ? c.K0_f : R.K[q];
         const float4 r = a.rowF[gj];  // rho_p(P_ref(j)) for w, n, g
         P.p[0][q] = pw;
         P.p[1][q] = pn;
@@ -159,13 +205,35 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   };
 
   double acc[3] = {0., 0., 0.}, rmax = 0., nonfinite = 0.;
-  if (!PLANAR) fill(kb - 1);
-  fill(kb);
+  // Pipeline: the raw copy of plane k+2 is in flight while plane k+1 is
+  // derived and plane k updated; plane k+1 goes into a ring slot that no
+  // thread still reads (the update of k-1 read k-2..k), so one barrier per
+  // plane suffices.  Raw stage of plane q: (q - kb + 1) & 1.
+  if (PLANAR) {
+    issue(kb, 0);
+    cp_async_wait<0>();
+    fill(kb, 0);
+  } else {
+    issue(kb - 1, 0);
+    issue(kb, 1);
+    cp_async_wait<1>();
+    fill(kb - 1, 0);
+    if (kb + 1 <= ke) issue(kb + 1, 0);
+    else cp_async_commit();  // keep one group per plane
+    cp_async_wait<1>();
+    fill(kb, 1);
+  }
   for (int k = kb; k < ke; k++) {
-    if (!PLANAR) fill(k + 1);
+    if (!PLANAR) {
+      const int b1 = (k + 1 - kb + 1) & 1;  // stage of plane k+1
+      if (k + 2 <= ke) issue(k + 2, b1 ^ 1);
+      else cp_async_commit();
+      cp_async_wait<1>();
+      fill(k + 1, b1);
+    }
     __syncthreads();
     if (active) {
-      const Plane3F& C = ring[k % 3];
+      const Plane3F& C = ring[k % NRING];
       const long long l = i + j * c.sy + (long long)k * c.sz;
       const float mc = a.m[l];
       const float sw0 = a.s_w[l], sn0 = a.s_n[l];
@@ -192,8 +260,8 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         float s = fx + fy;
         float comp = (s - fx) - fy;
         if (!PLANAR) {
-          const Plane3F& Mz = ring[(k + 2) % 3];
-          const Plane3F& Qz = ring[(k + 1) % 3];
+          const Plane3F& Mz = ring[(k - 1) % NRING];
+          const Plane3F& Qz = ring[(k + 1) % NRING];
           const float fz = face((Mz.p[ph][cidx] - pc) * c.inv_hz2_f, (pc - Qz.p[ph][cidx]) * c.inv_hz2_f, Mc,
                                 Mz.M[ph][cidx], Qz.M[ph][cidx]);
           const float y = fz - comp;
@@ -307,8 +375,8 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         if (!finite) nonfinite += 1.;
       }
     }
-    __syncthreads();
   }
+  cp_async_wait<0>();
 
   if (DIAG) {
     __shared__ double red[NTHREADS / 32][5];
