@@ -4,7 +4,9 @@
 // P_w, P_n, P_g from the per-row reference pressure P_ref(j) (the row means
 // of P_w when it was set), saturations S_w, S_n from their grid means.  One
 // launch per step, tiled as the FP64 three-phase step (32 x 8 columns per
-// CTA marching along z with a 3-plane ring in shared memory):
+// CTA marching along z); the raw state of each plane's window is copied into
+// shared memory with cp.async two planes ahead, and the derived planes live
+// in a 4-slot ring, so one barrier per plane suffices:
 //   - every cell of the plane window is derived in FP32: effective
 //     saturations, the reference CPU relative permeabilities
 //     (three-phase.cpp:146-186; square roots when A = 2), densities from the
@@ -13,10 +15,11 @@
 //   - the upwind flux difference of each phase (cpu.cpp:236-264 in select
 //     form) is formed per axis as out - in, the three axis terms Kahan-summed
 //     in FP32; d(rho S)_p = -dt/m div F_p goes to FP64;
-//   - two Newton iterations in FP64 solve the exact bilinear increment
-//     equations rho_p(P + dP)(S_p + dS_p) - rho_p(P) S_p = d(rho S)_p for
-//     (dP, dS_w, dS_n) (S_g = 1 - S_w - S_n), with the 3x3 Jacobian solved
-//     by Cramer's rule; the new deviations are rounded to FP32 once;
+//   - one Newton step in FP64 from the stored state solves the bilinear
+//     increment equations rho_p(P + dP)(S_p + dS_p) - rho_p(P) S_p =
+//     d(rho S)_p for (dP, dS_w, dS_n) (S_g = 1 - S_w - S_n) up to the dP dS
+//     terms, with the 3x3 Jacobian solved by Cramer's rule and a refined
+//     FP32-seeded reciprocal; the new deviations are rounded to FP32 once;
 //   - boundary cells (Border_S, Border_P of three-phase.cpp:345-427) are
 //     written by the thread of their basic-coordinate cell in FP64 from its
 //     new state, as in the FP64 step.
