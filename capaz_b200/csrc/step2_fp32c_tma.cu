@@ -251,6 +251,9 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
   }
 
   double acc_w = 0., acc_n = 0., rmax = 0., nonfinite = 0.;
+  // Diagnostics: masses summed without the cell volume (applied once per
+  // CTA), residuals scaled by 1/rho_0 (one division per thread).
+  const double inv_ro0_w = DIAG ? 1. / f.ro0_w : 0., inv_ro0_n = DIAG ? 1. / f.ro0_n : 0.;
   // Everything above overlaps the previous kernel's tail; the work counter and
   // the state are touched only after it has completed.
   grid_dependency_wait();
@@ -385,9 +388,9 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
         const double S1 = S_ref + (double)snew;
         const double P1rel = prel + (double)pn;
         const double rw1 = fma(f.aw, P1rel, f.ro0_w), rn1 = fma(f.bn, P1rel, f.ro0_n);
-        acc_w += (double)mc * rw1 * (1. - S1) * f.vol;
-        acc_n += (double)mc * rn1 * S1 * f.vol;
-        const double r = fmax(fabs(F1) / f.ro0_w, fabs(F2) / f.ro0_n);
+        acc_w += (double)mc * rw1 * (1. - S1);
+        acc_n += (double)mc * rn1 * S1;
+        const double r = fmax(fabs(F1) * inv_ro0_w, fabs(F2) * inv_ro0_n);
         if (!(r <= rmax)) rmax = r;
         if (!finite) nonfinite += 1.;
       }
@@ -488,8 +491,8 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
         t3 += red[q][3];
       }
       double* out = diag_partials + (size_t)DIAG_STRIDE * blockIdx.x;
-      out[0] = t0;
-      out[1] = t1;
+      out[0] = t0 * f.vol;
+      out[1] = t1 * f.vol;
       out[2] = 0.;
       out[3] = t2;
       out[4] = t3;
