@@ -109,6 +109,23 @@ class HaloExchange:
                 set_plane(f, L.nz_local - 1, self.recv[(f, "hi")])
 
 
+def reduce_diag(d: dict, device, group=None) -> dict:
+    """Diagnostics of the whole grid from each rank's slab diagnostics (the
+    reference's global checks after its MPI exchanges): one all-reduce of the
+    phase masses and non-finite counts (sum) and one of the largest Newton
+    residual (max).  A slab's diagnostics cover its local interior cells,
+    which are exactly its owned interior cells (halo planes are local
+    boundary planes), so the sums count every interior cell of the grid once."""
+    import torch
+    import torch.distributed as dist
+    sums = torch.tensor(list(d["mass"]) + [d["nonfinite_cells"]], dtype=torch.float64, device=device)
+    mx = torch.tensor([d["max_residual"]], dtype=torch.float64, device=device)
+    dist.all_reduce(sums, op=dist.ReduceOp.SUM, group=group)
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX, group=group)
+    v = sums.cpu().tolist()
+    return {"mass": v[:3], "max_residual": float(mx.cpu().item()), "nonfinite_cells": v[3]}
+
+
 def state_fields(p: Params) -> list[str]:
     return ["P_w", "S_n"] + (["S_w", "P_n", "P_g"] if p.phases == 3 else [])
 
@@ -149,6 +166,11 @@ class SlabSimulation:
         for _ in range(nsteps):
             self.sim.step(1, self.stream)
             self.halo.exchange(self._get, self._set)
+
+    def diag(self) -> dict:
+        """Diagnostics of the last step over the whole grid (needs
+        FLAG_DIAGNOSTICS; every rank calls it)."""
+        return reduce_diag(self.sim.diag(self.stream), self.device, self.group)
 
     def owned_field(self, name: str) -> np.ndarray:
         return self.layout.owned(self.sim.get_field(name))

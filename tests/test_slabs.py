@@ -12,8 +12,9 @@ import socket
 import numpy as np
 import pytest
 
+from capaz_b200 import native
 from capaz_b200.native import FORM_FP32C, FORM_FP64
-from capaz_b200.slabs import HaloExchange, SlabLayout, partition, state_fields
+from capaz_b200.slabs import HaloExchange, SlabLayout, partition, reduce_diag, state_fields
 from capaz_b200.simulation import default_params
 
 
@@ -69,10 +70,19 @@ def _gloo_rank(rank, world, port, nz, nsteps, out):
         L = SlabLayout(nz, rank, world)
         slab = OracleSlab(p, L, m)
         halo = HaloExchange(L, p.nx * p.ny, state_fields(p), "cpu")
-        for _ in range(nsteps):
-            slab.step()
+        for t in range(nsteps):
+            if t == nsteps - 1:
+                # the last step with diagnostics, reduced over the ranks
+                q = slab.p.copy()
+                q.flags |= native.FLAG_DIAGNOSTICS
+                r = slab.O.step(q, slab.state, 1, slab.m, diag=True)
+                slab.state = {k: r[k] for k in slab.state}
+                d = reduce_diag(r["diag"], "cpu")
+            else:
+                slab.step()
             halo.exchange(slab.get_plane, slab.set_plane)
-        np.savez(os.path.join(out, f"r{rank}.npz"), P=L.owned(slab.state["P_w"]), S=L.owned(slab.state["S_n"]))
+        np.savez(os.path.join(out, f"r{rank}.npz"), P=L.owned(slab.state["P_w"]), S=L.owned(slab.state["S_n"]),
+                 mass=np.array(d["mass"]), rmax=d["max_residual"], nonfinite=d["nonfinite_cells"])
     finally:
         dist.destroy_process_group()
 
@@ -95,6 +105,16 @@ def test_decomposed_oracle_equals_whole_grid(tmp_path, world):
     P = np.concatenate([q["P"] for q in parts])
     S = np.concatenate([q["S"] for q in parts])
     assert np.array_equal(P, ref["P_w"]) and np.array_equal(S, ref["S_n"])
+    # global diagnostics: every rank holds the same reduction, equal to the
+    # whole grid's up to the order of the sums
+    q = p.copy()
+    q.flags |= native.FLAG_DIAGNOSTICS
+    whole = O.step(q, {"P_w": st["P_w"], "S_n": st["S_n"]}, nsteps, m, diag=True)["diag"]
+    for part in parts:
+        for a in range(2):
+            assert abs(part["mass"][a] - whole["mass"][a]) <= 1e-12 * abs(whole["mass"][a])
+        assert float(part["rmax"]) == whole["max_residual"]
+        assert float(part["nonfinite"]) == whole["nonfinite_cells"] == 0
 
 
 @pytest.mark.gpu
