@@ -40,7 +40,9 @@ __device__ __forceinline__ double directed(double x1, double x2, double Xc, doub
 // on [a | I] that looks for another pivot row only when |pivot| < 1e-8,
 // taking the last row below with entry > 1e-8.  Returns false where the
 // reference reports a zero determinant (it then leaves `a` unchanged).
-template <int N>
+// RCP: scale the pivot row by the pivot's reciprocal (one division per row
+// instead of 2N; each entry within an ulp of the reference's quotient).
+template <int N, bool RCP = false>
 __device__ __forceinline__ bool reverse_matrix(double* a) {
   const double e = 1E-8;
   double matr[N][2 * N];
@@ -71,8 +73,14 @@ __device__ __forceinline__ bool reverse_matrix(double* a) {
       }
       if (det_flag == 0) return false;
     }
+    if (RCP) {
+      const double r = 1. / f;
 #pragma unroll
-    for (int j = 0; j < 2 * N; j++) matr[k][j] /= f;
+      for (int j = 0; j < 2 * N; j++) matr[k][j] *= r;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 2 * N; j++) matr[k][j] /= f;
+    }
 #pragma unroll
     for (int i = 0; i < N; i++)
       if (i != k) {

@@ -308,7 +308,7 @@ __global__ void energy_newton_kernel(const Step3Const c, EnergyState st, const d
     dF[4 + N * 4] = ml * (Sw * (dwT * Hw + ro_w(c, P, T) * c_w(T)) + Sn * (dnT * Hn + ro_n(c, P, T) * c_n(T)) +
                           Sg * (dgT * Hg + ro_g(c, P, T) * c_g(T))) +
                     (1. - ml) * ro_r * c_r(T);
-    phys3::reverse_matrix<N>(dF);
+    phys3::reverse_matrix<N, true>(dF);
     double corr[N];
 #pragma unroll
     for (int a = 0; a < N; a++) {
