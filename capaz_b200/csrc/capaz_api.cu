@@ -125,6 +125,9 @@ Step2Const make_step2_const(const capaz_params& p) {
   c.se_fast_min = 0.;
   if (p.P_d == 0. && lam > 0. && (1. - p.S_wr) > 0. && isfinite(c.e_aaa) && c.e_aaa < 0.)
     c.se_fast_min = ldexp(1.0, (int)floor(1000. / c.e_aaa) + 1);
+  // num > 2 t (1 - S_wr) gives num / (1 - S_wr) > 2 t exactly, so the
+  // rounded quotient is >= t: the Newton iterations skip the division.
+  c.se_fast_num = 2. * c.se_fast_min * (1. - p.S_wr);
   c.vol = p.hx * p.hy * p.hz;
   return c;
 }

@@ -45,6 +45,7 @@ struct Step2Const {
   double e_pk;        // -1./lambda                two-phase.cpp:13, 36
   double e_aaa;       // (-1./lambda) - 1.         two-phase.cpp:37
   double se_fast_min; // S_e at or above which P_d*pow(S_e, e) == +0 exactly
+  double se_fast_num; // 1 - S_n - S_wr above which S_e >= se_fast_min without dividing
   double vol;         // hx*hy*hz (diagnostics)
 };
 

@@ -69,9 +69,13 @@ template <bool PD0>
 __device__ __forceinline__ void newton2(const Step2Const& c, double roS_w, double roS_n, double& Pw,
                                         double& Sn) {
   for (int w = 1; w <= c.iters; w++) {
-    double S_e = (1 - Sn - c.S_wr) / (1 - c.S_wr);
     double P_k, PkS;
-    if (PD0 && S_e >= c.se_fast_min) {
+    // P_d == 0: P_k and PkS are +0 whenever S_e is above the threshold;
+    // the numerator alone decides that in all but a sliver next to it.
+    if (PD0 && (1 - Sn - c.S_wr) > c.se_fast_num) {
+      P_k = 0.;
+      PkS = 0.;
+    } else if (double S_e = (1 - Sn - c.S_wr) / (1 - c.S_wr); PD0 && S_e >= c.se_fast_min) {
       P_k = 0.;
       PkS = 0.;
     } else {
