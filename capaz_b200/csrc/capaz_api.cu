@@ -662,6 +662,14 @@ int capaz_read_diag(capaz_ctx* ctx, capaz_diag* out, void* stream) {
   if (!ctx || !out) return CAPAZ_ERR_INVALID_ARGUMENT;
   return ctx->read_diag(out, (cudaStream_t)stream);
 }
+int capaz_post_diag(capaz_ctx* ctx, int slot, void* stream) {
+  if (!ctx || slot < 0 || slot >= CAPAZ_DIAG_SLOTS) return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->post_diag(slot, (cudaStream_t)stream);
+}
+int capaz_wait_diag(capaz_ctx* ctx, int slot, capaz_diag* out) {
+  if (!ctx || !out || slot < 0 || slot >= CAPAZ_DIAG_SLOTS) return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->wait_diag(slot, out);
+}
 int capaz_sync(capaz_ctx* ctx) {
   if (!ctx) return CAPAZ_ERR_INVALID_ARGUMENT;
   return ctx->sync();
@@ -703,6 +711,10 @@ int capaz_ctx::allocate() {
   CUDA_TRY(this, cudaMemset(err_flag, 0, sizeof(unsigned int)));
   CUDA_TRY(this, cudaMalloc(&diag_out, sizeof(double) * DIAG_STRIDE));
   CUDA_TRY(this, cudaMemset(diag_out, 0, sizeof(double) * DIAG_STRIDE));
+  CUDA_TRY(this, cudaHostAlloc(&diag_host, sizeof(double) * DIAG_STRIDE * (CAPAZ_DIAG_SLOTS + 1), cudaHostAllocMapped));
+  CUDA_TRY(this, cudaHostGetDevicePointer(&diag_host_dev, diag_host, 0));
+  for (int q = 0; q <= CAPAZ_DIAG_SLOTS; q++)
+    CUDA_TRY(this, cudaEventCreateWithFlags(&diag_ev[q], cudaEventDisableTiming));
   // Default porosity M_0 and a zero state until the caller sets one.
   for (int b = 0; b < 2; b++)
     for (int s = 0; s < nstate; s++) CUDA_TRY(this, cudaMemset(state[b][s], 0, n * es));
@@ -737,6 +749,9 @@ void capaz_ctx::release() {
   if (K) cudaFree(K);
   if (err_flag) cudaFree(err_flag);
   if (diag_out) cudaFree(diag_out);
+  if (diag_host) cudaFreeHost(diag_host);
+  for (int q = 0; q <= CAPAZ_DIAG_SLOTS; q++)
+    if (diag_ev[q]) cudaEventDestroy(diag_ev[q]);
   if (diag_partials) cudaFree(diag_partials);
   if (scratch) cudaFree(scratch);
   if (Pref) cudaFree(Pref);
@@ -999,12 +1014,27 @@ int capaz_ctx::sync() {
 }
 
 int capaz_ctx::read_diag(capaz_diag* out, cudaStream_t s) {
+  const int st = post_diag(CAPAZ_DIAG_SLOTS, s);  // the slot kept for this call
+  return st ? st : wait_diag(CAPAZ_DIAG_SLOTS, out);
+}
+
+int capaz_ctx::post_diag(int slot, cudaStream_t s) {
   CUDA_TRY(this, cudaSetDevice(device));
   if (!(p.flags & CAPAZ_FLAG_DIAGNOSTICS))
     return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "diagnostics need CAPAZ_FLAG_DIAGNOSTICS");
-  double h[DIAG_STRIDE];
-  CUDA_TRY(this, cudaMemcpyAsync(h, diag_out, sizeof h, cudaMemcpyDeviceToHost, s));
-  CUDA_TRY(this, cudaStreamSynchronize(s));
+  CUDA_TRY(this, launch_diag_publish(diag_out, diag_host_dev + DIAG_STRIDE * slot, s));
+  launches++;
+  CUDA_TRY(this, cudaEventRecord(diag_ev[slot], s));
+  diag_posted[slot] = true;
+  return CAPAZ_OK;
+}
+
+int capaz_ctx::wait_diag(int slot, capaz_diag* out) {
+  if (!diag_posted[slot]) return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "no diagnostics posted to this slot");
+  CUDA_TRY(this, cudaSetDevice(device));
+  diag_posted[slot] = false;
+  CUDA_TRY(this, cudaEventSynchronize(diag_ev[slot]));
+  const double* h = diag_host + DIAG_STRIDE * slot;
   memset(out, 0, sizeof *out);
   out->mass[0] = h[0];
   out->mass[1] = h[1];

@@ -28,6 +28,12 @@ struct capaz_ctx {
   double* diag_partials = nullptr;   // per-block diagnostics
   int diag_blocks = 0;
   double* diag_out = nullptr;        // reduced diagnostics (DIAG_STRIDE)
+  // Pinned host ring of diagnostics copies: CAPAZ_DIAG_SLOTS posted slots and
+  // one more for capaz_read_diag; an event marks each slot's copy.
+  double* diag_host = nullptr;      // mapped: diag_host_dev is its device view
+  double* diag_host_dev = nullptr;
+  cudaEvent_t diag_ev[CAPAZ_DIAG_SLOTS + 1] = {};
+  bool diag_posted[CAPAZ_DIAG_SLOTS + 1] = {};
   double* scratch = nullptr;         // one float64 field, derived fields
   void* host_stage = nullptr;
   // Precision form: state stored as FP32 deviations from P_ref(j) and S_ref.
@@ -84,6 +90,8 @@ struct capaz_ctx {
   int get_derived(int field, bool from_current, void* dst, bool on_device, cudaStream_t s);
   int step(int nsteps, cudaStream_t s);
   int read_diag(capaz_diag* out, cudaStream_t s);
+  int post_diag(int slot, cudaStream_t s);
+  int wait_diag(int slot, capaz_diag* out);
   int check_flag();
   // Precision form: FP64 view of (P_w, S_n, m, K) of state buffer b.
   int decode_all(int b, cudaStream_t s);

@@ -210,6 +210,7 @@ cudaError_t launch_step2_fp64(const Step2Const& c, const double* Pw_in, const do
                               bool percell_k, double* diag_partials, unsigned int* err_flag,
                               cudaStream_t s, int* nlaunch);
 cudaError_t launch_diag_finalize(const double* partials, int nblocks, double* out, cudaStream_t s);
+cudaError_t launch_diag_publish(const double* d, double* host_mapped, cudaStream_t s);
 // Derived field `field` of the start-of-step state (Pw, Sn) into out.
 cudaError_t launch_derived2_fp64(const Step2Const& c, int field, const double* Pw, const double* Sn,
                                  const double* m, const double* K, bool percell_k, double* out,

@@ -250,10 +250,12 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
     halo_row = hy;
   }
 
-  double acc_w = 0., acc_n = 0., rmax = 0., nonfinite = 0.;
+  double acc_w = 0., acc_n = 0., nonfinite = 0.;
+  float rmax = 0.f;
   // Diagnostics: masses summed without the cell volume (applied once per
-  // CTA), residuals scaled by 1/rho_0 (one division per thread).
-  const double inv_ro0_w = DIAG ? 1. / f.ro0_w : 0., inv_ro0_n = DIAG ? 1. / f.ro0_n : 0.;
+  // CTA), residuals scaled by 1/rho_0.
+  const float iro0w_f = DIAG ? (float)(1. / f.ro0_w) : 0.f, iro0n_f = DIAG ? (float)(1. / f.ro0_n) : 0.f;
+  const float aw_ro0w_f = DIAG ? (float)(f.aw / f.ro0_w) : 0.f, bn_ro0n_f = DIAG ? (float)(f.bn / f.ro0_n) : 0.f;
   // Everything above overlaps the previous kernel's tail; the work counter and
   // the state are touched only after it has completed.
   grid_dependency_wait();
@@ -362,17 +364,28 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
       const double rw = fma(f.aw, pr, f.ro0_w);
       const double rn = fma(f.bn, pr, f.ro0_n);
       const double J11 = f.aw * (1. - S), J21 = f.bn * S;
-      const double inv = rcp64(fma(J11, rn, rw * J21));  // det = J11 J22 - J12 J21, J12 = -rw, J22 = rn
+      const double det = fma(J11, rn, rw * J21);  // J11 J22 - J12 J21, J12 = -rw, J22 = rn
+      const double inv = rcp64(det);
       // One Newton step from the stored state: the Jacobian solve of the
       // bilinear system, exact up to the dP*dS terms (relative size
-      // |dS| / S ~ 1e-8 of the increments).  Diagnostics evaluate the
-      // residual of the reference's Newton functions at the result.
+      // |dS| / S ~ 1e-8 of the increments).
       const double dP = (rn * Aw + rw * An) * inv;
       const double dS = (J11 * An - J21 * Aw) * inv;
-      double F1 = 0., F2 = 0.;
+      float rf = 0.f;
       if (DIAG) {
-        F1 = fma(f.aw * dP, 1. - S - dS, -rw * dS) - Aw;
-        F2 = fma(f.bn * dP, S + dS, rn * dS) - An;
+        // The reference's Newton functions at (dP, dS),
+        //   F1 = (rw + a_w dP)(1 - S - dS) - rw (1 - S) - Aw,
+        //   F2 = (rn + b_n dP)(S + dS) - rn S - An,
+        // are, for the solve above, exactly F1 = Aw e - a_w dP dS and
+        // F2 = An e + b_n dP dS with e = det * inv - 1 (the linear part
+        // leaves Aw e, An e).  Written so they have no cancellation left;
+        // FP32 holds their size (~1e-14 of Aw) to 1e-7, and they are
+        // reported scaled by 1/rho_0.
+        const float e = (float)fma(det, inv, -1.);
+        const float q = (float)(dP * dS);
+        const float F1 = fmaf(Awf * iro0w_f, e, -aw_ro0w_f * q);
+        const float F2 = fmaf(Anf * iro0n_f, e, bn_ro0n_f * q);
+        rf = fmaxf(fabsf(F1), fabsf(F2));
       }
       const float pn = (float)((double)C0.p + dP);
       const float snew = (float)((double)sc + dS);
@@ -385,13 +398,12 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
       const bool finite = isfinite(pn) && isfinite(snew);
       bad |= active && !finite;
       if (DIAG && active) {
-        const double S1 = S_ref + (double)snew;
+        const double md = (double)mc;
+        const double mS1 = md * (S_ref + (double)snew);  // m S_n; m (1 - S_n) = m - m S_n
         const double P1rel = prel + (double)pn;
-        const double rw1 = fma(f.aw, P1rel, f.ro0_w), rn1 = fma(f.bn, P1rel, f.ro0_n);
-        acc_w += (double)mc * rw1 * (1. - S1);
-        acc_n += (double)mc * rn1 * S1;
-        const double r = fmax(fabs(F1) * inv_ro0_w, fabs(F2) * inv_ro0_n);
-        if (!(r <= rmax)) rmax = r;
+        acc_w = fma(md - mS1, fma(f.aw, P1rel, f.ro0_w), acc_w);
+        acc_n = fma(mS1, fma(f.bn, P1rel, f.ro0_n), acc_n);
+        if (!(rf <= rmax)) rmax = rf;
         if (!finite) nonfinite += 1.;
       }
     };
@@ -474,7 +486,7 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
   if (DIAG) {
     double(*red)[4] = sm.red;
     const int lane = tid & 31, wid = tid >> 5;
-    const double s0 = warp_sum(acc_w), s1 = warp_sum(acc_n), r = warp_max(rmax), nf = warp_sum(nonfinite);
+    const double s0 = warp_sum(acc_w), s1 = warp_sum(acc_n), r = warp_max((double)rmax), nf = warp_sum(nonfinite);
     if (lane == 0) {
       red[wid][0] = s0;
       red[wid][1] = s1;

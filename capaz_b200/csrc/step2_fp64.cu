@@ -358,6 +358,9 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 // Sums the per-block partials in block order (deterministic) into out[5].
 __global__ void diag_finalize_kernel(const double* __restrict__ partials, int nblocks, double* __restrict__ out) {
   __shared__ double red[4][DIAG_STRIDE];
+  // Launched as a programmatic dependent of the step's last kernel: wait for
+  // it (a no-op for an ordinary launch).
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double s[DIAG_STRIDE] = {0, 0, 0, 0, 0};
   // Each thread takes a contiguous range so the order is fixed.
@@ -587,9 +590,37 @@ int step2_fp64_batch_grid(int device) {
   return sms * per;
 }
 
+// One block launched with programmatic stream serialisation: its launch
+// overlaps the tail of the kernel before it, which it waits for on entry.
+template <typename... Params, typename... Args>
+static cudaError_t launch_single_dependent(void (*kernel)(Params...), int threads, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(1);
+  cfg.blockDim = dim3(threads);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 cudaError_t launch_diag_finalize(const double* partials, int nblocks, double* out, cudaStream_t s) {
-  diag_finalize_kernel<<<1, 128, 0, s>>>(partials, nblocks, out);
-  return cudaGetLastError();
+  return launch_single_dependent(diag_finalize_kernel, 128, s, partials, nblocks, out);
+}
+
+// Copies the reduced diagnostics into mapped pinned host memory: the kernel's
+// stores reach the host without a copy-engine transfer, and the event recorded
+// after it tells the host when they have landed.
+__global__ void diag_publish_kernel(const double* __restrict__ d, double* __restrict__ host_mapped) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (threadIdx.x < DIAG_STRIDE) host_mapped[threadIdx.x] = d[threadIdx.x];
+  __threadfence_system();
+}
+
+cudaError_t launch_diag_publish(const double* d, double* host_mapped, cudaStream_t s) {
+  return launch_single_dependent(diag_publish_kernel, 32, s, d, host_mapped);
 }
 
 cudaError_t launch_derived2_fp64(const Step2Const& c, int field, const double* Pw, const double* Sn,

@@ -27,6 +27,7 @@ ERR_UNSUPPORTED = 9
 
 # Largest (ny-2)*max(nz-2,1) that capaz_mass_noalloc accepts.
 NOALLOC_MAX_ROWS = 131072
+DIAG_SLOTS = 4  # CAPAZ_DIAG_SLOTS
 
 MODEL_DEFAULT = 0
 MODEL_BUCKLEY_LEVERETT = 1
@@ -117,6 +118,8 @@ PROTOTYPES = {
     "capaz_get_derived": (C.c_int, [_VP, C.c_int, C.c_int, _VP, C.c_int, _VP]),
     "capaz_step": (C.c_int, [_VP, C.c_int, _VP]),
     "capaz_read_diag": (C.c_int, [_VP, C.POINTER(Diag), _VP]),
+    "capaz_post_diag": (C.c_int, [_VP, C.c_int, _VP]),
+    "capaz_wait_diag": (C.c_int, [_VP, C.c_int, C.POINTER(Diag)]),
     "capaz_set_dt": (C.c_int, [_VP, C.c_double]),
     "capaz_launch_count": (C.c_int64, [_VP]),
     "capaz_batch_create": (_VP, [C.POINTER(Params), C.c_int, C.c_int, C.POINTER(C.c_int)]),

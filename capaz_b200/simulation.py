@@ -146,6 +146,17 @@ class Simulation:
         check(self.lib.capaz_read_diag(self.ctx, C.byref(d), stream or None), self.ctx)
         return {"mass": list(d.mass), "max_residual": d.max_residual, "nonfinite_cells": d.nonfinite_cells}
 
+    def post_diag(self, slot: int, stream: int = 0) -> None:
+        """Queues the copy of the last step's diagnostics into pinned slot
+        `slot` (< native.DIAG_SLOTS) without waiting."""
+        check(self.lib.capaz_post_diag(self.ctx, int(slot), stream or None), self.ctx)
+
+    def wait_diag(self, slot: int) -> dict:
+        """Waits for the copy posted to `slot` and returns it (the form of diag())."""
+        d = Diag()
+        check(self.lib.capaz_wait_diag(self.ctx, int(slot), C.byref(d)), self.ctx)
+        return {"mass": list(d.mass), "max_residual": d.max_residual, "nonfinite_cells": d.nonfinite_cells}
+
     def sync(self) -> None:
         check(self.lib.capaz_sync(self.ctx), self.ctx)
 

@@ -179,7 +179,11 @@ enum capaz_field {
  *                  final iterate, max_p |F_p| / ro0_p (F_p = rho_p(P) S_p -
  *                  roS_p, the reference's Newton functions) — a saturation-
  *                  equivalent, dimensionless residual;
- *   nonfinite_cells = interior cells whose new P or S is NaN/Inf. */
+ *   nonfinite_cells = interior cells whose new P or S is NaN/Inf.
+ * The two-phase precision form's tiled sweep (nx a multiple of 4) takes one
+ * linearised Newton step and evaluates F_p through the exact identities
+ * F_w = A_w e - a_w dP dS, F_n = A_n e + b_n dP dS (e = det * inv - 1 of its
+ * solve), to 1e-7 relative. */
 typedef struct capaz_diag {
   double mass[3];
   double max_residual;
@@ -250,6 +254,16 @@ int capaz_reference_init(const capaz_params* p, double* m, int m_given, double* 
  * device; capaz_read_diag copies them out (synchronising on `stream`). */
 int capaz_step(capaz_ctx* ctx, int nsteps, void* stream);
 int capaz_read_diag(capaz_ctx* ctx, capaz_diag* out, void* stream);
+/* Pipelined diagnostics.  capaz_post_diag enqueues on `stream` the copy of the
+ * last step's diagnostics into slot `slot` (0 <= slot < CAPAZ_DIAG_SLOTS) of a
+ * pinned host ring owned by the context and returns without waiting;
+ * capaz_wait_diag waits for that slot's copy and returns it.  Posting after
+ * step i and waiting for step i - 1 keeps step i queued on the device while
+ * the host reads.  Waiting on a slot with no copy posted since its last wait
+ * is CAPAZ_ERR_INVALID_ARGUMENT. */
+#define CAPAZ_DIAG_SLOTS 4
+int capaz_post_diag(capaz_ctx* ctx, int slot, void* stream);
+int capaz_wait_diag(capaz_ctx* ctx, int slot, capaz_diag* out);
 /* Sets dt for the following steps (a per-step parameter in the reference:
  * consts.dt); host value, no device traffic beyond the kernel argument. */
 int capaz_set_dt(capaz_ctx* ctx, double dt);

@@ -129,3 +129,10 @@ def test_null_arguments_return_errors():
     assert lib.capaz_step(None, 1, None) == native.ERR_INVALID_ARGUMENT
     assert lib.capaz_destroy(None) == native.ERR_INVALID_ARGUMENT
     assert lib.capaz_params_default(None) == native.ERR_INVALID_ARGUMENT
+    assert lib.capaz_post_diag(None, 0, None) == native.ERR_INVALID_ARGUMENT
+    assert lib.capaz_wait_diag(None, 0, None) == native.ERR_INVALID_ARGUMENT
+
+
+def test_diag_slot_count_matches_header():
+    text = open(os.path.join(ROOT, "include", "capaz_b200.h")).read()
+    assert re.search(r"#define CAPAZ_DIAG_SLOTS (\d+)", text).group(1) == str(native.DIAG_SLOTS)

@@ -142,6 +142,52 @@ def test_gpu_diagnostics_match_oracle():
     assert d["nonfinite_cells"] == 0
 
 
+@pytest.mark.parametrize("form", [native.FORM_FP64, native.FORM_FP32C])
+def test_gpu_pipelined_diagnostics_equal_synchronous_reads(form):
+    """post_diag after step i and wait_diag for step i - 1 return, step by
+    step, what read_diag returns right after each step."""
+    p = cfg_params(nx=64, ny=32, nz=19, source=4, S_n_gr=0.1)
+    p.form = form
+    p.flags |= native.FLAG_DIAGNOSTICS
+    state, m = random_case(p, 17)
+    nsteps = 7
+
+    def fresh(s):
+        s.set_field("m", m)
+        for k, v in state.items():
+            s.set_field(k, v)
+
+    with Simulation(p) as s:
+        fresh(s)
+        want = []
+        for _ in range(nsteps):
+            s.step(1)
+            want.append(s.diag())
+    with Simulation(p) as s:
+        fresh(s)
+        got = []
+        for i in range(nsteps):
+            s.step(1)
+            s.post_diag(i % native.DIAG_SLOTS)
+            if i > 0:
+                got.append(s.wait_diag((i - 1) % native.DIAG_SLOTS))
+        got.append(s.wait_diag((nsteps - 1) % native.DIAG_SLOTS))
+        with pytest.raises(native.CapazError) as e:
+            s.wait_diag(0)  # nothing posted since its last wait
+        assert e.value.code == native.ERR_INVALID_ARGUMENT
+    if form == native.FORM_FP64:
+        assert got == want
+    else:
+        # The precision form's sweep hands out tiles from a work counter, so
+        # its per-CTA partial sums (and their FP64 rounding) vary from run
+        # to run; the state itself does not.
+        for a, b in zip(got, want):
+            for i in range(2):
+                assert abs(a["mass"][i] - b["mass"][i]) <= 1e-13 * abs(b["mass"][i])
+            assert a["max_residual"] == b["max_residual"] and a["nonfinite_cells"] == b["nonfinite_cells"]
+    assert len({d["mass"][0] for d in got}) > 1  # the steps differ
+
+
 def test_gpu_nonfinite_state_is_reported():
     """S_n above 1 - S_wr makes S_e < 0 and P_k NaN, as in the reference;
     the step reports CAPAZ_ERR_NONFINITE instead of returning silently."""
