@@ -31,8 +31,10 @@
 namespace capaz {
 namespace {
 
+// The neighbours' derived values (the cell's own S_n comes from global
+// memory): 6 fields, 49 KB for the ring, so that four CTAs fit an SM.
 struct Plane2 {
-  double Pw[PC], Pn[PC], ro_w[PC], ro_n[PC], Xi_w[PC], Xi_n[PC], Sn[PC];
+  double Pw[PC], Pn[PC], ro_w[PC], ro_n[PC], Xi_w[PC], Xi_n[PC];
 };
 constexpr size_t kSmem2 = 3 * sizeof(Plane2);
 
@@ -203,7 +205,6 @@ __device__ __forceinline__ void fp64_tile(const Step2Const& c, const double* __r
         P.ro_n[q] = ro_n;
         P.Xi_w[q] = Xi_w;
         P.Xi_n[q] = Xi_n;
-        P.Sn[q] = Sn;
       }
     }
   };
@@ -219,7 +220,7 @@ __device__ __forceinline__ void fp64_tile(const Step2Const& c, const double* __r
       const Plane2& C = ring[k % 3];
       const long long l = i + j * c.sy + (long long)k * c.sz;
       const double mc = m[l];
-      const double Pw = C.Pw[cidx], Pn = C.Pn[cidx], Sn = C.Sn[cidx];
+      const double Pw = C.Pw[cidx], Pn = C.Pn[cidx], Sn = Sn_in[l];
       const double rw = C.ro_w[cidx], rn = C.ro_n[cidx];
       const double q_w = 0., q_n = 0.;  // wells_q (two-phase.cpp:187-192)
       const double roS_w = rw * (1. - Sn);
@@ -313,7 +314,7 @@ __device__ __forceinline__ void fp64_tile(const Step2Const& c, const double* __r
 }
 
 template <bool UNIK, bool PD0, bool PLANAR, bool DIAG>
-__global__ void __launch_bounds__(NTHREADS, 2)
+__global__ void __launch_bounds__(NTHREADS, 4)
     step2_fp64_kernel(const Step2Const c, const double* __restrict__ Pw_in, const double* __restrict__ Sn_in,
                       double* __restrict__ Pw_out, double* __restrict__ Sn_out, const double* __restrict__ m,
                       const double* __restrict__ K, double* __restrict__ diag_partials,
@@ -330,7 +331,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 // size share one launch.  All instances have the same flags (K per cell,
 // P_d == 0); planar and 3-D instances may be mixed.
 template <bool UNIK, bool PD0>
-__global__ void __launch_bounds__(NTHREADS, 2)
+__global__ void __launch_bounds__(NTHREADS, 4)
     step2_fp64_batch_kernel(const Inst64* __restrict__ insts, const int4* __restrict__ items, int nitems, int parity,
                             unsigned int* __restrict__ counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
