@@ -83,8 +83,10 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
+// Three CTAs per SM (3 x 73 KB of plane ring, 85 registers): the FP64
+// pipeline needs the resident warps more than the registers.
 template <bool UNIK, bool PLANAR, bool DIAG>
-__global__ void __launch_bounds__(NTHREADS, 1)
+__global__ void __launch_bounds__(NTHREADS, 3)
     step3_fp64_kernel(const Step3Const c, Step3Buffers in, Step3Buffers out, const double* __restrict__ m,
                       const double* __restrict__ K, double* __restrict__ diag_partials,
                       unsigned int* __restrict__ err_flag) {
