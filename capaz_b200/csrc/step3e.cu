@@ -256,8 +256,11 @@ __global__ void energy_balance_kernel(const Step3Const c, EnergyState st, const 
 // 4: P_S_calculation, the 5x5 Newton of energy.cpp:348-462 on one interior
 // cell in place.  reverse_matrix leaves dF as it is when it finds no pivot,
 // and the reference uses dF all the same.
-__global__ void energy_newton_kernel(const Step3Const c, EnergyState st, const double* __restrict__ m,
-                                     double* __restrict__ w, unsigned int* __restrict__ err) {
+// Two CTAs of 256 threads per SM (128 registers, some spills to L1): twice
+// the resident warps of the unbounded build pay for the spills.
+__global__ void __launch_bounds__(256, 2)
+    energy_newton_kernel(const Step3Const c, EnergyState st, const double* __restrict__ m, double* __restrict__ w,
+                         unsigned int* __restrict__ err) {
   const long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (l >= c.ncell) return;
   const Cell q = cell_of(c, l);
