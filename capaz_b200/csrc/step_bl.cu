@@ -127,7 +127,8 @@ __device__ __forceinline__ void bl_fluxes(const BLConst& b, const double* Pw, co
   }
 }
 
-__global__ void step_bl_interior_kernel(const BLConst b, const double* __restrict__ Pw, const double* __restrict__ Sn,
+// Four CTAs of 256 threads per SM (64 registers).
+__global__ void __launch_bounds__(256, 4) step_bl_interior_kernel(const BLConst b, const double* __restrict__ Pw, const double* __restrict__ Sn,
                                         double* __restrict__ Pw_out, double* __restrict__ Sn_out,
                                         const double* __restrict__ m, const double* __restrict__ K, bool percell,
                                         unsigned int* __restrict__ err) {
