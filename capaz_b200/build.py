@@ -48,7 +48,7 @@ CUDA_SOURCES = [
     ("media.cu", []),
     ("slab.cu", []),
 ]
-HEADERS = ["capaz_internal.h", "capaz_ctx.h", "phys3.cuh"]
+HEADERS = ["capaz_internal.h", "capaz_ctx.h", "phys3.cuh", "diag_reduce.cuh"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -176,9 +176,12 @@ constexpr int TMA_TILE_Y = 2 * TMA_TY;
 // Launches the sweep over the interior cells and then the boundary kernel
 // (bitems: (instance, first boundary cell) blocks of BOUND_BLOCK cells).
 constexpr int BOUND_BLOCK = 256;
+// With diag_partials, the sweep writes per-CTA diagnostics partials (grid
+// of them) and the boundary kernel reduces them into diag_out.
 cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems,
                                    const int2* bitems, int nbitems, int parity, bool unik, bool planar,
-                                   unsigned int* counter, double* diag_partials, int grid, cudaStream_t s);
+                                   unsigned int* counter, double* diag_partials, int grid, cudaStream_t s,
+                                   double* diag_out = nullptr);
 // Boundary cells of an nx x ny x nz grid (faces, edges, corners; nz == 1: the
 // four sides of the plane).
 inline int boundary_cells(int nx, int ny, int nz) {

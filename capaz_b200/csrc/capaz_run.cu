@@ -81,17 +81,14 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
     }
     for (int t = 0; t < nsteps; t++) {
       const bool last = t == nsteps - 1;
+      // With diagnostics, the last step's boundary kernel also reduces the
+      // sweep's partials into diag_out.
       e = launch_step2_fp32c_tma(f, tma_inst, tma_items, tma_nitems, tma_bitems, tma_nbitems, cur, unik, p.nz == 1,
-                                 tma_counter, (diag && last) ? diag_partials : nullptr, tma_grid, s);
+                                 tma_counter, (diag && last) ? diag_partials : nullptr, tma_grid, s, diag_out);
       launches += 2;
       if (e != cudaSuccess) return fail_cuda(e, "step2_fp32c_tma launch");
       cur ^= 1;
       steps_done++;
-    }
-    if (diag) {
-      e = launch_diag_finalize(diag_partials, tma_grid, diag_out, s);
-      launches++;
-      if (e != cudaSuccess) return fail_cuda(e, "diag finalize launch");
     }
     return CAPAZ_OK;
   }

@@ -43,6 +43,7 @@
 #include <utility>
 
 #include "capaz_internal.h"
+#include "diag_reduce.cuh"
 
 namespace capaz {
 namespace {
@@ -519,14 +520,21 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
 // (rho_n S_n + rho_w (1 - S_n)) m g hy of the basic cell with its new S_n and
 // start-of-step densities (Border_P, main.cpp:255-267).  One thread per
 // boundary cell; items are (instance, first cell) blocks of BOUND_BLOCK.
-__global__ void __launch_bounds__(BOUND_BLOCK) boundary_fp32c_kernel(const __grid_constant__ PhysF f,
-                                                                     const InstT* __restrict__ insts,
-                                                                     const int2* __restrict__ bitems, int parity,
-                                                                     unsigned int* __restrict__ counter) {
+// With diagnostics, block 0 also reduces the sweep's per-CTA partials into
+// diag_out (they are complete once the sweep is), so the step needs no
+// separate reduction launch.
+__global__ void __launch_bounds__(BOUND_BLOCK)
+    boundary_fp32c_kernel(const __grid_constant__ PhysF f, const InstT* __restrict__ insts,
+                          const int2* __restrict__ bitems, int parity, unsigned int* __restrict__ counter,
+                          const double* __restrict__ diag_partials, int nparts, double* __restrict__ diag_out) {
   grid_dependency_wait();  // the sweep's interior values and its use of the counter
   // The sweep before this launch has taken all its work items: rearm its
   // work counter for the next step.
   if (blockIdx.x == 0 && threadIdx.x == 0) *counter = 0u;
+  if (diag_out != nullptr && blockIdx.x == 0) {
+    __shared__ double red[BOUND_BLOCK / 32][DIAG_STRIDE];
+    diag_reduce_block<BOUND_BLOCK / 32>(diag_partials, nparts, diag_out, red);
+  }
   const int2 it = bitems[blockIdx.x];
   const InstT* __restrict__ I = insts + it.x;
   const int q0 = it.y + (int)threadIdx.x;
@@ -652,7 +660,8 @@ cudaError_t launch_p(bool planar, const PhysF& f, const InstT* insts, const int4
 
 cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems,
                                    const int2* bitems, int nbitems, int parity, bool unik, bool planar,
-                                   unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
+                                   unsigned int* counter, double* diag_partials, int grid, cudaStream_t s,
+                                   double* diag_out) {
   // `counter` is zero on entry: zeroed at allocation and rearmed by every
   // boundary launch.
   cudaError_t e;
@@ -664,7 +673,7 @@ cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int
                       : launch_p<false, false>(planar, f, insts, items, nitems, parity, counter, nullptr, grid, s);
   if (e != cudaSuccess) return e;
   return launch_dependent(boundary_fp32c_kernel, dim3(nbitems), dim3(BOUND_BLOCK), 0, s, f, insts, bitems, parity,
-                          counter);
+                          counter, (const double*)diag_partials, grid, diag_partials ? diag_out : nullptr);
 }
 
 int step2_fp32c_tma_grid(int device, bool unik) {

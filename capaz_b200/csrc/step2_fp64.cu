@@ -27,6 +27,7 @@
 #include <math.h>
 
 #include "capaz_internal.h"
+#include "diag_reduce.cuh"
 
 namespace capaz {
 namespace {
@@ -362,46 +363,7 @@ __global__ void diag_finalize_kernel(const double* __restrict__ partials, int nb
   // Launched as a programmatic dependent of the step's last kernel: wait for
   // it (a no-op for an ordinary launch).
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double s[DIAG_STRIDE] = {0, 0, 0, 0, 0};
-  // Each thread takes a contiguous range so the order is fixed.
-  const int per = (nblocks + blockDim.x - 1) / blockDim.x;
-  const int b0 = threadIdx.x * per, b1 = min(nblocks, b0 + per);
-  for (int b = b0; b < b1; b++) {
-    const double* p = partials + (size_t)DIAG_STRIDE * b;
-    s[0] += p[0];
-    s[1] += p[1];
-    s[2] += p[2];
-    s[3] = fmax(s[3], p[3]);
-    s[4] += p[4];
-  }
-  // Ordered tree over the lanes of each warp, then over warps.
-  for (int o = 1; o < 32; o <<= 1) {
-    double t0 = __shfl_down_sync(0xffffffffu, s[0], o), t1 = __shfl_down_sync(0xffffffffu, s[1], o);
-    double t2 = __shfl_down_sync(0xffffffffu, s[2], o), t3 = __shfl_down_sync(0xffffffffu, s[3], o);
-    double t4 = __shfl_down_sync(0xffffffffu, s[4], o);
-    if ((lane & (2 * o - 1)) == 0) {
-      s[0] += t0;
-      s[1] += t1;
-      s[2] += t2;
-      s[3] = fmax(s[3], t3);
-      s[4] += t4;
-    }
-  }
-  if (lane == 0)
-    for (int q = 0; q < DIAG_STRIDE; q++) red[wid][q] = s[q];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double r[DIAG_STRIDE] = {0, 0, 0, 0, 0};
-    for (int w = 0; w < (int)(blockDim.x / 32); w++) {
-      r[0] += red[w][0];
-      r[1] += red[w][1];
-      r[2] += red[w][2];
-      r[3] = fmax(r[3], red[w][3]);
-      r[4] += red[w][4];
-    }
-    for (int q = 0; q < DIAG_STRIDE; q++) out[q] = r[q];
-  }
+  diag_reduce_block<4>(partials, nblocks, out, red);  // 128 threads
 }
 
 template <bool UNIK, bool PD0, bool PLANAR, bool DIAG>
