@@ -202,7 +202,8 @@ __global__ void adj_phase1_kernel(const AdjConst c, const double* __restrict__ l
 // Phase 2: adjoint of the start-of-step state of every cell and the
 // gradient increments.  Abar is read only at interior cells.
 template <bool PD0>
-__global__ void __launch_bounds__(256) adj_phase2_kernel(
+// Three CTAs per SM (85 registers, some spills): 6 % faster than two.
+__global__ void __launch_bounds__(256, 3) adj_phase2_kernel(
     const AdjConst c, const double* __restrict__ P, const double* __restrict__ S, const double* __restrict__ K,
     const double* __restrict__ m, const double* __restrict__ Mw, const double* __restrict__ Mn,
     const double* __restrict__ PnArr, const double* __restrict__ Aw, const double* __restrict__ An,
