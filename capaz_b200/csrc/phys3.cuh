@@ -96,5 +96,59 @@ __device__ __forceinline__ bool reverse_matrix(double* a) {
   return true;
 }
 
+// x = a^-1 F by Gauss-Jordan on [a | F] with reverse_matrix's pivot rule
+// (another pivot row only when |pivot| < 1e-8: the last row below with entry
+// > 1e-8) and the pivot row scaled by the pivot's reciprocal.  The left block
+// goes through exactly the operations reverse_matrix applies to it, so the
+// pivot decisions are the same; the right-hand side replaces the identity
+// block, which saves the product with the inverse (the result differs from
+// inverse-times-F by rounding only).  Returns false, leaving x unset, where
+// reverse_matrix finds no pivot.
+template <int N>
+__device__ __forceinline__ bool solve_gj(const double* a, const double* F, double* x) {
+  const double e = 1E-8;
+  double matr[N][N + 1];
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+#pragma unroll
+    for (int j = 0; j < N; j++) matr[i][j] = a[j + N * i];
+    matr[i][N] = F[i];
+  }
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    double f = matr[k][k];
+    if (fabs(f) < e) {
+      int det_flag = 0;
+#pragma unroll
+      for (int i = k + 1; i < N; i++) {
+        if (matr[i][k] > e) {
+          det_flag = 1;
+#pragma unroll
+          for (int j = 0; j <= N; j++) {
+            double row = matr[k][j];
+            matr[k][j] = matr[i][j];
+            matr[i][j] = row;
+          }
+          f = matr[k][k];
+        }
+      }
+      if (det_flag == 0) return false;
+    }
+    const double r = 1. / f;
+#pragma unroll
+    for (int j = 0; j <= N; j++) matr[k][j] *= r;
+#pragma unroll
+    for (int i = 0; i < N; i++)
+      if (i != k) {
+        double f1 = matr[i][k];
+#pragma unroll
+        for (int j = 0; j <= N; j++) matr[i][j] -= (matr[k][j] * f1);
+      }
+  }
+#pragma unroll
+  for (int i = 0; i < N; i++) x[i] = matr[i][N];
+  return true;
+}
+
 }  // namespace phys3
 }  // namespace capaz

@@ -311,13 +311,17 @@ __global__ void __launch_bounds__(256, 2)
     dF[4 + N * 4] = ml * (Sw * (dwT * Hw + ro_w(c, P, T) * c_w(T)) + Sn * (dnT * Hn + ro_n(c, P, T) * c_n(T)) +
                           Sg * (dgT * Hg + ro_g(c, P, T) * c_g(T))) +
                     (1. - ml) * ro_r * c_r(T);
-    phys3::reverse_matrix<N, true>(dF);
+    // corr = dF^-1 F (energy.cpp inverts dF with reverse_matrix and
+    // multiplies); where no pivot is found the reference multiplies by dF
+    // itself, which reverse_matrix left unchanged.
     double corr[N];
+    if (!phys3::solve_gj<N>(dF, F, corr)) {
 #pragma unroll
-    for (int a = 0; a < N; a++) {
-      corr[a] = 0;
+      for (int a = 0; a < N; a++) {
+        corr[a] = 0;
 #pragma unroll
-      for (int b = 0; b < N; b++) corr[a] += dF[b + N * a] * F[b];
+        for (int b = 0; b < N; b++) corr[a] += dF[b + N * a] * F[b];
+      }
     }
     Sw = Sw - corr[0];
     Sn = Sn - corr[1];
