@@ -168,6 +168,89 @@ __global__ void __launch_bounds__(256, 4) step_bl_interior_kernel(const BLConst 
   if (!(isfinite(P) && isfinite(S))) atomicOr(err, 1u);
 }
 
+// The same interior update with the x and y neighbours' derived values
+// staged in shared memory: a CTA takes a TX x TY tile of one z-plane, every
+// window cell (halo included) is derived once, and the stencil reads the
+// window; z neighbours (3-D grids) are derived in place as above.  The values
+// and the operation order are those of step_bl_interior_kernel.
+__global__ void __launch_bounds__(NTHREADS, 4)
+    step_bl_tile_kernel(const BLConst b, const double* __restrict__ Pw, const double* __restrict__ Sn,
+                        double* __restrict__ Pw_out, double* __restrict__ Sn_out, const double* __restrict__ m,
+                        const double* __restrict__ K, bool percell, unsigned int* __restrict__ err) {
+  __shared__ double sP[PC], srw[PC], srn[PC], sXw[PC], sXn[PC];
+  const Step2Const& c = b.c;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
+  const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
+  const int k = c.nz < 2 ? 0 : 1 + (int)blockIdx.z;
+  const long long kz = (long long)k * c.sz;
+  for (int q = tid; q < PC; q += NTHREADS) {
+    const int gi = i0 - 1 + q % PX, gj = j0 - 1 + q / PX;
+    if (gi < c.nx && gj < c.ny) {
+      const long long lq = gi + gj * c.sy + kz;
+      sP[q] = Pw[lq];
+      bl_derive_at(b, Pw, Sn, K, percell, lq, srw[q], srn[q], sXw[q], sXn[q]);
+    }
+  }
+  __syncthreads();
+  const int i = i0 + tx, j = j0 + ty;
+  if (i > c.nx - 2 || j > c.ny - 2) return;
+  const int q = (ty + 1) * PX + (tx + 1);
+  const long long l = i + j * c.sy + kz;
+  const double mc = m[l];  // > 0 on every cell (checked when m is set)
+  double P = sP[q], S = Sn[l];
+  const double rw = srw[q], rn = srn[q], Xw = sXw[q], Xn = sXn[q];
+  double q_w, q_n;
+  bl_wells(b, i, j, S, q_w, q_n);
+  const double roS_w = rw * (1. - S), roS_n = rn * S;
+  double f_w[3], f_n[3];
+  for (int axis = 0; axis < 3; axis++) {
+    f_w[axis] = 0.;
+    f_n[axis] = 0.;
+    if (axis == 2 && c.nz < 2) continue;
+    const double h = axis == 0 ? c.hx : axis == 1 ? c.hy : c.hz;
+    double rmw, rmn, Xmw, Xmn, rpw, rpn, Xpw, Xpn, Pm, Pp;
+    if (axis < 2) {
+      const int a = axis == 0 ? q - 1 : q - PX, bq = axis == 0 ? q + 1 : q + PX;
+      rmw = srw[a], rmn = srn[a], Xmw = sXw[a], Xmn = sXn[a], Pm = sP[a];
+      rpw = srw[bq], rpn = srn[bq], Xpw = sXw[bq], Xpn = sXn[bq], Pp = sP[bq];
+    } else {
+      bl_derive_at(b, Pw, Sn, K, percell, l - c.sz, rmw, rmn, Xmw, Xmn);
+      bl_derive_at(b, Pw, Sn, K, percell, l + c.sz, rpw, rpn, Xpw, Xpn);
+      Pm = Pw[l - c.sz];
+      Pp = Pw[l + c.sz];
+    }
+    const double Pc = P;
+    double x2 = -1. * ((Pp - Pc) / h), x1 = -1. * ((Pc - Pm) / h);
+    double x2w = x2, x1w = x1, x2n = x2, x1n = x1;
+    if (axis == 1) {
+      x2w = x2 + c.g * (rw);
+      x1w = x1 + c.g * (rw);
+      x2n = x2 + c.g * (rn);
+      x1n = x1 + c.g * (rn);
+    }
+    f_w[axis] = bl_directed(x1w, x2w, Xw, rw, Xmw, rmw, Xpw, rpw, h);
+    f_n[axis] = bl_directed(x1n, x2n, Xn, rn, Xmn, rmn, Xpn, rpn, h);
+  }
+  const double A1 = roS_w - (c.dt / mc) * (-q_w + f_w[0] + f_w[1] + f_w[2]);
+  const double A2 = roS_n - (c.dt / mc) * (-q_n + f_n[0] + f_n[1] + f_n[2]);
+  for (int w = 1; w <= c.iters; w++) {
+    const double F1 = c.ro0_w * (1. + (c.beta_w) * (P - c.P_atm)) * (1. - S) - A1;
+    const double F2 = c.ro0_n * (1. + (c.beta_n) * (P - c.P_atm)) * S - A2;
+    const double F1P = c.ro0_w * (c.beta_w) * (1 - S);
+    const double F2P = c.ro0_n * (c.beta_n) * S;
+    const double F1S = (-1) * (c.ro0_w) * (1 + (c.beta_w) * (P - c.P_atm));
+    const double F2S = c.ro0_n * (1 + (c.beta_n) * (P - c.P_atm));
+    const double det = F1P * F2S - F1S * F2P;
+    const double nP = P - (1. / det) * (F2S * F1 - F1S * F2);
+    const double nS = S - (1. / det) * (F1P * F2 - F2P * F1);
+    P = nP;
+    S = nS;
+  }
+  Pw_out[l] = P;
+  Sn_out[l] = S;
+  if (!(isfinite(P) && isfinite(S))) atomicOr(err, 1u);
+}
+
 // Border_S and Border_P (b-l.cpp:104-171) on every cell, then the wells'
 // pressures.  Interior cells are their own basic coordinate, so only the
 // interior well cells change there; every boundary cell whose basic
@@ -278,7 +361,13 @@ unsigned bl_blocks(long long n) { return (unsigned)((n + 255) / 256); }
 cudaError_t launch_step_bl(const BLConst& b, const double* Pw_in, const double* Sn_in, double* Pw_out, double* Sn_out,
                            const double* m, const double* K, bool percell_k, unsigned int* err, cudaStream_t s) {
   const unsigned nb = bl_blocks(b.c.ncell);
-  step_bl_interior_kernel<<<nb, 256, 0, s>>>(b, Pw_in, Sn_in, Pw_out, Sn_out, m, K, percell_k, err);
+  const Step2Const& c = b.c;
+  const dim3 tiles((unsigned)((c.nx - 2 + TX - 1) / TX), (unsigned)((c.ny - 2 + TY - 1) / TY),
+                   (unsigned)(c.nz < 2 ? 1 : c.nz - 2));
+  if (tiles.y <= 65535u && tiles.z <= 65535u)
+    step_bl_tile_kernel<<<tiles, dim3(TX, TY), 0, s>>>(b, Pw_in, Sn_in, Pw_out, Sn_out, m, K, percell_k, err);
+  else  // beyond the grid's y/z block limits: one thread per cell
+    step_bl_interior_kernel<<<nb, 256, 0, s>>>(b, Pw_in, Sn_in, Pw_out, Sn_out, m, K, percell_k, err);
   step_bl_boundary_kernel<<<nb, 256, 0, s>>>(b, Pw_out, Sn_out, m);
   return cudaGetLastError();
 }
