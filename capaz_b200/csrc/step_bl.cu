@@ -166,6 +166,9 @@ __global__ void __launch_bounds__(256, 4) step_bl_interior_kernel(const BLConst 
   Pw_out[l] = P;
   Sn_out[l] = S;
   if (!(isfinite(P) && isfinite(S))) atomicOr(err, 1u);
+  // The wells hold their pressures (b-l.cpp:165-170) on interior cells too.
+  if (bl_injection(i, j)) Pw_out[l] = b.injwell_Pw;
+  if (bl_output(c, i, j)) Pw_out[l] = b.outwell_Pw;
 }
 
 // The same interior update with the x and y neighbours' derived values
@@ -249,25 +252,57 @@ __global__ void __launch_bounds__(NTHREADS, 4)
   Pw_out[l] = P;
   Sn_out[l] = S;
   if (!(isfinite(P) && isfinite(S))) atomicOr(err, 1u);
+  if (bl_injection(i, j)) Pw_out[l] = b.injwell_Pw;
+  if (bl_output(c, i, j)) Pw_out[l] = b.outwell_Pw;
 }
 
-// Border_S and Border_P (b-l.cpp:104-171) on every cell, then the wells'
-// pressures.  Interior cells are their own basic coordinate, so only the
-// interior well cells change there; every boundary cell whose basic
-// coordinate is an interior well cell is itself a well cell, so no thread
-// reads a value another thread of this launch writes.
+// Border_S and Border_P (b-l.cpp:104-171), then the wells' pressures, on the
+// boundary cells: one thread per cell q of the grid's shell (faces, then
+// edges and corners, as boundary_cells counts them).  Interior cells are
+// their own basic coordinate; the interior update has already given the
+// interior well cells their wells' pressures.  Every boundary cell whose
+// basic coordinate is an interior well cell is itself a well cell, so no
+// thread reads a value another thread of this launch writes, and none reads
+// a well pressure it keeps.
 __global__ void step_bl_boundary_kernel(const BLConst b, double* __restrict__ Pw_out, double* __restrict__ Sn_out,
-                                        const double* __restrict__ m) {
+                                        const double* __restrict__ m, int nbound) {
   const Step2Const& c = b.c;
-  const long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (l >= c.ncell) return;
-  const int i = (int)(l % c.nx), j = (int)((l / c.nx) % c.ny), k = (int)(l / c.sz);
-  const bool inj = bl_injection(i, j), out = bl_output(c, i, j);
-  if (bl_interior(c, i, j, k)) {
-    if (inj) Pw_out[l] = b.injwell_Pw;
-    if (out) Pw_out[l] = b.outwell_Pw;
-    return;
+  int q = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (q >= nbound) return;
+  const int nx = c.nx, ny = c.ny, nz = c.nz;
+  int i, j, k;
+  if (nz == 1) {
+    k = 0;
+    if (q < 2 * nx) {
+      j = q < nx ? 0 : ny - 1;
+      i = q % nx;
+    } else {
+      q -= 2 * nx;
+      i = q < ny - 2 ? 0 : nx - 1;
+      j = 1 + q % (ny - 2);
+    }
+  } else {
+    const int A = nx * nz, B = (ny - 2) * nz, C = (nx - 2) * (ny - 2);
+    if (q < 2 * A) {
+      j = q < A ? 0 : ny - 1;
+      q %= A;
+      i = q % nx;
+      k = q / nx;
+    } else if ((q -= 2 * A) < 2 * B) {
+      i = q < B ? 0 : nx - 1;
+      q %= B;
+      j = 1 + q % (ny - 2);
+      k = q / (ny - 2);
+    } else {
+      q -= 2 * B;
+      k = q < C ? 0 : nz - 1;
+      q %= C;
+      i = 1 + q % (nx - 2);
+      j = 1 + q / (nx - 2);
+    }
   }
+  const long long l = i + j * c.sy + (long long)k * c.sz;
+  const bool inj = bl_injection(i, j), out = bl_output(c, i, j);
   int i1 = i, j1 = j, k1 = k;
   if ((i == 0) && (c.nx > 2)) i1++;
   if ((i == c.nx - 1) && (c.nx > 2)) i1--;
@@ -368,7 +403,8 @@ cudaError_t launch_step_bl(const BLConst& b, const double* Pw_in, const double* 
     step_bl_tile_kernel<<<tiles, dim3(TX, TY), 0, s>>>(b, Pw_in, Sn_in, Pw_out, Sn_out, m, K, percell_k, err);
   else  // beyond the grid's y/z block limits: one thread per cell
     step_bl_interior_kernel<<<nb, 256, 0, s>>>(b, Pw_in, Sn_in, Pw_out, Sn_out, m, K, percell_k, err);
-  step_bl_boundary_kernel<<<nb, 256, 0, s>>>(b, Pw_out, Sn_out, m);
+  const int nbound = boundary_cells(c.nx, c.ny, c.nz);
+  step_bl_boundary_kernel<<<(unsigned)((nbound + 255) / 256), 256, 0, s>>>(b, Pw_out, Sn_out, m, nbound);
   return cudaGetLastError();
 }
 
