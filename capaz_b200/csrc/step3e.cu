@@ -87,8 +87,10 @@ __device__ __forceinline__ Cell cell_of(const Step3Const& c, long long l) {
 
 // 1: S_calculation, ro_P_Xi_calculation, H_E_current_calculation and the
 // effective conductivity (energy.cpp:54-81) of every cell.
-__global__ void energy_derive_kernel(const Step3Const c, EnergyState st, const double* __restrict__ m,
-                                     const double* __restrict__ K, double* __restrict__ w) {
+// Four CTAs of 256 threads per SM (64 registers).
+__global__ void __launch_bounds__(256, 4)
+    energy_derive_kernel(const Step3Const c, EnergyState st, const double* __restrict__ m,
+                         const double* __restrict__ K, double* __restrict__ w) {
   const long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (l >= c.ncell) return;
   const Cell q = cell_of(c, l);
@@ -172,8 +174,10 @@ __global__ void energy_velocity_kernel(const Step3Const c, EnergyState st, doubl
 
 // 3: roS_calculation (NR form, cpu.cpp:619-731, rates zero) and
 // E_calculation on interior cells.
-__global__ void energy_balance_kernel(const Step3Const c, EnergyState st, const double* __restrict__ m,
-                                      double* __restrict__ w) {
+// Three CTAs of 256 threads per SM (85 registers).
+__global__ void __launch_bounds__(256, 3)
+    energy_balance_kernel(const Step3Const c, EnergyState st, const double* __restrict__ m,
+                          double* __restrict__ w) {
   const long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (l >= c.ncell) return;
   const Cell q = cell_of(c, l);
@@ -256,9 +260,9 @@ __global__ void energy_balance_kernel(const Step3Const c, EnergyState st, const 
 // 4: P_S_calculation, the 5x5 Newton of energy.cpp:348-462 on one interior
 // cell in place.  reverse_matrix leaves dF as it is when it finds no pivot,
 // and the reference uses dF all the same.
-// Two CTAs of 256 threads per SM (128 registers, some spills to L1): twice
-// the resident warps of the unbounded build pay for the spills.
-__global__ void __launch_bounds__(256, 2)
+// Three CTAs of 256 threads per SM (85 registers, some spills to L1): the
+// resident warps pay for the spills.
+__global__ void __launch_bounds__(256, 3)
     energy_newton_kernel(const Step3Const c, EnergyState st, const double* __restrict__ m, double* __restrict__ w,
                          unsigned int* __restrict__ err) {
   const long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x;
