@@ -260,11 +260,13 @@ def run_reference(args) -> None:
 
 
 # ---------------------------------------------------------------------------
-def time_form(sim, K, W, stream, ws, local, clocks=None):
+def time_form(sim, K, W, stream, ws, local, clocks=None, repeats=0):
     """W untimed steps, then exactly K steps between two CUDA events on the
     launching stream; barrier + synchronize on both sides.  A step is the
     form's kernels for one time step (the precision form: the sweep and its
-    boundary kernel), so the per-step time is also the kernels' time."""
+    boundary kernel), so the per-step time is also the kernels' time.  With
+    `repeats`, that many more blocks of K steps are timed the same way
+    afterwards (reported beside the measurement, with their median)."""
     import torch
     sh = stream.cuda_stream
     with torch.cuda.stream(stream):
@@ -285,8 +287,18 @@ def time_form(sim, K, W, stream, ws, local, clocks=None):
         barrier(ws, local)
         launches = sim.launch_count - l0
         total_ms = start.elapsed_time(end)
+        reps = []
+        for _ in range(repeats):
+            barrier(ws, local)
+            torch.cuda.synchronize()
+            start.record(stream)
+            sim.step(K, stream=sh)
+            end.record(stream)
+            torch.cuda.synchronize()
+            reps.append(reduce_max(start.elapsed_time(end), ws) / K)
     sim.sync()
-    return {"total_ms": reduce_max(total_ms, ws), "kern_ms": total_ms / K, "launches": launches}
+    return {"total_ms": reduce_max(total_ms, ws), "kern_ms": total_ms / K, "launches": launches,
+            "repeat_ms_per_step": reps}
 
 
 def tma_applies(p) -> bool:
@@ -724,7 +736,7 @@ def run_capaz(args) -> None:
             clocks = Clocks(dev)
             clocks.start()
             time.sleep(0.3)
-        timing[f] = time_form(sim, K, W, stream, ws, local, clocks)
+        timing[f] = time_form(sim, K, W, stream, ws, local, clocks, repeats=5 if f == head else 0)
         if clocks:
             clk = clocks.stop()
         sim.close()
@@ -869,6 +881,11 @@ def run_capaz(args) -> None:
                        "parallelism": f"replicas x{ws}",
                        "l2": "inputs larger than L2: each step reads P_w, S_n, m, K and writes P_w, S_n "
                              f"({ALGO_BYTES[(head, percell)] * ncell / 1e6:.0f} MB of the {126} MB L2)"},
+            "repeats": {"count": len(t["repeat_ms_per_step"]), "steps_each": K,
+                        "ms_per_step": t["repeat_ms_per_step"],
+                        "median_ms_per_step": (statistics.median(t["repeat_ms_per_step"])
+                                               if t["repeat_ms_per_step"] else None),
+                        "note": "further blocks of K steps timed the same way after the measurement"},
             "forms": forms_out,
             "speedup_fp32c_vs_fp64": (forms_out["fp32c"]["value"] / forms_out["fp64"]["value"]
                                       if "fp32c" in forms_out and "fp64" in forms_out else None),
