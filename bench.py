@@ -444,7 +444,7 @@ def bl_leg(dev, steps: int = 200, warmup: int = 5) -> dict:
     out = {"workload": "Buckley-Leverett 1000x1000x1, dt 2000 s, lognormal K, reference wells and fluids, FP64",
            "value": p.ncell / (ms * 1e-3), "unit": "cell-steps/s", "ms_per_step": ms, "steps": steps,
            "launches": launches, "finite": bool(np.isfinite(S).all()),
-           "kernel": "step_bl_interior_kernel + step_bl_boundary_kernel"}
+           "kernel": "step_bl_tile_kernel + step_bl_boundary_kernel"}
     try:
         from oracle import oracle as O
         q = buckley_leverett_params(nx=200, ny=200, nz=1, dt=2000.0)
