@@ -209,51 +209,104 @@ def cpu_baseline_port(w, nsteps: int = 2) -> dict:
                       f"reference CPU step), {dt:.1f} s"}
 
 
-def reference_sample_grid(total_steps: int, budget_s: float = 90.0, rate: float = 6.0e5):
-    """A slab of the workload grid small enough that total_steps reference
-    steps take about budget_s on one core."""
-    cells = max(3 * 16 * 16, min(256 * 128 * 8, int(rate * budget_s / max(total_steps, 1))))
-    nx = 64 if cells >= 64 * 16 * 3 else 16
-    ny = min(128, max(3, int(round(cells / (nx * 16)))))
-    nz = max(3, int(round(cells / (nx * ny))))
-    return nx, ny, nz
+def workload_config(grid, ws: int) -> dict:
+    """The `config` object both arms print for the two-phase workload: the
+    grid and what one step is.  What differs between the arms (the storage
+    form, the media fields, dt) is reported beside it, not in it."""
+    Nx, Ny, Nz = grid
+    cells = Nx * Ny * Nz
+    return {"workload": f"two-phase time step, {Nx}x{Ny}x{Nz} grid with gravity on z ({cells} cells); "
+                        "one step = one time step of the whole grid",
+            "grid_ref": [Nx, Nz, Ny], "cells": cells, "parallelism": f"replicas x{ws}",
+            "l2": ("inputs larger than L2" if 24 * cells > 126e6 else "inputs smaller than L2 (not a roofline size)")
+                  + f": every step reads and writes the whole state ({24 * cells / 1e6:.0f} MB in the "
+                    f"FP32-storage form, {48 * cells / 1e6:.0f} MB in FP64; the GPU's L2 is 126 MB)"}
+
+
+# The reference's CPU build, run as a subprocess: the harness that the oracle
+# recipe (oracle/Makefile) links from the reference's own main.cpp, cpu.cpp and
+# two-phase.cpp.  The arm writes its defines.ini itself so that nothing of this
+# repository's package or oracle library is loaded into the process.
+REF_BINARY_2PH = os.path.join(ROOT, "oracle", "_ref", "capaz_ref_2ph")
+REF_MAX_STEPS = 25
+
+
+def reference_ini(nx: int, ny: int, nz: int, dt: float) -> str:
+    """defines.ini (KEY=value, the reference's read_defines format) for the
+    workload's fluids on the reference model: mu 1e-3/5e-3 Pa s, rho
+    1000/850 kg/m^3, beta 1e-9 1/Pa, Brooks-Corey lambda 2, S_wr 0.1, no
+    capillary pressure, h = 1 m, K = 1e-12 m^2 and porosity 0.3 uniform (the
+    reference model reads K_0 and M_0 only), S_n = 0.1 injected over the whole
+    top face, 10 Newton iterations."""
+    vals = [("NX", nx), ("NY", ny), ("NZ", nz), ("HX", 1.0), ("HY", 1.0), ("HZ", 1.0), ("DT", dt),
+            ("TAU", 1e-7), ("L", 1e-4), ("C_W", 1500), ("C_N", 1000), ("C_G", 330),
+            ("BETA_W", 1e-9), ("BETA_N", 1e-9), ("BETA_G", 9.2e-6), ("RO_W", 1000.0), ("RO_N", 850.0),
+            ("RO_G", 1.4), ("MU_W", 1e-3), ("MU_N", 5e-3), ("MU_G", 1.84e-5), ("G_CONST", 9.81),
+            ("P_ATM", 1e5), ("LAMBDA_0", 2.0), ("LAMBDA_1", 2.0), ("M_0", 0.3), ("M_1", 0.3),
+            ("S_WR_0", 0.1), ("S_WR_1", 0.1), ("S_NR_0", 0.0), ("S_NR_1", 0.0), ("S_GR_0", 0.0),
+            ("S_GR_1", 0.0), ("K_0", 1e-12), ("K_1", 1e-12), ("P_D_0", 0.0), ("P_D_1", 0.0),
+            ("P_D_NW_0", 0.0), ("P_D_NW_1", 0.0), ("P_D_GN_0", 0.0), ("P_D_GN_1", 0.0),
+            ("S_N_GR", 0.1), ("S_W_GR", 0.4), ("S_W_INIT", 0.4), ("S_N_INIT", 0.3),
+            ("SOURCE", max(nx, nz)), ("ITERATIONS", 10), ("TIMEX", 100.0),
+            ("SAVE_PLOTS", 1000000), ("PRINT_SCREEN", 1000000)]
+    return "".join(f"{k}={v!r}\n" if isinstance(v, float) else f"{k}={v}\n" for k, v in vals)
+
+
+def reference_cpu_step(grid, nsteps: int) -> dict:
+    """Runs the reference's own CPU time step (single-threaded, as written) on
+    the workload grid for `nsteps` steps from its data_initialization state.
+    dt is 0.4 x the explicit scheme's stability bound for the uniform media,
+    0.4 h^2 m mu_w beta / (6 K) = 0.02 s; the work per cell-step does not
+    depend on it.  Returns the harness's own timing of the step loop."""
+    import tempfile
+    Nx, Ny, Nz = grid
+    nx, ny, nz = Nx, Nz, Ny                       # reference axes: NY vertical
+    dt = 0.4 * 1.0 * 0.3 * 1e-3 * 1e-9 / (6.0 * 1e-12)
+    with tempfile.TemporaryDirectory() as wd:
+        with open(os.path.join(wd, "defines.ini"), "w") as f:
+            f.write(reference_ini(nx, ny, nz, dt))
+        out = os.path.join(wd, "out.bin")
+        t0 = time.perf_counter()
+        res = subprocess.run([REF_BINARY_2PH, wd, str(nsteps), "-", out], capture_output=True, text=True)
+        wall = time.perf_counter() - t0
+        if res.returncode != 0:
+            raise RuntimeError(f"reference step failed ({res.returncode}): {res.stderr[-500:]}")
+        info = json.loads([ln for ln in res.stdout.splitlines() if ln.startswith("RESULT ")][-1][7:])
+        S = np.fromfile(out, dtype=np.float64)[nx * ny * nz:]
+    return {"cells": nx * ny * nz, "steps": nsteps, "seconds": info["seconds"], "wall": wall, "dt": dt,
+            "finite": bool(np.isfinite(S).all())}
 
 
 def run_reference(args) -> None:
-    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    """The reference arm: the reference's own CPU time step on the workload's
+    full grid, through its own code path (main.cpp's time_step_function over
+    cpu.cpp and two-phase.cpp).  Rank 0 only; other ranks exit."""
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from capaz_b200.configs import two_phase_params
-    from oracle import oracle as O
     K, W = args.steps, args.warmup
-    Nx, Ny, Nz = args.grid
     line = {"impl": "reference", "metric": "cell-steps/s", "unit": "cell-steps/s", "higher_is_better": True,
             "n_gpus": args.gpus, "steps": K, "warmup": W, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic"}
-    if not O.ref_available(2):
+            "dtype": "f64", "data": "synthetic", "config": workload_config(args.grid, args.gpus)}
+    if not os.path.exists(REF_BINARY_2PH):
         line["unavailable"] = "reference CPU binaries (oracle/_ref) were not built"
         print(json.dumps(line), flush=True)
         return
-    nx, ny, nz = reference_sample_grid(K + W)
-    p = two_phase_params(nx, ny, nz, percell_k=False)
-    # The reference model has no top-pressure offset, background saturation
-    # or per-cell K: uniform K = 1e-12 (the field's median) and its own
-    # initial state; the work per cell-step is the same.
-    p.P_top_offset = 0.0
-    p.S_n_background = 0.0
-    p.dt = 1e-3
-    t0 = time.perf_counter()
-    r = O.ref_run(p, K + W)
-    wall = time.perf_counter() - t0
-    secs = r["info"]["seconds"]
-    val = p.ncell * (K + W) / secs
+    # One step of the full grid takes seconds on one core: the run steps the
+    # whole grid K + W times, at most REF_MAX_STEPS, and times every step.
+    n = max(1, min(K + W, REF_MAX_STEPS))
+    r = reference_cpu_step(args.grid, n)
+    val = r["cells"] * n / r["seconds"]
     line.update({
-        "value": val, "ms_per_step": 1e3 * secs / (K + W),
-        "config": {"workload": f"reference two-phase CPU step on a {nx}x{ny}x{nz} slab of the "
-                               f"{Nx}x{Ny}x{Nz} workload (uniform K)", "grid_ref": [nx, ny, nz]},
+        "value": val, "ms_per_step": 1e3 * r["seconds"] / n,
+        "form": "f64 (the reference's CPU step, single-threaded as written)",
+        "media": "uniform K 1e-12 and porosity 0.3 (the reference model has no per-cell K); the work per "
+                 "cell-step does not depend on the values",
+        "dt": r["dt"], "finite": r["finite"],
         "cpu_baseline": {"value": val, "unit": "cell-steps/s", "cores": 1, "kind": "reference",
-                         "sample": f"{K + W} steps of a {nx}x{ny}x{nz} grid with the reference's own CPU "
-                                   f"step (single-threaded as written), {secs:.1f} s loop, {wall:.1f} s wall"},
+                         "sample": f"{n} steps of the full {args.grid[0]}x{args.grid[1]}x{args.grid[2]} grid "
+                                   f"with the reference's own CPU step, {r['seconds']:.1f} s step loop "
+                                   f"({r['wall']:.1f} s with set-up)"},
         "e2e": {"value": val, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     })
     print(json.dumps(line), flush=True)
@@ -803,22 +856,29 @@ def run_capaz(args) -> None:
         sim2 = Simulation(q, device=dev)
         slots = native.DIAG_SLOTS
 
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
         def e2e_pass(nsteps):
             """Upload, nsteps steps with their diagnostics, download.  Each
             step's diagnostics are read one step behind: the copy is posted
             after step i and waited for after step i + 1 has been queued, so
-            the device never idles while the host reads."""
+            the device never idles while the host reads.  Events on the
+            stream split the pass into upload, steps and download."""
+            ev[0].record(stream)
             for name in ("m", "K", "P_w", "S_n"):
                 native.check(sim2.lib.capaz_set_field(sim2.ctx, native.FIELDS[name], host[name].data_ptr(), sh),
                              sim2.ctx)
+            ev[1].record(stream)
             for i in range(nsteps):
                 sim2.step(1, stream=sh)
                 sim2.post_diag(i % slots, stream=sh)
                 if i > 0:
                     sim2.wait_diag((i - 1) % slots)
+            ev[2].record(stream)
             sim2.wait_diag((nsteps - 1) % slots)
             native.check(sim2.lib.capaz_get_field(sim2.ctx, native.FIELDS["P_w"], out_P.data_ptr(), sh), sim2.ctx)
             native.check(sim2.lib.capaz_get_field(sim2.ctx, native.FIELDS["S_n"], out_S.data_ptr(), sh), sim2.ctx)
+            ev[3].record(stream)
 
         # Warm-up pass (W steps): the context's first download allocates its
         # FP64 decode buffers; the timed pass starts from the same upload.
@@ -830,10 +890,18 @@ def run_capaz(args) -> None:
         e2e_s = time.perf_counter() - t0
         barrier(ws, local)
         e2e_s = reduce_max(e2e_s, ws)
+        torch.cuda.synchronize()
+        up_ms, loop_ms, down_ms = (ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]),
+                                   ev[2].elapsed_time(ev[3]))
         h2d = 4 * ncell * 8
         d2h = 2 * ncell * 8 + K * 40
         e2e = {"value": ncell * K * ws / e2e_s, "unit": "cell-steps/s",
                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+               "upload_ms": up_ms, "download_ms": down_ms, "step_with_diag_ms": loop_ms / K,
+               "per_step_value": ncell * ws / (loop_ms * 1e-3 / K),
+               "breakdown": "device-stream events: upload (4 float64 fields, encoded on the device) and download "
+                            "(2 fields, decoded) once per pass; step_with_diag_ms = a step plus its posted "
+                            "diagnostics read, what every further step costs; per_step_value = cells / that",
                "definition": "float64 pinned-host upload of P_w, S_n, m, K; K steps each followed by a "
                              "device-to-host read of that step's diagnostics (mass balance, Newton residual, "
                              "40 B into a pinned ring, waited for one step behind); float64 download of P_w, "
@@ -853,12 +921,25 @@ def run_capaz(args) -> None:
             "algorithmic_bytes_per_cell": ALGO_BYTES[(head, percell)],
             "kernel_ms": t["kern_ms"], "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
 
-    cpu = None
+    # ---- CPU baselines: the reference's own step (one core, as written) and
+    # the OpenMP oracle (all host threads), both on the full workload grid --
+    cpu = cpu_port = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline_port(w)
+            r = reference_cpu_step(args.grid, 2)
+            cpu = {"value": r["cells"] * r["steps"] / r["seconds"], "unit": "cell-steps/s", "cores": 1,
+                   "kind": "reference",
+                   "sample": f"{r['steps']} steps of the full {args.grid[0]}x{args.grid[1]}x{args.grid[2]} grid "
+                             f"with the reference's own CPU step (oracle/_ref, uniform K), "
+                             f"{r['seconds']:.1f} s step loop"}
         except Exception as e:  # the baseline is informative, never fatal
-            cpu = {"value": None, "unit": "cell-steps/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
+            cpu = {"value": None, "unit": "cell-steps/s", "cores": 1, "kind": "reference",
+                   "sample": f"failed: {e}"}
+        try:
+            cpu_port = cpu_baseline_port(w)
+        except Exception as e:  # the baseline is informative, never fatal
+            cpu_port = {"value": None, "unit": "cell-steps/s", "cores": 0, "kind": "port",
+                        "sample": f"failed: {e}"}
 
     if rank == 0:
         forms_out = {}
@@ -875,12 +956,10 @@ def run_capaz(args) -> None:
                                   "(Fermi-era GPU)",
             "dtype": "f64" if head == "fp64" else "f32 storage+stencil (compensated), f64 Newton",
             "data": "synthetic (seeded lognormal K and porosity fields)",
-            "config": {"workload": f"two-phase {args.grid[0]}x{args.grid[1]}x{args.grid[2]} gravity on z, "
-                                   f"lognormal K sigma 1 ell 8, form {head}",
-                       "grid_ref": [p.nx, p.ny, p.nz], "cells": ncell, "form": head, "dt": p.dt,
-                       "parallelism": f"replicas x{ws}",
-                       "l2": "inputs larger than L2: each step reads P_w, S_n, m, K and writes P_w, S_n "
-                             f"({ALGO_BYTES[(head, percell)] * ncell / 1e6:.0f} MB of the {126} MB L2)"},
+            "config": workload_config(args.grid, ws),
+            "form": head, "dt": p.dt,
+            "media": "lognormal K (sigma 1, correlation length 8 cells, seeded FFT field), porosity "
+                     "0.25 + 0.02 G clipped to [0.1, 0.4]",
             "repeats": {"count": len(t["repeat_ms_per_step"]), "steps_each": K,
                         "ms_per_step": t["repeat_ms_per_step"],
                         "median_ms_per_step": (statistics.median(t["repeat_ms_per_step"])
@@ -895,8 +974,18 @@ def run_capaz(args) -> None:
             "ensemble": ens,
             "buckley_leverett": bl,
             "energy": energy,
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": t["launches"],
+            "roofline": roof, "cpu_baseline": cpu, "cpu_baseline_port": cpu_port,
+            "e2e": e2e, "clocks": clk, "gpu_launches": t["launches"],
         }
+        ref_v = cpu["value"] if cpu else None
+        if ref_v:
+            # Speed-ups over the reference's own CPU step timed in this run
+            # (one core, as the reference is written): the headline form, the
+            # plain FP64 form (the like-for-like arithmetic), and end to end.
+            line["speedup_vs_reference_cpu"] = {
+                "form_" + f: forms_out[f]["value"] / ref_v for f in forms_out}
+            if e2e:
+                line["speedup_vs_reference_cpu"]["e2e"] = e2e["value"] / ref_v
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

@@ -62,11 +62,12 @@ def grf(shape, ell: float, seed: int) -> np.ndarray:
         sh[ax] = -1
         r2 = r2 + (a.reshape(sh)) ** 2
     cov = np.exp(-np.sqrt(r2) / ell)
-    lam = np.fft.rfftn(cov).real
+    axes_all = tuple(range(len(pad)))
+    lam = np.fft.rfftn(cov, axes=axes_all).real
     np.maximum(lam, 0.0, out=lam)
     del cov, r2
     noise = rng.standard_normal(pad)
-    f = np.fft.irfftn(np.sqrt(lam) * np.fft.rfftn(noise), s=pad)
+    f = np.fft.irfftn(np.sqrt(lam) * np.fft.rfftn(noise, axes=axes_all), s=pad, axes=axes_all)
     g = f[tuple(slice(0, s) for s in shape)]
     g = (g - g.mean()) / g.std()
     return np.ascontiguousarray(g)

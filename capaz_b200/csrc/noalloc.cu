@@ -148,6 +148,9 @@ extern "C" int capaz_mass_noalloc(const capaz_params* p, const double* P_w, cons
                                   double* out, void* stream) {
   if (!p || !P_w || !S_n || !m || !out) return fail(CAPAZ_ERR_INVALID_ARGUMENT, "capaz_mass_noalloc: null argument");
   if (p->phases != 2) return fail(CAPAZ_ERR_UNSUPPORTED, "capaz_mass_noalloc: two-phase states only");
+  if (p->model != CAPAZ_MODEL_DEFAULT && p->model != CAPAZ_MODEL_BUCKLEY_LEVERETT)
+    return fail(CAPAZ_ERR_UNSUPPORTED,
+                "capaz_mass_noalloc: the isothermal two-phase and Buckley-Leverett models only");
   if (p->nx < 3 || p->ny < 3 || p->nz < 1 || p->nz == 2)
     return fail(CAPAZ_ERR_UNSUPPORTED_GRID, "capaz_mass_noalloc: grid needs nx,ny>=3 and nz==1 or >=3");
   const long long rows = (long long)(p->ny - 2) * (p->nz == 1 ? 1 : p->nz - 2);
@@ -168,12 +171,23 @@ extern "C" int capaz_mass_noalloc(const capaz_params* p, const double* P_w, cons
   if (!on_device(P_w, dev) || !on_device(S_n, dev) || !on_device(m, dev) || !on_device(out, dev))
     return fail(CAPAZ_ERR_INVALID_ARGUMENT, "capaz_mass_noalloc: pointers must be device memory of the current device");
 
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(s, &capture);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CAPAZ_ERR_INVALID_ARGUMENT, "capaz_mass_noalloc: stream does not belong to the current device");
+  }
   double* scratch;
   {
-    // Set-up, once per device with that device current: the address of the
-    // fixed scratch in this device's copy of the module.
+    // The address of the fixed scratch in the current context's copy of the
+    // module.  It is looked up again on every call made outside stream
+    // capture (a lookup, no allocation), so a device reset or a caller's own
+    // non-primary context gets the address of its own copy; a call on a
+    // capturing stream uses the address the device's last uncaptured call
+    // found, so the first call on a device must come before any capture.
     std::lock_guard<std::mutex> g(g_setup_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (capture == cudaStreamCaptureStatusNone) {
       void* a = nullptr;
       e = cudaGetSymbolAddress(&a, g_mass_scratch);
       if (e != cudaSuccess || !a) {
@@ -181,6 +195,9 @@ extern "C" int capaz_mass_noalloc(const capaz_params* p, const double* P_w, cons
         return fail(CAPAZ_ERR_CUDA, "capaz_mass_noalloc: cudaGetSymbolAddress of the fixed scratch failed");
       }
       g_scratch_ptr[dev] = (double*)a;
+    } else if (!g_scratch_ptr[dev]) {
+      return fail(CAPAZ_ERR_BAD_STATE,
+                  "capaz_mass_noalloc: the first call on a device must not be made on a capturing stream");
     }
     scratch = g_scratch_ptr[dev];
   }
@@ -201,7 +218,6 @@ extern "C" int capaz_mass_noalloc(const capaz_params* p, const double* P_w, cons
   c.P_atm = p->P_atm;
   c.vol = p->hx * p->hy * p->hz;
   const int nblocks = (int)((rows + kRowsPerBlock - 1) / kRowsPerBlock);
-  cudaStream_t s = (cudaStream_t)stream;
   mass_rows_kernel<<<nblocks, 32 * kRowsPerBlock, 0, s>>>(c, P_w, S_n, m, scratch);
   mass_finalize_kernel<<<1, 128, 0, s>>>(scratch, nblocks, out);
   e = cudaGetLastError();

@@ -372,10 +372,14 @@ int capaz_backward(capaz_adjoint* a, double* grad_lnK, double* grad_m, int dst_o
  * CAPAZ_FLAG_DIAGNOSTICS: out[0..4] (device memory, the capaz_diag layout)
  * receive mass_w, mass_n, 0, 0 and the count of cells whose P or S is not
  * finite.  All scratch is a fixed device array of the library, so no call
- * allocates memory.  The first call on a device (with that device current)
- * does a one-time set-up of the scratch address; make it before any stream
- * capture.  Grids with (ny-2)*max(nz-2,1) > CAPAZ_NOALLOC_MAX_ROWS are
- * rejected with CAPAZ_ERR_UNSUPPORTED_GRID.  Calls that overlap on one
+ * allocates memory.  Every call made outside stream capture looks up the
+ * scratch address in the current context's copy of the library (a lookup,
+ * no allocation); a call on a capturing stream reuses the address of the
+ * device's last uncaptured call, so make the first call on a device (with
+ * that device current) before any stream capture.  Models other than
+ * CAPAZ_MODEL_DEFAULT and CAPAZ_MODEL_BUCKLEY_LEVERETT are rejected with
+ * CAPAZ_ERR_UNSUPPORTED; grids with (ny-2)*max(nz-2,1) >
+ * CAPAZ_NOALLOC_MAX_ROWS with CAPAZ_ERR_UNSUPPORTED_GRID.  Calls that overlap on one
  * device (other streams or host threads) share the scratch and race: order
  * them.  Errors are reported through capaz_last_error(NULL). */
 #define CAPAZ_NOALLOC_MAX_ROWS 131072

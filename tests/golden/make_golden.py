@@ -62,7 +62,7 @@ def save(name, p, nsteps, state, m, with_derived):
 
 def main():
     if not (O.ref_available(2) and O.ref_available(3)):
-        raise SystemExit("build the reference binaries first: make -C oracle ref")
+        raise SystemExit("build the reference binaries first: make -C oracle REF=<reference tree> ref")
     rng = np.random.default_rng(20261203)
 
     # The reference's own Two-phase/defines.ini values, its own initial state.
@@ -118,7 +118,7 @@ def main_energy():
     column case from its own initial state, and random 3-D states with a
     random temperature field."""
     if not os.path.exists(O.ref_binary(3, 2)):
-        raise SystemExit("build the reference binaries first: make -C oracle ref")
+        raise SystemExit("build the reference binaries first: make -C oracle REF=<reference tree> ref")
     rng = np.random.default_rng(20261204)
     p3 = default_params(phases=3, nx=1, ny=15, nz=1, newton_iterations=7, lambda_=3.25, S_wr=0.0,
                         ro0_n=850.0, ro0_g=1.4, mu_n=1e-3, mu_g=1.84e-5, beta_g=9.2e-6, S_w_gr=0.4,
@@ -168,7 +168,7 @@ def save_bl(name, p, nsteps, seed):
 
 def main_bl():
     if not os.path.exists(O.ref_binary(2, 1)):
-        raise SystemExit("build the reference binaries first: make -C oracle ref")
+        raise SystemExit("build the reference binaries first: make -C oracle REF=<reference tree> ref")
     save_bl("gbl_planar_20x15x1", bl_params(20, 15, 1, 0.0, 2000.0), 40, 20)
     save_bl("gbl_3d_gravity_12x10x6", bl_params(12, 10, 6, 9.81, 200.0), 30, 12)
 

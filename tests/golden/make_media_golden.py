@@ -51,7 +51,7 @@ def reference_K(noise_path: str, nx: int, ny: int, nz: int) -> np.ndarray:
 
 def main():
     if not os.path.exists(LOADK):
-        sys.exit("build oracle/_ref/capaz_ref_loadk first (make -C oracle ref)")
+        sys.exit("build oracle/_ref/capaz_ref_loadk first (make -C oracle REF=<reference tree> ref)")
     nx, ny = 13, 9
     rng = np.random.default_rng(20)
     vals = rng.normal(0.0, 1.5, size=(ny, nx))

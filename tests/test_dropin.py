@@ -48,7 +48,7 @@ def test_dropin_covers_what_the_reference_host_program_needs(exe, lib):
     """Every symbol the reference's main.cpp takes from its arch backend is
     among those the drop-in exports (checked on the linked test binary)."""
     if not os.path.exists(exe):
-        pytest.skip("drop-in link binaries not built (make -C oracle all)")
+        pytest.skip("drop-in link binaries not built (make -C oracle REF=<reference tree> all)")
     res = subprocess.run(["ldd", exe], capture_output=True, text=True)
     assert "not found" not in res.stdout
     assert lib in res.stdout
@@ -121,7 +121,7 @@ def test_dropin3_harness_matches_reference(name):
     """The reference's three-phase step loop driven through
     libcapaz_dropin_3ph reproduces the reference CPU results."""
     if not os.path.exists(HARNESS3):
-        pytest.skip("drop-in link binaries not built (make -C oracle all)")
+        pytest.skip("drop-in link binaries not built (make -C oracle REF=<reference tree> all)")
     p, g = load_golden(name)
     names = ["P_w", "S_w", "S_n", "P_n", "P_g"]
     if "in_P_w" in g:
@@ -149,7 +149,7 @@ def test_reference_three_phase_program_runs_unmodified_on_the_dropin(tmp_path, s
     data_initialization left, while the CPU backend updates it in place."""
     from capaz_b200.simulation import default_params
     if not os.path.exists(MAIN_DROPIN3):
-        pytest.skip("drop-in link binaries not built (make -C oracle all)")
+        pytest.skip("drop-in link binaries not built (make -C oracle REF=<reference tree> all)")
     nx, ny, nz = shape
     p = default_params(phases=3, nx=nx, ny=ny, nz=nz, newton_iterations=7, lambda_=2.0, S_wr=0.1, S_nr=0.05,
                        S_gr=0.02, ro0_w=1000.0, ro0_n=850.0, ro0_g=1.2, mu_w=1e-3, mu_n=3e-3, mu_g=1.8e-5,

@@ -36,7 +36,7 @@ def reference_plots(p, tmp_path, save_every, noise=None):
     (read from ../noise.dat)."""
     exe = MAIN_REF[{native.MODEL_BUCKLEY_LEVERETT: "bl", native.MODEL_ENERGY: "energy"}.get(p.model, p.phases)]
     if not os.path.exists(exe):
-        pytest.skip("reference whole-program binaries not built (make -C oracle ref)")
+        pytest.skip("reference whole-program binaries not built (make -C oracle REF=<reference tree> ref)")
     ini = O.ref_ini_text(p).replace("SAVE_PLOTS=1000000", f"SAVE_PLOTS={save_every}")
     wd = tmp_path / "ref"
     (wd / "run").mkdir(parents=True)

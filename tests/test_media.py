@@ -23,7 +23,7 @@ def test_reader_matches_reference_golden():
     assert np.array_equal(K, g["K"])
 
 
-@pytest.mark.skipif(not os.path.exists(mg.LOADK), reason="reference harness not built (make -C oracle ref)")
+@pytest.mark.skipif(not os.path.exists(mg.LOADK), reason="reference harness not built (make -C oracle REF=<reference tree> ref)")
 @pytest.mark.parametrize("shape,seed", [((17, 11, 1), 1), ((8, 6, 5), 2)])
 def test_reader_matches_reference_live(tmp_path, shape, seed):
     """Any field, any z depth: every z layer takes the file's (i, j) value."""

@@ -116,7 +116,7 @@ def test_reverse_matrix_singular_and_pivot():
     assert np.allclose(inv @ a, np.eye(3))
 
 
-@pytest.mark.skipif(not O.ref_available(2), reason="reference binaries not built (make -C oracle ref)")
+@pytest.mark.skipif(not O.ref_available(2), reason="reference binaries not built (make -C oracle REF=<reference tree> ref)")
 @pytest.mark.parametrize("seed", [1, 2])
 def test_oracle_vs_reference_binary_random(seed):
     """Fresh random cases straight against the compiled reference."""

@@ -71,7 +71,14 @@ def test_noalloc_mass_matches_step_diagnostics(shape, P_d):
             sim.get_field_device("m", M.data_ptr())
             sim.sync()
             first = _noalloc(lib, p, P, S, M, out)
+            torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info(0)[0]
             second = _noalloc(lib, p, P, S, M, out)
+            for _ in range(4):
+                _noalloc(lib, p, P, S, M, out)
+            torch.cuda.synchronize()
+            # the property the entry point exists for: calls allocate nothing
+            assert torch.cuda.mem_get_info(0)[0] == free0, "device free memory changed across the calls"
             _check(diag, first)
             _check(diag, second)
             assert np.array_equal(first, second), "two calls in a row differ"
@@ -97,3 +104,17 @@ def test_noalloc_rejects_grids_beyond_fixed_scratch():
     st = lib.capaz_mass_noalloc(C.byref(p), fake, fake, fake, fake, None)
     assert st == native.ERR_UNSUPPORTED_GRID
     assert b"exceed the fixed scratch" in lib.capaz_last_error(None)
+
+
+@pytest.mark.parametrize("model", [native.MODEL_ENERGY, 7])
+def test_noalloc_rejects_other_models(model):
+    """Only the isothermal two-phase and Buckley-Leverett models are summed;
+    anything else is rejected from the parameters alone, before any pointer
+    is touched."""
+    lib = native.load()
+    p, _, _ = _case(8, 8, 3, 0.0, 0)
+    p.model = model
+    fake = 0x1000
+    st = lib.capaz_mass_noalloc(C.byref(p), fake, fake, fake, fake, None)
+    assert st == native.ERR_UNSUPPORTED
+    assert b"models only" in lib.capaz_last_error(None)
