@@ -228,7 +228,7 @@ def workload_config(grid, ws: int) -> dict:
 # two-phase.cpp.  The arm writes its defines.ini itself so that nothing of this
 # repository's package or oracle library is loaded into the process.
 REF_BINARY_2PH = os.path.join(ROOT, "oracle", "_ref", "capaz_ref_2ph")
-REF_MAX_STEPS = 25
+REF_MAX_STEPS = 12
 
 
 def reference_ini(nx: int, ny: int, nz: int, dt: float) -> str:
