@@ -28,6 +28,7 @@ struct capaz_batch {
   unsigned int* counter = nullptr;
   int zchunk = 16;
   int ctas_per_sm = 0;  // 0: as many as fit
+  int tile_y = TMA_TILE_Y;  // rows of a sweep tile (precision form)
   int grid = 0;
   std::vector<double> built_dt, built_Sref;
   bool built = false;
@@ -61,7 +62,7 @@ int bcuda(capaz_batch* b, cudaError_t e, const char* what) {
 int occupancy(const capaz_batch* b) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-  const int full = b->fp32 ? step2_fp32c_tma_grid(b->device, b->unik) : step2_fp64_batch_grid(b->device);
+  const int full = b->fp32 ? step2_fp32c_tma_grid(b->device, b->unik, b->tile_y) : step2_fp64_batch_grid(b->device);
   return std::max(1, full / std::max(1, sms));
 }
 
@@ -76,7 +77,8 @@ int build(capaz_batch* b) {
     for (int q = 0; q < n; q++) {
       capaz_ctx* x = b->ctx[q];
       // The instance's own TMA descriptor carries its maps and arguments;
-      // rebuild it with the batch's z-chunk depth.
+      // rebuild it for the batch's tile shape and z-chunk depth.
+      x->tma_tile_y = b->tile_y;
       int st = x->tma_prepare();
       if (st) return bfail(b, st, x->last_error);
       BTRY(b, cudaMemcpy(&h[q], x->tma_inst, sizeof(InstT), cudaMemcpyDeviceToHost));
@@ -172,7 +174,7 @@ int kernels_per_step(const capaz_batch* b) { return b->fp32 ? 2 : 1; }
 cudaError_t launch_one(capaz_batch* b, int parity, cudaStream_t s) {
   if (b->fp32)
     return launch_step2_fp32c_tma(b->phys, b->d_instT, b->d_items, b->nitems, b->d_bitems, b->nbitems, parity,
-                                  b->unik, b->planar, b->counter, nullptr, b->grid, s);
+                                  b->unik, b->planar, b->counter, nullptr, b->grid, s, nullptr, b->tile_y);
   return launch_step2_fp64_batch(b->d_inst64, b->d_items, b->nitems, parity, b->unik, b->pd0, b->counter, b->grid, s);
 }
 
@@ -345,30 +347,38 @@ int capaz_batch_autotune(capaz_batch* b, void* stream, int* zchunk_out, int* per
   }
   std::vector<long long> done0;
   for (auto* x : b->ctx) done0.push_back(x->steps_done);
-  const int occ = occupancy(b);
   const int zc_cands[4] = {8, 16, 32, 64};
+  // Tile shapes: 32 x 16 and 32 x 32 for the precision form's sweep; the
+  // FP64 batch kernel has one.
+  const int tile_cands[2] = {16, 32};
+  const int ntile = b->fp32 ? 2 : 1;
   float best = 1e30f;
-  int best_zc = b->zchunk, best_per = 0;
+  int best_zc = b->zchunk, best_per = 0, best_tile = b->tile_y;
   cudaEvent_t e0, e1;
   BTRY(b, cudaEventCreate(&e0));
   BTRY(b, cudaEventCreate(&e1));
   int rc = CAPAZ_OK;
-  for (int zc : zc_cands) {
-    for (int per = 1; per <= occ && rc == CAPAZ_OK; per++) {
-      b->zchunk = zc;
-      b->ctas_per_sm = per;
-      if ((rc = build(b))) break;
-      if ((rc = run_steps(b, 2, s, false))) break;  // warm-up (even: parity preserved)
-      cudaEventRecord(e0, s);
-      if ((rc = run_steps(b, 6, s, false))) break;
-      cudaEventRecord(e1, s);
-      cudaEventSynchronize(e1);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best) {
-        best = ms;
-        best_zc = zc;
-        best_per = per;
+  for (int ti = 0; ti < ntile && rc == CAPAZ_OK; ti++) {
+    if (b->fp32) b->tile_y = tile_cands[ti];
+    const int occ = occupancy(b);
+    for (int zc : zc_cands) {
+      for (int per = 1; per <= occ && rc == CAPAZ_OK; per++) {
+        b->zchunk = zc;
+        b->ctas_per_sm = per;
+        if ((rc = build(b))) break;
+        if ((rc = run_steps(b, 2, s, false))) break;  // warm-up (even: parity preserved)
+        cudaEventRecord(e0, s);
+        if ((rc = run_steps(b, 6, s, false))) break;
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+          best = ms;
+          best_zc = zc;
+          best_per = per;
+          best_tile = b->tile_y;
+        }
       }
     }
   }
@@ -388,11 +398,31 @@ int capaz_batch_autotune(capaz_batch* b, void* stream, int* zchunk_out, int* per
   if (rc) return rc;
   b->zchunk = best_zc;
   b->ctas_per_sm = best_per;
+  b->tile_y = best_tile;
   int st = build(b);
   if (st) return st;
   if (zchunk_out) *zchunk_out = best_zc;
   if (per_sm_out) *per_sm_out = best_per;
   return CAPAZ_OK;
+}
+
+int capaz_batch_get_tuning(const capaz_batch* b, int* zchunk, int* ctas_per_sm, int* tile_y) {
+  if (!b) return CAPAZ_ERR_INVALID_ARGUMENT;
+  if (zchunk) *zchunk = b->zchunk;
+  if (ctas_per_sm) *ctas_per_sm = b->ctas_per_sm;
+  if (tile_y) *tile_y = b->fp32 ? b->tile_y : 0;
+  return CAPAZ_OK;
+}
+
+int capaz_batch_set_tuning(capaz_batch* b, int zchunk, int ctas_per_sm, int tile_y) {
+  if (!b || zchunk < 1 || ctas_per_sm < 0) return CAPAZ_ERR_INVALID_ARGUMENT;
+  if (b->fp32 && !tma_tile_supported(tile_y)) return bfail(b, CAPAZ_ERR_UNSUPPORTED, "tile_y must be 16 or 32");
+  BTRY(b, cudaSetDevice(b->device));
+  BTRY(b, cudaDeviceSynchronize());  // earlier steps may still read the descriptors
+  b->zchunk = zchunk;
+  b->ctas_per_sm = ctas_per_sm;
+  if (b->fp32) b->tile_y = tile_y;
+  return build(b);
 }
 
 }  // extern "C"

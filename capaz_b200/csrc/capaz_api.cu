@@ -615,6 +615,13 @@ int capaz_set_dt(capaz_ctx* ctx, double dt) {
   return CAPAZ_OK;
 }
 
+int capaz_set_sweep_tile(capaz_ctx* ctx, int tile_y) {
+  if (!ctx) return CAPAZ_ERR_INVALID_ARGUMENT;
+  if (!tma_tile_supported(tile_y)) return fail(ctx, CAPAZ_ERR_UNSUPPORTED, "tile_y must be 16 or 32");
+  ctx->tma_tile_y = tile_y;  // the descriptor is rebuilt before the next step
+  return CAPAZ_OK;
+}
+
 int capaz_set_field(capaz_ctx* ctx, int field, const double* host, void* stream) {
   if (!ctx || !host) return CAPAZ_ERR_INVALID_ARGUMENT;
   return ctx->set_field(field, host, false, (cudaStream_t)stream);
@@ -860,6 +867,9 @@ int capaz_ctx::set_field(int field, const void* src, bool on_device, cudaStream_
 int capaz_ctx::check_flag() {
   unsigned int f = 0;
   CUDA_TRY(this, cudaMemcpy(&f, err_flag, sizeof f, cudaMemcpyDeviceToHost));
+  if (f & 2u)
+    return fail(this, CAPAZ_ERR_CUDA,
+                "a bounded wait for a shared-memory copy ran out (device error bit 1); the step is incomplete");
   if (f) return fail(this, CAPAZ_ERR_NONFINITE, "a step produced a non-finite P or S");
   return CAPAZ_OK;
 }

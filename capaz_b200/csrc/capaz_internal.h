@@ -160,18 +160,21 @@ struct alignas(128) InstT {
   float dt_f;
   float sgr_dev_f;  // S_n_gr - S_ref (stored deviation of the source saturation)
   int nbound;       // boundary cells (written by the boundary kernel after the sweep)
+  int tile_y;       // rows of a tile (the tensor maps' box is 36 x (tile_y + 2))
+  // Bytes each raw stage announces beyond what its copies bring: 0, except
+  // under CAPAZ_FLAG_TEST_WAIT_TIMEOUT, where it makes the first bounded
+  // wait of every CTA run out (a test of the timeout path; nothing faults).
+  unsigned int test_tx_extra;
   double S_ref, dt;
   const float4* rowF;  // ny: (rho_w/mu_w, rho_n/mu_n at P_ref(j), (P_ref(j+1)-P_ref(j))/hy^2, 0)
   const double* Pref;  // ny
   Step2FArgs a[2];     // a[parity]: state pointers and the error flag
 };
-// Tile of the TMA-staged precision step: TX x TMA_TILE_Y interior cells,
-// CAPAZ_TMA_TY thread rows each owning two cell rows.
-#ifndef CAPAZ_TMA_TY
-#define CAPAZ_TMA_TY 8
-#endif
-constexpr int TMA_TY = CAPAZ_TMA_TY;
-constexpr int TMA_TILE_Y = 2 * TMA_TY;
+// Tiles of the TMA-staged precision step: TX x tile_y interior cells, one
+// warp per four rows; tile_y is 16 (four warps, four CTAs per SM) or 32
+// (eight warps, two CTAs per SM).  TMA_TILE_Y is the default.
+constexpr int TMA_TILE_Y = 16;
+bool tma_tile_supported(int tile_y);
 // All instances of one launch are planar (nz == 1) or all three-dimensional.
 // Launches the sweep over the interior cells and then the boundary kernel
 // (bitems: (instance, first boundary cell) blocks of BOUND_BLOCK cells).
@@ -181,15 +184,15 @@ constexpr int BOUND_BLOCK = 256;
 cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems,
                                    const int2* bitems, int nbitems, int parity, bool unik, bool planar,
                                    unsigned int* counter, double* diag_partials, int grid, cudaStream_t s,
-                                   double* diag_out = nullptr);
+                                   double* diag_out, int tile_y);
 // Boundary cells of an nx x ny x nz grid (faces, edges, corners; nz == 1: the
 // four sides of the plane).
 inline int boundary_cells(int nx, int ny, int nz) {
   if (nz == 1) return 2 * nx + 2 * (ny - 2);
   return 2 * nx * nz + 2 * (ny - 2) * nz + 2 * (nx - 2) * (ny - 2);
 }
-int step2_fp32c_tma_grid(int device, bool unik);
-int encode_field_map(CUtensorMap* map, const float* base, int nx, int ny, int nz);
+int step2_fp32c_tma_grid(int device, bool unik, int tile_y);
+int encode_field_map(CUtensorMap* map, const float* base, int nx, int ny, int nz, int tile_y);
 cudaError_t launch_row_tables(const double* Pref, int ny, const PhysF& f, float4* rowF, cudaStream_t s);
 
 // Field preparation (fields.cu).

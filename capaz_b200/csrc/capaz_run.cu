@@ -84,7 +84,8 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
       // With diagnostics, the last step's boundary kernel also reduces the
       // sweep's partials into diag_out.
       e = launch_step2_fp32c_tma(f, tma_inst, tma_items, tma_nitems, tma_bitems, tma_nbitems, cur, unik, p.nz == 1,
-                                 tma_counter, (diag && last) ? diag_partials : nullptr, tma_grid, s, diag_out);
+                                 tma_counter, (diag && last) ? diag_partials : nullptr, tma_grid, s, diag_out,
+                                 tma_tile_y);
       launches += 2;
       if (e != cudaSuccess) return fail_cuda(e, "step2_fp32c_tma launch");
       cur ^= 1;
@@ -340,7 +341,8 @@ bool capaz_ctx::tma_applies() const {
 // step: tensor maps of both state buffers and of K and m, the geometry, dt
 // and S_ref, and the work-item list.
 int capaz_ctx::tma_prepare() {
-  if (tma_ready && tma_dt == p.dt && tma_S_ref == S_ref) return CAPAZ_OK;
+  if (tma_ready && tma_dt == p.dt && tma_S_ref == S_ref && tma_built_tile_y == tma_tile_y) return CAPAZ_OK;
+  const int ty = tma_tile_y;
   InstT h;
   memset(&h, 0, sizeof h);
   const Step2Const d = make_step2_const(p);
@@ -348,7 +350,8 @@ int capaz_ctx::tma_prepare() {
   h.ny = p.ny;
   h.nz = p.nz;
   h.tiles_x = d.tiles_x;
-  h.tiles_y = (p.ny - 2 + TMA_TILE_Y - 1) / TMA_TILE_Y;
+  h.tiles_y = (p.ny - 2 + ty - 1) / ty;
+  h.tile_y = ty;
   h.source = p.source;
   window_k(p, &h.win_k0, &h.win_k1);
   h.sy = d.sy;
@@ -367,18 +370,19 @@ int capaz_ctx::tma_prepare() {
   h.dt_f = (float)p.dt;
   h.sgr_dev_f = (float)(p.S_n_gr - S_ref);
   h.nbound = boundary_cells(p.nx, p.ny, p.nz);
+  h.test_tx_extra = (p.flags & CAPAZ_FLAG_TEST_WAIT_TIMEOUT) ? 16u : 0u;
   h.S_ref = S_ref;
   h.dt = p.dt;
   h.rowF = rowF;
   h.Pref = Pref;
   for (int b = 0; b < 2; b++) {
-    if (encode_field_map(&h.map_p[b], (const float*)state[b][0], p.nx, p.ny, p.nz) ||
-        encode_field_map(&h.map_s[b], (const float*)state[b][1], p.nx, p.ny, p.nz))
+    if (encode_field_map(&h.map_p[b], (const float*)state[b][0], p.nx, p.ny, p.nz, ty) ||
+        encode_field_map(&h.map_s[b], (const float*)state[b][1], p.nx, p.ny, p.nz, ty))
       return fail_msg(CAPAZ_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   }
-  if (encode_field_map(&h.map_m, (const float*)m, p.nx, p.ny, p.nz))
+  if (encode_field_map(&h.map_m, (const float*)m, p.nx, p.ny, p.nz, ty))
     return fail_msg(CAPAZ_ERR_CUDA, "cuTensorMapEncodeTiled failed (m)");
-  if (K && encode_field_map(&h.map_K, (const float*)K, p.nx, p.ny, p.nz))
+  if (K && encode_field_map(&h.map_K, (const float*)K, p.nx, p.ny, p.nz, ty))
     return fail_msg(CAPAZ_ERR_CUDA, "cuTensorMapEncodeTiled failed (K)");
   if (!K) h.map_K = h.map_m;  // unused (uniform K)
   for (int b = 0; b < 2; b++) {
@@ -411,19 +415,32 @@ int capaz_ctx::tma_prepare() {
   }
   e = cudaMemcpy(tma_inst, &h, sizeof h, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy(tma descriptor)");
-  if (!tma_items) {
+  if (!tma_items || tma_built_tile_y != ty) {
     // Items ordered z-chunk-major: CTAs that run together work on the same
     // z range, so the halos of neighbouring tiles meet in L2.
     const int ntiles = h.tiles_x * h.tiles_y;
     std::vector<int4> items;
     for (int zc = 0; zc < h.nzchunks; zc++)
       for (int t = 0; t < ntiles; t++) items.push_back(make_int4(0, t, zc, 0));
+    if (tma_items && (int)items.size() > tma_nitems) {
+      cudaFree(tma_items);
+      tma_items = nullptr;
+    }
     tma_nitems = (int)items.size();
-    e = cudaMalloc(&tma_items, sizeof(int4) * items.size());
-    if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(items)");
+    if (!tma_items) {
+      e = cudaMalloc(&tma_items, sizeof(int4) * items.size());
+      if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(items)");
+    }
     e = cudaMemcpy(tma_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy(items)");
-    tma_grid = std::min(tma_nitems, step2_fp32c_tma_grid(device, !(p.flags & CAPAZ_FLAG_PERCELL_K)));
+    tma_grid = std::min(tma_nitems, step2_fp32c_tma_grid(device, !(p.flags & CAPAZ_FLAG_PERCELL_K), ty));
+    if (diag_partials && diag_blocks < tma_grid) {
+      // The diagnostics partials are sized for the previous grid.
+      cudaFree(diag_partials);
+      diag_partials = nullptr;
+    }
+  }
+  if (!tma_bitems) {
     std::vector<int2> bitems;
     for (int q = 0; q < h.nbound; q += BOUND_BLOCK) bitems.push_back(make_int2(0, q));
     tma_nbitems = (int)bitems.size();
@@ -434,6 +451,7 @@ int capaz_ctx::tma_prepare() {
   }
   tma_dt = p.dt;
   tma_S_ref = S_ref;
+  tma_built_tile_y = ty;
   tma_ready = true;
   return CAPAZ_OK;
 }

@@ -8,33 +8,33 @@
 //   - persistent CTAs take (instance, tile, z-chunk) work items from a global
 //     counter, so one launch covers one grid or a whole ensemble of uneven
 //     grids without tail waves;
-//   - a tile is 32 x 16 cells; each of the 256 threads owns two cells of a
-//     column (rows ty and ty + 8), which halves the per-cell share of the
-//     plane loop's fixed work and brings the halo down to 96 cells per 512;
-//   - one elected thread streams the raw planes (p, s, K, m) of the tile's
-//     window (a 36 x 18 box at x = 32*ti, a 128-byte-aligned start) into a
-//     3-stage shared-memory ring with cp.async.bulk.tensor (TMA, 3-D tensor
-//     maps, no multicast) completing on mbarriers;
-//   - every thread derives its cells (three warps one halo cell more; the
-//     window's corners are never read) into a 3-slot ring of derived planes,
-//     (p, M_w, M_n) packed as float4, and reads the centre plane and its
-//     -z / +z neighbours from the ring: one barrier per plane, and few enough
-//     registers for three CTAs per SM;
+//   - a tile is 32 x 16 cells, a CTA four warps; each thread owns a column
+//     segment of four cells and keeps their derived values in registers
+//     across planes, so only the x neighbours and the segment ends go
+//     through shared memory (the sweep kernel's comment has the details);
+//   - the raw planes (p, s, K, m) of the tile's window (a 36 x 18 box at
+//     x = 32*ti, a 128-byte-aligned start) stream into a two-stage ring with
+//     cp.async.bulk.tensor (TMA, 3-D tensor maps, no multicast) completing on
+//     mbarriers, issued by a thread of the warp that derives no halo cells;
+//   - 124 registers and 51 KB of shared memory: four CTAs per SM;
 //   - physics constants are kernel parameters (constant-bank operands);
 //     per-row quantities (rho at the row's reference pressure, the scaled
 //     reference-pressure step) come from small per-instance tables.
 // Arithmetic per face (cpu.cpp:236-264 in select form): the driving force
 // x = -dP/h (+ g rho_c on the vertical axis) is evaluated once for both
 // phases; outflow through the + face is x2 * M(upwind), inflow through the
-// - face x1 * M(upwind); the in/out difference of an axis is formed first
-// (exact when the two nearly cancel, by Sterbenz's lemma) and the three axis
-// terms are Kahan-summed, both phases at once in packed f32x2 arithmetic.
-// d(rho S) = -dt/m * div goes to FP64, where one Newton step with the
-// Jacobian at the stored state solves the bilinear system for (dP, dS).
-// Boundary cells are written by a second, small kernel over the boundary
-// shell after the sweep, which keeps the sweep free of per-cell face tests.
-// Waits on mbarriers are bounded; a wait that runs out sets bit 1 of the
-// error flag and the CTA carries on, so the kernel always finishes.
+// - face x1 * M(upwind); the out - in term of an axis is one fused
+// multiply-add and the three axis terms are Kahan-summed, both phases at once
+// in packed f32x2 arithmetic.  d(rho S) = -dt/m * div goes to FP64, where one
+// Newton step with the Jacobian at the stored state solves the bilinear
+// system for (dP, dS).  Boundary cells are written by a second, small kernel
+// over the boundary shell after the sweep, which keeps the sweep free of
+// per-cell face tests.
+// Waits on mbarriers are bounded (about a second of SM clocks).  A wait that
+// runs out in any thread stops the whole CTA: the per-plane barrier votes on
+// it, the CTA sets bit 1 of the error flag, waits (bounded again) for the
+// copies it still has in flight, and leaves its work list; no stage is
+// consumed or re-armed after a timeout, so the kernel always finishes.
 #include <cuda.h>
 #include <math.h>
 #include <stdint.h>
@@ -48,23 +48,30 @@
 namespace capaz {
 namespace {
 
-constexpr int TYK = TMA_TY;        // thread rows of a CTA
-constexpr int NTK = TX * TYK;      // threads of a CTA
-constexpr int TYT = TMA_TILE_Y;    // tile height: each thread row owns two cell rows (ty, ty + TYK)
 constexpr int WX = TX + 2;         // derived-plane window: tile plus a one-cell halo
-constexpr int WY = TYT + 2;
-constexpr int WCELLS = WX * WY;
-constexpr int NHALO = 2 * TX + 2 * TYT;  // halo cells derived by threads 0..NHALO-1 (no corners)
 constexpr int BXW = 36;            // TMA box width (floats): 144 bytes, a multiple of 16
-constexpr int BYW = WY;            // TMA box height
-constexpr int NST = 3;             // planes in flight (raw stages and derived slots)
-constexpr int RAWN = (BXW * BYW + 31) / 32 * 32;  // floats reserved per array per stage (128-B multiple)
-static_assert(BXW * BYW <= RAWN, "raw stage too small");
-static_assert(NHALO <= NTK && 2 * TYT <= 32, "halo cells exceed the block");
-constexpr unsigned long long WAIT_LIMIT = 1ull << 22;  // try_wait polls before giving up
+constexpr long long WAIT_CYCLES = 2000000000ll;  // bounded waits give up after ~1 s of SM clocks
 
+// Geometry of a tile of TYT interior rows (TMA_TILE_SHAPES): the window with
+// its halo, the raw TMA box, the CTA (one warp per four rows) and the CTAs
+// that fit an SM.
+template <int TYT_>
+struct Tile {
+  static constexpr int TYT = TYT_;
+  static constexpr int WY = TYT + 2;
+  static constexpr int WCELLS = WX * WY;
+  static constexpr int NHALO = 2 * TX + 2 * TYT;  // halo cells derived by threads 0..NHALO-1 (no corners)
+  static constexpr int BYW = WY;                  // TMA box height
+  static constexpr int RAWN = (BXW * BYW + 31) / 32 * 32;  // floats per array per stage (128-B multiple)
+  static constexpr int R = 4;                     // cells per thread
+  static constexpr int NW = TYT / R;              // warps per CTA
+  static constexpr int NT = TX * NW;              // threads per CTA
+  static constexpr int MINB = TYT <= 16 ? 4 : 2;  // CTAs per SM the launch bounds aim for
+};
+
+template <int RAWN_>
 struct alignas(128) RawStage {
-  float p[RAWN], s[RAWN], K[RAWN], m[RAWN];
+  float p[RAWN_], s[RAWN_], K[RAWN_], m[RAWN_];
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
@@ -87,6 +94,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// Waits for the completion of phase `par` of a stage barrier; false if it
+// has not completed after WAIT_CYCLES.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t par) {
+  if (mbar_try_wait(bar, par)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, par))
+    if (clock64() - t0 > WAIT_CYCLES) return false;
+  return true;
+}
+__device__ __forceinline__ void st_global(float* p, float v) {
+  asm volatile("st.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
@@ -100,39 +119,6 @@ __device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepco
 
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// Derived values of one cell: pressure deviation and the two phases'
-// mobility-density M = K k_r rho / mu (= -Xi * rho of the reference).
-struct Der {
-  float p, Mw, Mn;
-};
-// The centre cell also needs its saturation deviation, porosity and
-// densities.
-struct Ctr {
-  float s, m, rw, rn;
-};
-
-__device__ __forceinline__ void derive(const PhysF& f, float c1, float Aw, float An, float p, float s, float K,
-                                       Der& d) {
-  // Aw, An: rho_p / mu_p at the row's reference pressure; rho_p(P) / mu_p is
-  // linear in the pressure deviation p.
-  const float S_e = (c1 - s) * f.inv_one_m_swr;
-  const float e2 = S_e * S_e;
-  const float om = 1.f - S_e;
-  const float kw = e2 * e2;
-  const float kn = om * om * (1.f - e2);
-  d.p = p;
-  d.Mw = K * kw * fmaf(f.cw_mu, p, Aw);
-  d.Mn = K * kn * fmaf(f.cn_mu, p, An);
-}
-
-// In/out difference of one axis for one phase: x1, x2 are the scaled driving
-// forces on the - and + faces (positive towards +).
-__device__ __forceinline__ float face_diff(float x1, float x2, float Mc, float Mm, float Mp) {
-  const float out = x2 * (x2 > 0.f ? Mc : Mp);
-  const float in = x1 * (x1 > 0.f ? Mm : Mc);
-  return out - in;
 }
 
 // Two FP32 values in one 64-bit register pair for sm_100's packed f32x2
@@ -162,6 +148,11 @@ __device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
   return d;
 }
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
 
 // Kahan sum of three terms of both phases at once, the first term taken as
 // the start.
@@ -177,15 +168,6 @@ struct Kahan2 {
   __device__ __forceinline__ f32x2 sum() const { return sub2(s, c); }
 };
 
-__device__ __forceinline__ double rcp64(double x) {
-  // FP32 seed refined by one Newton-Raphson step r <- r (2 - x r), which
-  // squares the relative error: 2^-23 -> 2^-46, far below the FP32 storage
-  // of the result.
-  double r = (double)__frcp_rn((float)x);
-  r = r * fma(-x, r, 2.0);
-  return r;
-}
-
 __device__ __forceinline__ bool in_window(const InstT* I, int i, int k) {
   return (i >= I->nx / 2 - I->source) && (i <= I->nx / 2 + I->source) && (k >= I->win_k0) && (k <= I->win_k1);
 }
@@ -199,66 +181,92 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-// Shared memory of one CTA (dynamic, 62 KB: three CTAs per SM).
-struct Smem {
-  RawStage raw[NST];
-  float4 der[NST][WCELLS];  // (p, M_w, M_n, -) of the window, one slot per plane in flight
-  uint64_t bar[NST];
-  float4 rowF[WY];          // (rho_w/mu_w, rho_n/mu_n at the row's P_ref, dP_ref/hy^2 to the next row, -)
-  double rowPrel[WY];       // P_ref - P_atm
-  double rowPref[WY];
-  double red[NTK / 32][4];  // diagnostics reduction
+// The sweep.  A CTA of four warps covers a 32 x 16 tile of interior cells
+// (a 34 x 18 window with its halo); thread (tx, ty) owns the column segment of
+// four cells at x = tx, rows 4 ty .. 4 ty + 3.  Per z-plane, one elected
+// thread of the warp without halo work streams the raw window (p, s, K, m)
+// into a two-stage ring with cp.async.bulk.tensor (3-D tensor maps, no
+// multicast) completing on mbarriers; every thread derives its four cells
+// (three warps also one halo cell each) into registers and into the plane's
+// shared derived slot, as the pair (p, p) and the pair (M_w, M_n) with
+// M = K k_r rho / mu.  After one barrier per plane the thread updates its
+// cells of the plane below: the x neighbours and the segment's two end
+// neighbours come from the shared slot, the vertical neighbours inside the
+// segment and both z neighbours from registers, and the -z inflow of each
+// cell is the +z outflow it computed on the plane below (the same product),
+// carried in registers.  Both phases run in packed f32x2 arithmetic: a face's
+// pressure difference is a (dp, dp) pair, the selected upwind mobilities a
+// (M_w, M_n) pair, the out - in term of an axis one multiply and one fused
+// multiply-add; on the vertical axis the phases' gravity terms are one pair
+// (g rho_p / hy at the centre, minus the reference profile's step, per row).
+// The three axis terms are Kahan-summed per phase.  The FP64 Newton takes the
+// densities from the row's reference densities plus the stored pressure
+// deviation, and its reciprocal from the hardware double-precision estimate
+// refined by one Newton-Raphson step (two with diagnostics).  The plane loop
+// is unrolled by two so the register roles of consecutive planes swap
+// without copies; the three derived slots (planes k - 1, k, k + 1) rotate.
+constexpr int RC_NRAW = 2;               // raw planes in flight
+constexpr int RC_NDER = 3;               // derived planes: read (k-1), written (k), next (k+1)
+template <int TYT>
+struct SmemRC {
+  using TL = Tile<TYT>;
+  RawStage<TL::RAWN> raw[RC_NRAW];
+  ulonglong2 der[RC_NDER][TL::WCELLS];
+  uint64_t bar[RC_NRAW];
+  float4 rowF[TL::WY];
+  double2 rowR[TL::WY];
+  double rowPrel[TL::WY];
+  double red[TL::NW][4];
   int w_sh;
 };
-constexpr size_t kSmemBytes = sizeof(Smem);
 
-#ifndef CAPAZ_TMA_MIN_BLOCKS
-#define CAPAZ_TMA_MIN_BLOCKS 3
-#endif
-template <bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
-__global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
+template <int TYT, bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
+__global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
     step2_fp32c_tma_kernel(const __grid_constant__ PhysF f, const InstT* __restrict__ insts,
-                           const int4* __restrict__ items, int nitems, int parity, unsigned int* __restrict__ counter,
-                           double* __restrict__ diag_partials) {
+                          const int4* __restrict__ items, int nitems, int parity, unsigned int* __restrict__ counter,
+                          double* __restrict__ diag_partials) {
+  using TL = Tile<TYT>;
+  constexpr int WY = TL::WY, NHALO = TL::NHALO, BYW = TL::BYW, RC_R = TL::R, RC_TY = TL::NW, RC_NT = TL::NT;
+  static_assert(NHALO <= RC_NT - 32, "a warp without halo work issues the copies");
   extern __shared__ __align__(128) unsigned char smem_bytes[];
-  Smem& sm = *reinterpret_cast<Smem*>(smem_bytes);
+  SmemRC<TYT>& sm = *reinterpret_cast<SmemRC<TYT>*>(smem_bytes);
+  constexpr int ISS = RC_NT - 32;  // issuer: the first thread of the last warp, which derives no halo cells
 
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + TX * ty;
-  if (tid == 0) {
-    for (int q = 0; q < NST; q++) mbar_init(&sm.bar[q], 1);
+  if (tid == ISS) {
+    for (int q = 0; q < RC_NRAW; q++) mbar_init(&sm.bar[q], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  uint32_t phase = 0;  // bit q: parity of the next completion of stage q
+  uint32_t phase = 0;
+  uint32_t armed = 0;
+  bool stopped = false;
 
-  // The thread's two cells are tile rows ty and ty + TYK (window rows +1).
-  const int ownA = (ty + 1) * WX + (tx + 1), ownB = ownA + TYK * WX;
-  const int rawA = (ty + 1) * BXW + (tx + 1), rawB = rawA + TYK * BXW;
-  // Halo cells of the 7-point stencil (the window's corners are never read):
-  // warp 0 the row above the tile, warp 1 the row below, warp 2 the columns
-  // left (lanes 0-15) and right (lanes 16-31).
+  const int own0 = (RC_R * ty + 1) * WX + (tx + 1);   // window index of the segment's first cell
+  const int raw0 = (RC_R * ty + 1) * BXW + (tx + 1);
   int halo_slot = -1, halo_raw = 0, halo_row = 0;
   if (tid < NHALO) {
-    const int wq = tid >> 5, lane = tid & 31;
+    // Halo cells of the 7-point stencil (the window's corners are never
+    // read): the row above the tile, the row below, the left column, the
+    // right column.
     int hx, hy;
-    if (wq == 0) hx = lane + 1, hy = 0;
-    else if (wq == 1) hx = lane + 1, hy = WY - 1;
-    else if (lane < TYT) hx = 0, hy = lane + 1;
-    else hx = WX - 1, hy = lane - TYT + 1;
+    if (tid < TX) hx = tid + 1, hy = 0;
+    else if (tid < 2 * TX) hx = tid - TX + 1, hy = WY - 1;
+    else if (tid < 2 * TX + TYT) hx = 0, hy = tid - 2 * TX + 1;
+    else hx = WX - 1, hy = tid - 2 * TX - TYT + 1;
     halo_slot = hy * WX + hx;
     halo_raw = hy * BXW + hx;
     halo_row = hy;
   }
+  const f32x2 CR = pack2(f.cw_mu, f.cn_mu);
+  const f32x2 CG = pack2(f.g_mu_w * f.cw_mu, f.g_mu_n * f.cn_mu);
+  const f32x2 HX2 = pack2(f.inv_hx2, f.inv_hx2), HY2 = pack2(f.inv_hy2, f.inv_hy2), HZ2 = pack2(f.inv_hz2, f.inv_hz2);
 
   double acc_w = 0., acc_n = 0., nonfinite = 0.;
   float rmax = 0.f;
-  // Diagnostics: masses summed without the cell volume (applied once per
-  // CTA), residuals scaled by 1/rho_0.
   const float iro0w_f = DIAG ? (float)(1. / f.ro0_w) : 0.f, iro0n_f = DIAG ? (float)(1. / f.ro0_n) : 0.f;
   const float aw_ro0w_f = DIAG ? (float)(f.aw / f.ro0_w) : 0.f, bn_ro0n_f = DIAG ? (float)(f.bn / f.ro0_n) : 0.f;
-  // Everything above overlaps the previous kernel's tail; the work counter and
-  // the state are touched only after it has completed.
   grid_dependency_wait();
 
   for (;;) {
@@ -266,15 +274,13 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
     __syncthreads();
     const int w = sm.w_sh;
     if (w >= nitems) {
-      // No work left for this CTA: the boundary kernel may be scheduled (it
-      // waits for the whole sweep with griddepcontrol.wait).
       asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
       break;
     }
     const int4 it = items[w];
     const InstT* __restrict__ I = insts + it.x;
     const int nx = I->nx, ny = I->ny, nz = I->nz;
-    const int sy32 = (int)I->sy, sz32 = (int)I->sz;  // instances hold < 2^31 cells
+    const int sy32 = (int)I->sy, sz32 = (int)I->sz;
     const float c1 = I->c1_f;
     const float dt_f = I->dt_f;
     const double S_ref = I->S_ref;
@@ -285,123 +291,142 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
     const int tile = it.y, zc = it.z;
     const int ti = tile % I->tiles_x, tj = tile / I->tiles_x;
     const int i0 = 1 + ti * TX, j0 = 1 + tj * TYT;
-    const int x0 = i0 - 1;  // == 32 * ti: 128-byte aligned TMA start
-    const int i = i0 + tx, jA = j0 + ty, jB = jA + TYK;
-    const bool activeA = (i <= nx - 2) && (jA <= ny - 2);
-    const bool activeB = (i <= nx - 2) && (jB <= ny - 2);
-    const int lA0 = i + jA * sy32;
+    const int x0 = i0 - 1;
+    const int i = i0 + tx, jS = j0 + RC_R * ty;  // the segment's first row
+    unsigned active = 0;
+#pragma unroll
+    for (int r = 0; r < RC_R; r++)
+      if (i <= nx - 2 && jS + r <= ny - 2) active |= 1u << r;
+    const int l0 = i + jS * sy32;
     bool bad = false;
+    float chk = 0.f;  // sum of |p| + |s| of the written cells (non-diagnostic steps)
     const int kb = PLANAR ? 0 : 1 + zc * I->zchunk;
-    const int ke = PLANAR ? 0 : min(kb + I->zchunk, nz - 1);  // last plane loaded
-    const int pb = PLANAR ? 0 : kb - 1;                         // first plane loaded
-    const uint32_t stage_bytes = (UNIK ? 3u : 4u) * (uint32_t)(BXW * BYW * sizeof(float));
+    const int ke = PLANAR ? 0 : min(kb + I->zchunk, nz - 1);
+    const int pb = PLANAR ? 0 : kb - 1;
+    const uint32_t stage_bytes = (UNIK ? 3u : 4u) * (uint32_t)(BXW * BYW * sizeof(float)) + I->test_tx_extra;
 
     if (tid < WY) {
       const int gj = min(j0 - 1 + tid, ny - 1);
+      const double prel = I->Pref[gj] - f.P_atm;
       sm.rowF[tid] = I->rowF[gj];
-      sm.rowPrel[tid] = I->Pref[gj] - f.P_atm;
-      sm.rowPref[tid] = I->Pref[gj];
+      sm.rowR[tid] = make_double2(fma(f.aw, prel, f.ro0_w), fma(f.bn, prel, f.ro0_n));
+      sm.rowPrel[tid] = prel;
     }
-    if (tid == 0) {
-      for (int q = 0; q < NST && pb + q <= ke; q++) {
-        const int pl = pb + q;
-        mbar_expect_tx(&sm.bar[q], stage_bytes);
-        tma_load_3d(sm.raw[q].p, &I->map_p[parity], x0, j0 - 1, pl, &sm.bar[q]);
-        tma_load_3d(sm.raw[q].s, &I->map_s[parity], x0, j0 - 1, pl, &sm.bar[q]);
-        if (!UNIK) tma_load_3d(sm.raw[q].K, &I->map_K, x0, j0 - 1, pl, &sm.bar[q]);
-        tma_load_3d(sm.raw[q].m, &I->map_m, x0, j0 - 1, pl, &sm.bar[q]);
-      }
-    }
+    auto issue = [&](int q, int pl) {
+      mbar_expect_tx(&sm.bar[q], stage_bytes);
+      armed |= 1u << q;
+      tma_load_3d(sm.raw[q].p, &I->map_p[parity], x0, j0 - 1, pl, &sm.bar[q]);
+      tma_load_3d(sm.raw[q].s, &I->map_s[parity], x0, j0 - 1, pl, &sm.bar[q]);
+      if (!UNIK) tma_load_3d(sm.raw[q].K, &I->map_K, x0, j0 - 1, pl, &sm.bar[q]);
+      tma_load_3d(sm.raw[q].m, &I->map_m, x0, j0 - 1, pl, &sm.bar[q]);
+    };
+    if (tid == ISS)
+      for (int q = 0; q < RC_NRAW && pb + q <= ke; q++) issue(q, pb + q);
     __syncthreads();
-    const float4 rowA = sm.rowF[ty + 1], rowB = sm.rowF[ty + TYK + 1];
-    const float dnA = sm.rowF[ty].z, dnB = sm.rowF[ty + TYK].z;
+    // Row pairs of the segment's rows (see the packed sweep).
+    f32x2 AR[RC_R], G1[RC_R], G2[RC_R];
+#pragma unroll
+    for (int r = 0; r < RC_R; r++) {
+      const int wr = RC_R * ty + 1 + r;
+      const float4 rw = sm.rowF[wr];
+      const float dn = sm.rowF[wr - 1].z;
+      const float gw = f.g_mu_w * rw.x, gn = f.g_mu_n * rw.y;
+      AR[r] = pack2(rw.x, rw.y);
+      G1[r] = pack2(gw - dn, gn - dn);
+      G2[r] = pack2(gw - rw.z, gn - rw.z);
+    }
 
-    // The centre-plane update of one cell: D holds the centre plane, Dm / Dp
-    // the planes below and above it; sc, mc are the cell's saturation
-    // deviation and porosity.
-    auto update = [&](const float4* __restrict__ D, const float4* __restrict__ Dm, const float4* __restrict__ Dp,
-                      int own, float4 row, float dPs_dn, int wrow, float sc, float mc, int l, bool active) {
-      const float4 c4 = D[own];
-      const Der C0{c4.x, c4.y, c4.z};
-      f32x2 D2;  // (div F_w, div F_n)
-      {
-        const float4 a = D[own - 1], b = D[own + 1];
-        // Forces: pressure differences of neighbours (exact when they are
-        // close), scaled by 1/h^2 unless the spacing is 1.
-        const float x1 = UNITH ? a.x - C0.p : (a.x - C0.p) * f.inv_hx2;
-        const float x2 = UNITH ? C0.p - b.x : (C0.p - b.x) * f.inv_hx2;
-        const bool u1 = x1 > 0.f, u2 = x2 > 0.f;
-        const float dxw = x2 * (u2 ? C0.Mw : b.y) - x1 * (u1 ? a.y : C0.Mw);
-        const float dxn = x2 * (u2 ? C0.Mn : b.z) - x1 * (u1 ? a.z : C0.Mn);
-        // y (vertical, gravity): P(j+1) - P(j) = dP_ref(j) + p(j+1) - p(j)
-        const float4 ya = D[own - WX], yb = D[own + WX];
-        const float gw = f.g_mu_w * fmaf(f.cw_mu, C0.p, row.x), gn = f.g_mu_n * fmaf(f.cn_mu, C0.p, row.y);
-        const float y1 = UNITH ? (ya.x - C0.p) - dPs_dn : fmaf(ya.x - C0.p, f.inv_hy2, -dPs_dn);
-        const float y2 = UNITH ? (C0.p - yb.x) - row.z : fmaf(C0.p - yb.x, f.inv_hy2, -row.z);
-        const float dyw = face_diff(y1 + gw, y2 + gw, C0.Mw, ya.y, yb.y);
-        const float dyn = face_diff(y1 + gn, y2 + gn, C0.Mn, ya.z, yb.z);
-        Kahan2 k(pack2(dxw, dxn));
-        k.add(pack2(dyw, dyn));
-        if (!PLANAR) {
-          const float4 m4 = Dm[own], p4 = Dp[own];
-          const Der m1{m4.x, m4.y, m4.z}, p1{p4.x, p4.y, p4.z};
-          const float z1 = UNITH ? m1.p - C0.p : (m1.p - C0.p) * f.inv_hz2;
-          const float z2 = UNITH ? C0.p - p1.p : (C0.p - p1.p) * f.inv_hz2;
-          const bool v1 = z1 > 0.f, v2 = z2 > 0.f;
-          k.add(pack2(z2 * (v2 ? C0.Mw : p1.Mw) - z1 * (v1 ? m1.Mw : C0.Mw),
-                      z2 * (v2 ? C0.Mn : p1.Mn) - z1 * (v1 ? m1.Mn : C0.Mn)));
-        }
-        D2 = k.sum();
+    auto derive_cell = [&](f32x2 ARr, float p, float sv, float K) -> ulonglong2 {
+      const float S_e = (c1 - sv) * f.inv_one_m_swr;
+      const float e2 = S_e * S_e;
+      const float om = 1.f - S_e;
+      const float kw = e2 * e2;
+      const float kn = om * om * (1.f - e2);
+      const f32x2 PP = pack2(p, p);
+      const f32x2 MM = mul2(pack2(K * kw, K * kn), fma2(CR, PP, ARr));
+      return make_ulonglong2(PP, MM);
+    };
+    auto xaxis = [&](ulonglong2 c, ulonglong2 a, ulonglong2 b) -> f32x2 {
+      f32x2 X2 = sub2(c.x, b.x), N1 = sub2(c.x, a.x);
+      if (!UNITH) {
+        X2 = mul2(X2, HX2);
+        N1 = mul2(N1, HX2);
       }
-      // Conserved increments d(rho S) = -dt/m * div F (FP32), Newton in FP64.
+      float x2, n1, t;
+      unpack2(X2, x2, t);
+      unpack2(N1, n1, t);
+      const f32x2 S2 = x2 > 0.f ? c.y : b.y;
+      const f32x2 S1 = n1 < 0.f ? a.y : c.y;
+      return fma2(N1, S1, mul2(X2, S2));
+    };
+    auto zflux = [&](ulonglong2 c, ulonglong2 b) -> f32x2 {
+      f32x2 X2 = sub2(c.x, b.x);
+      if (!UNITH) X2 = mul2(X2, HZ2);
+      float x2, t;
+      unpack2(X2, x2, t);
+      return mul2(X2, x2 > 0.f ? c.y : b.y);
+    };
+    auto yaxis = [&](ulonglong2 c, ulonglong2 ya, ulonglong2 yb, f32x2 g1, f32x2 g2) -> f32x2 {
+      f32x2 E2 = sub2(c.x, yb.x), E1 = sub2(c.x, ya.x);
+      if (!UNITH) {
+        E2 = mul2(E2, HY2);
+        E1 = mul2(E1, HY2);
+      }
+      const f32x2 Y2 = add2(E2, fma2(CG, c.x, g2));
+      const f32x2 N1 = sub2(E1, fma2(CG, c.x, g1));
+      float y2w, y2n, n1w, n1n, cw, cn, bw, bn_, aw_, an_;
+      unpack2(Y2, y2w, y2n);
+      unpack2(N1, n1w, n1n);
+      unpack2(c.y, cw, cn);
+      unpack2(yb.y, bw, bn_);
+      unpack2(ya.y, aw_, an_);
+      const f32x2 S2 = pack2(y2w > 0.f ? cw : bw, y2n > 0.f ? cn : bn_);
+      const f32x2 S1 = pack2(n1w < 0.f ? aw_ : cw, n1n < 0.f ? an_ : cn);
+      return fma2(N1, S1, mul2(Y2, S2));
+    };
+    // The Newton recovery of one cell from its flux difference pair D2.
+    auto finish = [&](ulonglong2 c, f32x2 D2, int r, float sc, float mc, int l, bool act) {
+      float pc, t0;
+      unpack2(c.x, pc, t0);
       const float dtm = __fdividef(dt_f, mc);
       float Awf, Anf;
       unpack2(mul2(pack2(-dtm, -dtm), D2), Awf, Anf);
-      const double Aw = (double)Awf;
-      const double An = (double)Anf;
-      const double S = S_ref + (double)sc;
-      const double prel = sm.rowPrel[wrow];
-      const double pr = prel + (double)C0.p;
-      const double rw = fma(f.aw, pr, f.ro0_w);
-      const double rn = fma(f.bn, pr, f.ro0_n);
-      const double J11 = f.aw * (1. - S), J21 = f.bn * S;
-      const double det = fma(J11, rn, rw * J21);  // J11 J22 - J12 J21, J12 = -rw, J22 = rn
-      const double inv = rcp64(det);
-      // One Newton step from the stored state: the Jacobian solve of the
-      // bilinear system, exact up to the dP*dS terms (relative size
-      // |dS| / S ~ 1e-8 of the increments).
-      const double dP = (rn * Aw + rw * An) * inv;
-      const double dS = (J11 * An - J21 * Aw) * inv;
-      float rf = 0.f;
+      const double Aw = (double)Awf, An = (double)Anf;
+      const double pd = (double)pc, sd = (double)sc;
+      const double2 rr = sm.rowR[RC_R * ty + 1 + r];
+      const double rw = fma(f.aw, pd, rr.x);
+      const double rn = fma(f.bn, pd, rr.y);
+      const double S = S_ref + sd;
+      const double J11 = fma(-f.aw, S, f.aw), J21 = f.bn * S;
+      const double det = fma(J11, rn, rw * J21);
+      double inv;
+      asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(inv) : "d"(det));
+      inv = fma(inv, fma(-det, inv, 1.), inv);
+      if (DIAG) inv = fma(inv, fma(-det, inv, 1.), inv);
+      const double dP = fma(rn, Aw, rw * An) * inv;
+      const double dS = fma(J11, An, -(J21 * Aw)) * inv;
+      const float pn = (float)(pd + dP);
+      const float snew = (float)(sd + dS);
+      if (act) {
+        st_global(p_out + l, pn);
+        st_global(s_out + l, snew);
+      }
+      bool finite = true;
       if (DIAG) {
-        // The reference's Newton functions at (dP, dS),
-        //   F1 = (rw + a_w dP)(1 - S - dS) - rw (1 - S) - Aw,
-        //   F2 = (rn + b_n dP)(S + dS) - rn S - An,
-        // are, for the solve above, exactly F1 = Aw e - a_w dP dS and
-        // F2 = An e + b_n dP dS with e = det * inv - 1 (the linear part
-        // leaves Aw e, An e).  Written so they have no cancellation left;
-        // FP32 holds their size (~1e-14 of Aw) to 1e-7, and they are
-        // reported scaled by 1/rho_0.
+        finite = isfinite(pn) && isfinite(snew);
+        bad |= act && !finite;
+      } else if (act) {
+        chk += fabsf(pn) + fabsf(snew);  // not finite (or beyond FLT_MAX) once any term is
+      }
+      if (DIAG && act) {
         const float e = (float)fma(det, inv, -1.);
         const float q = (float)(dP * dS);
         const float F1 = fmaf(Awf * iro0w_f, e, -aw_ro0w_f * q);
         const float F2 = fmaf(Anf * iro0n_f, e, bn_ro0n_f * q);
-        rf = fmaxf(fabsf(F1), fabsf(F2));
-      }
-      const float pn = (float)((double)C0.p + dP);
-      const float snew = (float)((double)sc + dS);
-      // Cells beyond the grid's interior (partial tiles) compute on the
-      // window's fill values and store nothing.
-      if (active) {
-        p_out[l] = pn;
-        s_out[l] = snew;
-      }
-      const bool finite = isfinite(pn) && isfinite(snew);
-      bad |= active && !finite;
-      if (DIAG && active) {
+        const float rf = fmaxf(fabsf(F1), fabsf(F2));
         const double md = (double)mc;
-        const double mS1 = md * (S_ref + (double)snew);  // m S_n; m (1 - S_n) = m - m S_n
-        const double P1rel = prel + (double)pn;
+        const double mS1 = md * (S_ref + (double)snew);
+        const double P1rel = sm.rowPrel[RC_R * ty + 1 + r] + (double)pn;
         acc_w = fma(md - mS1, fma(f.aw, P1rel, f.ro0_w), acc_w);
         acc_n = fma(mS1, fma(f.bn, P1rel, f.ro0_n), acc_n);
         if (!(rf <= rmax)) rmax = rf;
@@ -409,99 +434,125 @@ __global__ void __launch_bounds__(NTK, CAPAZ_TMA_MIN_BLOCKS)
       }
     };
 
-    // The sweep: plane pl is derived into ring slot u = (pl - pb) mod 3 while
-    // the centre plane pl - 1 is updated from the slots of pl - 2, pl - 1, pl.
-    // Unrolled by three so that every slot index is a compile-time constant.
-    float sA0 = 0.f, mA0 = 0.f, sB0 = 0.f, mB0 = 0.f;  // centre plane's s, m of the two cells
-    auto plane = [&](auto U, int pl) {
-      constexpr int u = decltype(U)::value;
-      {  // wait for the plane (bounded)
-        const uint32_t par = (phase >> u) & 1u;
-        unsigned long long tries = 0;
-        while (!mbar_try_wait(&sm.bar[u], par)) {
-          if (++tries > WAIT_LIMIT) {
-            atomicOr(err, 2u);
-            break;
-          }
-        }
-        phase ^= (1u << u);
+    // Derived cells of two consecutive planes in registers: planes pb, pb + 2,
+    // ... in X0, the others in X1 (the loop is unrolled by two, so the
+    // centre and next-plane roles swap without copies); likewise s and m.
+    static_assert(RC_NRAW == 2, "the unrolled plane loop alternates two raw stages");
+    ulonglong2 X0[RC_R], X1[RC_R];
+    f32x2 Zin[RC_R];                     // -z inflow pairs of the centre cells
+    float s0[RC_R], m0[RC_R], s1[RC_R], m1[RC_R];
+    // Derived slots of planes pl - 1, pl and pl + 1, rotated every plane.
+    ulonglong2* Dr = sm.der[RC_NDER - 1];
+    ulonglong2* Dw = sm.der[0];
+    ulonglong2* Dn = sm.der[1];
+    auto plane = [&](auto T, int pl) -> bool {
+      constexpr int t = decltype(T)::value;  // (pl - pb) mod 2, also plane pl's raw stage
+      ulonglong2(&N)[RC_R] = t ? X1 : X0;
+      ulonglong2(&C)[RC_R] = t ? X0 : X1;
+      float(&sN)[RC_R] = t ? s1 : s0;
+      float(&mN)[RC_R] = t ? m1 : m0;
+      float(&sC)[RC_R] = t ? s0 : s1;
+      float(&mC)[RC_R] = t ? m0 : m1;
+      const bool landed = mbar_wait_bounded(&sm.bar[t], (phase >> t) & 1u);
+      if (landed) {
+        phase ^= (1u << t);
+        armed &= ~(1u << t);
       }
-      const RawStage& R = sm.raw[u];
-      float4* __restrict__ D = sm.der[u];
-      float sA1, mA1, sB1, mB1;
       {
-        Der dA, dB;
-        sA1 = R.s[rawA];
-        sB1 = R.s[rawB];
-        mA1 = R.m[rawA];
-        mB1 = R.m[rawB];
-        derive(f, c1, rowA.x, rowA.y, R.p[rawA], sA1, UNIK ? f.K0 : R.K[rawA], dA);
-        derive(f, c1, rowB.x, rowB.y, R.p[rawB], sB1, UNIK ? f.K0 : R.K[rawB], dB);
-        D[ownA] = make_float4(dA.p, dA.Mw, dA.Mn, 0.f);
-        D[ownB] = make_float4(dB.p, dB.Mw, dB.Mn, 0.f);
+        const auto& R = sm.raw[t];
+#pragma unroll
+        for (int r = 0; r < RC_R; r++) {
+          const int ri = raw0 + r * BXW;
+          sN[r] = R.s[ri];
+          mN[r] = R.m[ri];
+          N[r] = derive_cell(AR[r], R.p[ri], sN[r], UNIK ? f.K0 : R.K[ri]);
+          Dw[own0 + r * WX] = N[r];
+        }
+        if (halo_slot >= 0) {
+          const float4 rh = sm.rowF[halo_row];
+          Dw[halo_slot] = derive_cell(pack2(rh.x, rh.y), R.p[halo_raw], R.s[halo_raw], UNIK ? f.K0 : R.K[halo_raw]);
+        }
       }
-      if (halo_slot >= 0) {
-        const float4 rh = sm.rowF[halo_row];
-        Der h;
-        derive(f, c1, rh.x, rh.y, R.p[halo_raw], R.s[halo_raw], UNIK ? f.K0 : R.K[halo_raw], h);
-        D[halo_slot] = make_float4(h.p, h.Mw, h.Mn, 0.f);
+      if (__syncthreads_or(!landed)) {
+        if (tid == ISS) {
+          atomicOr(err, 2u);
+          for (int qq = 0; qq < RC_NRAW; qq++)
+            if (armed & (1u << qq)) mbar_wait_bounded(&sm.bar[qq], (phase >> qq) & 1u);
+        }
+        __syncthreads();
+        return true;
       }
-      __syncthreads();
-      // Stage u has been read by every thread: refill it three planes ahead.
-      if (tid == 0 && pl + NST <= ke) {
+      if (tid == ISS && pl + RC_NRAW <= ke) {
         fence_proxy_async();
-        const int nxt = pl + NST;
-        mbar_expect_tx(&sm.bar[u], stage_bytes);
-        tma_load_3d(sm.raw[u].p, &I->map_p[parity], x0, j0 - 1, nxt, &sm.bar[u]);
-        tma_load_3d(sm.raw[u].s, &I->map_s[parity], x0, j0 - 1, nxt, &sm.bar[u]);
-        if (!UNIK) tma_load_3d(sm.raw[u].K, &I->map_K, x0, j0 - 1, nxt, &sm.bar[u]);
-        tma_load_3d(sm.raw[u].m, &I->map_m, x0, j0 - 1, nxt, &sm.bar[u]);
+        issue(t, pl + RC_NRAW);
       }
       if (PLANAR) {
-        const int lA = lA0, lB = lA0 + TYK * sy32;
-        update(D, D, D, ownA, rowA, dnA, ty + 1, sA1, mA1, lA, activeA);
-        update(D, D, D, ownB, rowB, dnB, ty + TYK + 1, sB1, mB1, lB, activeB);
+#pragma unroll
+        for (int r = 0; r < RC_R; r++) {
+          const int o = own0 + r * WX;
+          const ulonglong2 c = N[r];
+          const ulonglong2 ya = r == 0 ? Dw[o - WX] : N[r - 1];
+          const ulonglong2 yb = r == RC_R - 1 ? Dw[o + WX] : N[r + 1];
+          Kahan2 k(xaxis(c, Dw[o - 1], Dw[o + 1]));
+          k.add(yaxis(c, ya, yb, G1[r], G2[r]));
+          finish(c, k.sum(), r, sN[r], mN[r], l0 + r * sy32, (active >> r) & 1u);
+        }
+      } else if (pl == pb + 1) {
+#pragma unroll
+        for (int r = 0; r < RC_R; r++) Zin[r] = zflux(C[r], N[r]);  // inflow of plane kb through its -z face
       } else if (pl >= pb + 2) {
-        constexpr int uc = (u + 2) % NST, um = (u + 1) % NST;
-        const int k = pl - 1;
-        const int lA = lA0 + k * sz32, lB = lA + TYK * sy32;
-        update(sm.der[uc], sm.der[um], D, ownA, rowA, dnA, ty + 1, sA0, mA0, lA, activeA);
-        update(sm.der[uc], sm.der[um], D, ownB, rowB, dnB, ty + TYK + 1, sB0, mB0, lB, activeB);
+        // Centre plane pl - 1: x and segment-end neighbours from its shared
+        // slot, the rest from registers.
+        const int lk = l0 + (pl - 1) * sz32;
+#pragma unroll
+        for (int r = 0; r < RC_R; r++) {
+          const int o = own0 + r * WX;
+          const ulonglong2 c = C[r];
+          const ulonglong2 ya = r == 0 ? Dr[o - WX] : C[r - 1];
+          const ulonglong2 yb = r == RC_R - 1 ? Dr[o + WX] : C[r + 1];
+          Kahan2 k(xaxis(c, Dr[o - 1], Dr[o + 1]));
+          k.add(yaxis(c, ya, yb, G1[r], G2[r]));
+          const f32x2 out = zflux(c, N[r]);
+          k.add(sub2(out, Zin[r]));
+          Zin[r] = out;
+          finish(c, k.sum(), r, sC[r], mC[r], lk + r * sy32, (active >> r) & 1u);
+        }
       }
-      sA0 = sA1;
-      mA0 = mA1;
-      sB0 = sB1;
-      mB0 = mB1;
+      ulonglong2* const old = Dr;
+      Dr = Dw;
+      Dw = Dn;
+      Dn = old;
+      return false;
     };
-    for (int base = pb; base <= ke; base += NST) {
-      plane(std::integral_constant<int, 0>{}, base);
+    for (int base = pb; base <= ke; base += 2) {
+      if (plane(std::integral_constant<int, 0>{}, base)) { stopped = true; break; }
       if (base + 1 > ke) break;
-      plane(std::integral_constant<int, 1>{}, base + 1);
-      if (base + 2 > ke) break;
-      plane(std::integral_constant<int, 2>{}, base + 2);
+      if (plane(std::integral_constant<int, 1>{}, base + 1)) { stopped = true; break; }
     }
+    if (stopped) break;
+    if (!DIAG) bad = !(chk <= 3.0e38f);
     if (__any_sync(0xffffffffu, bad) && (tid & 31) == 0) atomicOr(err, 1u);
-    __syncthreads();  // the next item's loads reuse the stages and rows
+    __syncthreads();  // the next item's loads reuse the stages, slots and rows
   }
 
   if (DIAG) {
     double(*red)[4] = sm.red;
     const int lane = tid & 31, wid = tid >> 5;
-    const double s0 = warp_sum(acc_w), s1 = warp_sum(acc_n), r = warp_max((double)rmax), nf = warp_sum(nonfinite);
+    const double s0 = warp_sum(acc_w), s1 = warp_sum(acc_n), rr = warp_max((double)rmax), nf = warp_sum(nonfinite);
     if (lane == 0) {
       red[wid][0] = s0;
       red[wid][1] = s1;
-      red[wid][2] = r;
+      red[wid][2] = rr;
       red[wid][3] = nf;
     }
     __syncthreads();
     if (tid == 0) {
       double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-      for (int q = 0; q < NTK / 32; q++) {
-        t0 += red[q][0];
-        t1 += red[q][1];
-        t2 = fmax(t2, red[q][2]);
-        t3 += red[q][3];
+      for (int qq = 0; qq < RC_TY; qq++) {
+        t0 += red[qq][0];
+        t1 += red[qq][1];
+        t2 = fmax(t2, red[qq][2]);
+        t3 += red[qq][3];
       }
       double* out = diag_partials + (size_t)DIAG_STRIDE * blockIdx.x;
       out[0] = t0 * f.vol;
@@ -617,7 +668,7 @@ cudaError_t launch_dependent(void (*kernel)(Params...), dim3 grid, dim3 block, s
 }
 
 // Opts the kernel into its dynamic shared memory, once per device.
-template <bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
+template <int TYT, bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
 cudaError_t prepare_t() {
   static unsigned long long done = 0;  // bit d: set on device d
   int dev = 0;
@@ -625,78 +676,101 @@ cudaError_t prepare_t() {
   if (e != cudaSuccess) return e;
   const unsigned long long bit = 1ull << (dev & 63);
   if (__atomic_load_n(&done, __ATOMIC_ACQUIRE) & bit) return cudaSuccess;
-  e = cudaFuncSetAttribute(step2_fp32c_tma_kernel<UNIK, DIAG, PLANAR, UNITH>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+  e = cudaFuncSetAttribute(step2_fp32c_tma_kernel<TYT, UNIK, DIAG, PLANAR, UNITH>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SmemRC<TYT>));
   if (e == cudaSuccess) __atomic_fetch_or(&done, bit, __ATOMIC_ACQ_REL);
   return e;
 }
 
-template <bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
+template <int TYT, bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
 cudaError_t launch_t(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
                      unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
-  cudaError_t e = prepare_t<UNIK, DIAG, PLANAR, UNITH>();
+  cudaError_t e = prepare_t<TYT, UNIK, DIAG, PLANAR, UNITH>();
   if (e != cudaSuccess) return e;
-  return launch_dependent(step2_fp32c_tma_kernel<UNIK, DIAG, PLANAR, UNITH>, dim3(grid), dim3(TX, TYK), kSmemBytes,
-                          s, f, insts, items, nitems, parity, counter, diag_partials);
+  return launch_dependent(step2_fp32c_tma_kernel<TYT, UNIK, DIAG, PLANAR, UNITH>, dim3(grid),
+                          dim3(TX, Tile<TYT>::NW), sizeof(SmemRC<TYT>), s, f, insts, items, nitems, parity, counter,
+                          diag_partials);
 }
 
-template <bool UNIK, bool DIAG, bool PLANAR>
+template <int TYT, bool UNIK, bool DIAG, bool PLANAR>
 cudaError_t launch_h(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
                      unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
   // Unit spacing (the workloads' h = 1 m): forces are plain differences.
   const bool unith = f.inv_hx2 == 1.f && f.inv_hy2 == 1.f && f.inv_hz2 == 1.f;
-  return unith ? launch_t<UNIK, DIAG, PLANAR, true>(f, insts, items, nitems, parity, counter, diag_partials, grid, s)
-               : launch_t<UNIK, DIAG, PLANAR, false>(f, insts, items, nitems, parity, counter, diag_partials, grid, s);
+  return unith
+             ? launch_t<TYT, UNIK, DIAG, PLANAR, true>(f, insts, items, nitems, parity, counter, diag_partials, grid, s)
+             : launch_t<TYT, UNIK, DIAG, PLANAR, false>(f, insts, items, nitems, parity, counter, diag_partials, grid,
+                                                        s);
 }
 
-template <bool UNIK, bool DIAG>
-cudaError_t launch_p(bool planar, const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
-                     unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
-  return planar ? launch_h<UNIK, DIAG, true>(f, insts, items, nitems, parity, counter, diag_partials, grid, s)
-                : launch_h<UNIK, DIAG, false>(f, insts, items, nitems, parity, counter, diag_partials, grid, s);
+template <int TYT>
+cudaError_t launch_shape(bool unik, bool planar, const PhysF& f, const InstT* insts, const int4* items, int nitems,
+                         int parity, unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
+  const bool d = diag_partials != nullptr;
+  if (unik) {
+    if (d) return planar ? launch_h<TYT, true, true, true>(f, insts, items, nitems, parity, counter, diag_partials,
+                                                           grid, s)
+                         : launch_h<TYT, true, true, false>(f, insts, items, nitems, parity, counter, diag_partials,
+                                                            grid, s);
+    return planar ? launch_h<TYT, true, false, true>(f, insts, items, nitems, parity, counter, nullptr, grid, s)
+                  : launch_h<TYT, true, false, false>(f, insts, items, nitems, parity, counter, nullptr, grid, s);
+  }
+  if (d) return planar ? launch_h<TYT, false, true, true>(f, insts, items, nitems, parity, counter, diag_partials,
+                                                          grid, s)
+                       : launch_h<TYT, false, true, false>(f, insts, items, nitems, parity, counter, diag_partials,
+                                                           grid, s);
+  return planar ? launch_h<TYT, false, false, true>(f, insts, items, nitems, parity, counter, nullptr, grid, s)
+                : launch_h<TYT, false, false, false>(f, insts, items, nitems, parity, counter, nullptr, grid, s);
 }
 
-}  // namespace
-
-cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems,
-                                   const int2* bitems, int nbitems, int parity, bool unik, bool planar,
-                                   unsigned int* counter, double* diag_partials, int grid, cudaStream_t s,
-                                   double* diag_out) {
-  // `counter` is zero on entry: zeroed at allocation and rearmed by every
-  // boundary launch.
-  cudaError_t e;
-  if (unik)
-    e = diag_partials ? launch_p<true, true>(planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s)
-                      : launch_p<true, false>(planar, f, insts, items, nitems, parity, counter, nullptr, grid, s);
-  else
-    e = diag_partials ? launch_p<false, true>(planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s)
-                      : launch_p<false, false>(planar, f, insts, items, nitems, parity, counter, nullptr, grid, s);
-  if (e != cudaSuccess) return e;
-  return launch_dependent(boundary_fp32c_kernel, dim3(nbitems), dim3(BOUND_BLOCK), 0, s, f, insts, bitems, parity,
-                          counter, (const double*)diag_partials, grid, diag_partials ? diag_out : nullptr);
-}
-
-int step2_fp32c_tma_grid(int device, bool unik) {
+template <int TYT>
+int grid_shape(int device, bool unik) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   int per = 0;
   if (unik) {
-    prepare_t<true, true, false, false>();
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<true, true, false, false>, NTK,
-                                                  kSmemBytes);
+    prepare_t<TYT, true, true, false, false>();
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<TYT, true, true, false, false>,
+                                                  Tile<TYT>::NT, sizeof(SmemRC<TYT>));
   } else {
-    prepare_t<false, true, false, false>();
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<false, true, false, false>, NTK,
-                                                  kSmemBytes);
+    prepare_t<TYT, false, true, false, false>();
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step2_fp32c_tma_kernel<TYT, false, true, false, false>,
+                                                  Tile<TYT>::NT, sizeof(SmemRC<TYT>));
   }
   if (per < 1) per = 1;
   return sms * per;
 }
 
+}  // namespace
+
+bool tma_tile_supported(int tile_y) { return tile_y == 16 || tile_y == 32; }
+
+cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems,
+                                   const int2* bitems, int nbitems, int parity, bool unik, bool planar,
+                                   unsigned int* counter, double* diag_partials, int grid, cudaStream_t s,
+                                   double* diag_out, int tile_y) {
+  // `counter` is zero on entry: zeroed at allocation and rearmed by every
+  // boundary launch.
+  cudaError_t e;
+  if (tile_y == 32)
+    e = launch_shape<32>(unik, planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s);
+  else if (tile_y == 16)
+    e = launch_shape<16>(unik, planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s);
+  else
+    return cudaErrorInvalidValue;
+  if (e != cudaSuccess) return e;
+  return launch_dependent(boundary_fp32c_kernel, dim3(nbitems), dim3(BOUND_BLOCK), 0, s, f, insts, bitems, parity,
+                          counter, (const double*)diag_partials, grid, diag_partials ? diag_out : nullptr);
+}
+
+int step2_fp32c_tma_grid(int device, bool unik, int tile_y) {
+  return tile_y == 32 ? grid_shape<32>(device, unik) : grid_shape<16>(device, unik);
+}
+
 // Builds the 3-D tensor map of one float32 field of an nx x ny x nz grid
-// with the 36 x 10 x 1 box of the kernel.  nx must be a multiple of 4 (row
-// pitch a multiple of 16 bytes).
-int encode_field_map(CUtensorMap* map, const float* base, int nx, int ny, int nz) {
+// with the kernel's 36 x (tile_y + 2) x 1 box.  nx must be a multiple of 4
+// (row pitch a multiple of 16 bytes).
+int encode_field_map(CUtensorMap* map, const float* base, int nx, int ny, int nz, int tile_y) {
   typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -712,7 +786,7 @@ int encode_field_map(CUtensorMap* map, const float* base, int nx, int ny, int nz
   if (nx % 4 != 0) return -2;
   const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
   const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4};
-  const cuuint32_t box[3] = {(cuuint32_t)BXW, (cuuint32_t)BYW, 1};
+  const cuuint32_t box[3] = {(cuuint32_t)BXW, (cuuint32_t)(tile_y + 2), 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)base, dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,

@@ -40,6 +40,7 @@ FLAG_PERCELL_K = 0x1
 FLAG_DIAGNOSTICS = 0x2
 FLAG_SOURCE_WINDOW = 0x4
 FLAG_NO_TMA = 0x8
+FLAG_TEST_WAIT_TIMEOUT = 0x10
 
 ADJ_INIT_FROM_M = 0x1
 
@@ -121,6 +122,7 @@ PROTOTYPES = {
     "capaz_post_diag": (C.c_int, [_VP, C.c_int, _VP]),
     "capaz_wait_diag": (C.c_int, [_VP, C.c_int, C.POINTER(Diag)]),
     "capaz_set_dt": (C.c_int, [_VP, C.c_double]),
+    "capaz_set_sweep_tile": (C.c_int, [_VP, C.c_int]),
     "capaz_launch_count": (C.c_int64, [_VP]),
     "capaz_batch_create": (_VP, [C.POINTER(Params), C.c_int, C.c_int, C.POINTER(C.c_int)]),
     "capaz_batch_destroy": (C.c_int, [_VP]),
@@ -128,6 +130,8 @@ PROTOTYPES = {
     "capaz_batch_step": (C.c_int, [_VP, C.c_int, _VP]),
     "capaz_batch_autotune": (C.c_int, [_VP, _VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "capaz_batch_launch_count": (C.c_int64, [_VP]),
+    "capaz_batch_get_tuning": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "capaz_batch_set_tuning": (C.c_int, [_VP, C.c_int, C.c_int, C.c_int]),
     "capaz_sync": (C.c_int, [_VP]),
     "capaz_get_plane": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),
     "capaz_set_plane": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),

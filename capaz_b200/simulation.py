@@ -141,6 +141,9 @@ class Simulation:
     def set_dt(self, dt: float) -> None:
         check(self.lib.capaz_set_dt(self.ctx, float(dt)), self.ctx)
 
+    def set_sweep_tile(self, tile_y: int) -> None:
+        check(self.lib.capaz_set_sweep_tile(self.ctx, int(tile_y)), self.ctx)
+
     def diag(self, stream: int = 0) -> dict:
         d = Diag()
         check(self.lib.capaz_read_diag(self.ctx, C.byref(d), stream or None), self.ctx)
@@ -218,9 +221,16 @@ class Ensemble:
         check(self.lib.capaz_batch_step(self.b, int(nsteps), stream or None))
 
     def autotune(self, stream: int = 0) -> dict:
-        zc, per = C.c_int(0), C.c_int(0)
-        check(self.lib.capaz_batch_autotune(self.b, stream or None, C.byref(zc), C.byref(per)))
-        return {"zchunk": zc.value, "ctas_per_sm": per.value}
+        check(self.lib.capaz_batch_autotune(self.b, stream or None, None, None))
+        return self.tuning()
+
+    def tuning(self) -> dict:
+        zc, per, ty = C.c_int(0), C.c_int(0), C.c_int(0)
+        check(self.lib.capaz_batch_get_tuning(self.b, C.byref(zc), C.byref(per), C.byref(ty)))
+        return {"zchunk": zc.value, "ctas_per_sm": per.value, "tile": [32, ty.value] if ty.value else None}
+
+    def set_tuning(self, zchunk: int, ctas_per_sm: int = 0, tile_y: int = 16) -> None:
+        check(self.lib.capaz_batch_set_tuning(self.b, int(zchunk), int(ctas_per_sm), int(tile_y)))
 
     @property
     def launch_count(self) -> int:

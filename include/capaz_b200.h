@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define CAPAZ_ABI_VERSION 4
+#define CAPAZ_ABI_VERSION 5
 
 /* ---- status codes ------------------------------------------------------ */
 enum capaz_status {
@@ -71,6 +71,12 @@ enum capaz_form {
 /* Precision form: use the plain-load kernel even where the TMA-staged one
  * applies (nx a multiple of 4).  For comparisons and tests. */
 #define CAPAZ_FLAG_NO_TMA 0x8u
+/* Test only.  The TMA-staged precision sweep announces 16 bytes more per
+ * plane than its copies bring, so every CTA's first bounded wait runs out
+ * (about a second): the CTA stops its work, waits (bounded) for its copies
+ * in flight and exits, and the step reports CAPAZ_ERR_CUDA.  Exercises the
+ * timeout path without a fault or a hang. */
+#define CAPAZ_FLAG_TEST_WAIT_TIMEOUT 0x10u
 
 /*
  * Physical and numerical parameters: the subset of the reference's `consts`
@@ -267,6 +273,11 @@ int capaz_wait_diag(capaz_ctx* ctx, int slot, capaz_diag* out);
 /* Sets dt for the following steps (a per-step parameter in the reference:
  * consts.dt); host value, no device traffic beyond the kernel argument. */
 int capaz_set_dt(capaz_ctx* ctx, double dt);
+/* Precision form with the TMA-staged sweep: rows of the sweep's tile, 16
+ * (default; four warps per CTA, four CTAs per SM) or 32 (eight warps, two
+ * CTAs per SM).  The result does not depend on it.  CAPAZ_ERR_UNSUPPORTED
+ * for other values. */
+int capaz_set_sweep_tile(capaz_ctx* ctx, int tile_y);
 
 /* ---- ensembles ----------------------------------------------------------
  * A batch steps `count` independent two-phase instances of uneven grid
@@ -284,11 +295,18 @@ capaz_batch* capaz_batch_create(const capaz_params* params, int count, int devic
 int capaz_batch_destroy(capaz_batch* b);
 capaz_ctx* capaz_batch_instance(capaz_batch* b, int index);
 int capaz_batch_step(capaz_batch* b, int nsteps, void* stream);
-/* Times candidate launch shapes (z-chunk depth, CTAs per SM) on the batch's
+/* Times candidate launch shapes (z-chunk depth, CTAs per SM and, for the
+ * precision form, the sweep's tile: 32 x 16 or 32 x 32 cells) on the batch's
  * own data for a few steps each, keeps the fastest, and restores every
  * instance's state afterwards.  Writes the choice to zchunk / ctas_per_sm
- * (either may be NULL). */
+ * (either may be NULL; capaz_batch_get_tuning also returns the tile). */
 int capaz_batch_autotune(capaz_batch* b, void* stream, int* zchunk, int* ctas_per_sm);
+/* The batch's launch shape: z-chunk depth, CTAs per SM (0: as many as fit)
+ * and the precision form's tile rows (16 or 32; 0 for FP64 batches). */
+int capaz_batch_get_tuning(const capaz_batch* b, int* zchunk, int* ctas_per_sm, int* tile_y);
+/* Sets the launch shape directly (tile_y is ignored for FP64 batches);
+ * CAPAZ_ERR_UNSUPPORTED for a tile other than 16 or 32 rows. */
+int capaz_batch_set_tuning(capaz_batch* b, int zchunk, int ctas_per_sm, int tile_y);
 int64_t capaz_batch_launch_count(const capaz_batch* b);
 
 /* Number of kernels the library launched on this context so far. */

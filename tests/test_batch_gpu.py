@@ -42,6 +42,7 @@ def test_batch_autotune_keeps_state():
         before = [s.get_field("S_n") for s in ens.instances]
         choice = ens.autotune()
         assert choice["zchunk"] in (8, 16, 32, 64) and choice["ctas_per_sm"] >= 1
+        assert choice["tile"] in ([32, 16], [32, 32])
         after = [s.get_field("S_n") for s in ens.instances]
         for a, b in zip(before, after):
             assert np.array_equal(a, b)
@@ -52,3 +53,45 @@ def test_batch_autotune_keeps_state():
             setup(s, w)
             s.step(10)
             assert np.array_equal(s.get_field("S_n"), S)
+
+
+@pytest.mark.parametrize("tile_y,zchunk,per", [(16, 16, 0), (32, 16, 0), (32, 8, 1), (16, 64, 2)])
+def test_batch_tile_shapes_match_individual_runs(tile_y, zchunk, per):
+    """Every sweep tile shape the autotuner chooses among (32 x 16 and
+    32 x 32 cells) gives each instance exactly its own run's result."""
+    ws = config3(form=native.FORM_FP32C, seed=8, count=6, dims=(32, 40, 68), steps=9)
+    with Ensemble([w.params for w in ws]) as ens:
+        for sim, w in zip(ens.instances, ws):
+            setup(sim, w)
+        ens.set_tuning(zchunk, per, tile_y)
+        assert ens.tuning() == {"zchunk": zchunk, "ctas_per_sm": per, "tile": [32, tile_y]}
+        ens.step(9)
+        got = [(s.get_field("P_w"), s.get_field("S_n")) for s in ens.instances]
+    for w, (P, S) in zip(ws, got):
+        with Simulation(w.params) as s:
+            setup(s, w)
+            s.step(9)
+            assert np.array_equal(s.get_field("P_w"), P)
+            assert np.array_equal(s.get_field("S_n"), S)
+
+
+def test_sweep_tile_of_one_grid_is_bit_identical():
+    """The precision form's single-grid sweep with 32 x 32 tiles, switched
+    between steps, reproduces the 32 x 16 run bit for bit (ragged tiles in
+    both directions)."""
+    ws = config3(form=native.FORM_FP32C, seed=9, count=1, dims=(100,), steps=6)
+    w = ws[0]
+    out = {}
+    for tiles in ((16, 16, 16), (32, 32, 32), (16, 32, 16)):
+        with Simulation(w.params) as s:
+            setup(s, w)
+            for t in tiles:
+                s.set_sweep_tile(t)
+                s.step(2)
+            out[tiles] = (s.get_field("P_w"), s.get_field("S_n"))
+    ref = out[(16, 16, 16)]
+    for k, (P, S) in out.items():
+        assert np.array_equal(P, ref[0]) and np.array_equal(S, ref[1]), k
+    with Simulation(w.params) as s:
+        with pytest.raises(native.CapazError):
+            s.set_sweep_tile(24)

@@ -150,3 +150,35 @@ def test_fp32c_tma_path_matches_plain_load_path(shape, steps, h):
     for f in ("S_n", "P_w"):
         assert rel_l2(tma[f], ref[f]) <= 1e-6, f
         assert rel_l2(tma[f], plain[f]) <= 1e-6, f
+
+
+def test_tma_wait_timeout_stops_the_step_and_the_process_carries_on():
+    """The TMA-staged sweep's bounded waits: with CAPAZ_FLAG_TEST_WAIT_TIMEOUT
+    each stage announces more bytes than its copies bring, so every CTA's
+    first wait runs out after about a second.  The CTA stops (no stage is
+    consumed or re-armed), lets its copies land, and leaves; the step
+    reports CAPAZ_ERR_CUDA.  Nothing faults or hangs: a fresh context on the
+    same device then steps normally."""
+    import time
+
+    from capaz_b200.native import CapazError
+    p = two_phase_params(64, 40, 48, form=native.FORM_FP32C)
+    m, K = heterogeneous_fields((p.nz, p.ny, p.nx), 1.0, 4.0, 9)
+    p.dt = stable_dt(p, m, K)
+    q = p.copy()
+    q.flags |= native.FLAG_TEST_WAIT_TIMEOUT
+    t0 = time.time()
+    with Simulation(q) as s:
+        s.set_field("m", m)
+        s.set_field("K", K)
+        s.init_state()
+        with pytest.raises(CapazError) as e:
+            s.step(1)
+            s.sync()
+        assert e.value.code == native.ERR_CUDA
+        assert "bounded wait" in str(e.value)
+    assert time.time() - t0 < 60
+    ref = run(p, m, K, 5)
+    st = O.init(p, m)
+    exp = O.step(p, {"P_w": st["P_w"], "S_n": st["S_n"]}, 5, m, K)
+    assert rel_l2(ref["S_n"], exp["S_n"]) <= 1e-6 and rel_l2(ref["P_w"], exp["P_w"]) <= 1e-6
