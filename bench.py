@@ -184,6 +184,17 @@ def load_traffic(kernel: str, workload: str):
         return None
 
 
+def fp64_flops_per_cell(kernel: str):
+    """FP64 operations per cell-step of an FP64 step kernel (DADD + DMUL +
+    2 DFMA thread-instructions per launch / cells, from the committed ncu
+    counts), keyed by kernel and relative-permeability form."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "fp64_ops.json")) as f:
+            return json.load(f).get(kernel)
+    except Exception:
+        return None
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -362,10 +373,11 @@ def tma_applies(p) -> bool:
             and not (p.flags & native.FLAG_NO_TMA))
 
 
-def make_sim(w, form, dev, diag=False):
+def make_sim(w, form, dev, diag=False, flags=0):
     from capaz_b200 import Simulation, native
     p = w.params.copy()
     p.form = form
+    p.flags |= flags
     if diag:
         p.flags |= native.FLAG_DIAGNOSTICS
     sim = Simulation(p, device=dev)
@@ -420,9 +432,12 @@ def three_phase_leg(dev, steps: int = 200, warmup: int = 5) -> dict:
     out = {"workload": f"cfg2 three-phase {w.notes['workload_grid']} (reference axes {w.notes['ref_grid']}), "
                        f"dt {p.dt:.3g} s, per-cell K, 3x3 top source"}
     final = {}
-    for form, name, nbytes in ((native.FORM_FP64, "fp64", 64), (native.FORM_FP32C, "fp32c", 32)):
+    for form, name, nbytes in ((native.FORM_FP64, "fp64", 64), (native.FORM_FP32C, "fp32c", 32),
+                               (native.FORM_FP64, "fp64_products", 64)):
         q = p.copy()
         q.form = form
+        if name == "fp64_products":
+            q.flags |= native.FLAG_POW_PRODUCTS
         with Simulation(q, device=dev) as sim:
             sim.set_field("m", w.m)
             sim.set_field("K", w.K)
@@ -447,6 +462,11 @@ def three_phase_leg(dev, steps: int = 200, warmup: int = 5) -> dict:
         out[name] = {"value": p.ncell / (ms * 1e-3), "unit": "cell-steps/s", "ms_per_step": ms, "steps": steps,
                      "launches": launches, "algorithmic_bytes_per_cell": nbytes, "achieved_gbs": gbs,
                      "hbm_frac": gbs / peak, "finite": bool(np.isfinite(final[name]["S_n"]).all())}
+        fl = fp64_flops_per_cell("step3_fp64_kernel") if form == native.FORM_FP64 else None
+        if fl:
+            per = fl["products" if name == "fp64_products" else "pow"]
+            out[name]["fp64_flops_per_cell"] = per
+            out[name]["fp64_gflops"] = per * p.ncell / (ms * 1e-3) / 1e9
     out["value"], out["unit"], out["ms_per_step"] = out["fp64"]["value"], "cell-steps/s", out["fp64"]["ms_per_step"]
     out["speedup_fp32c_vs_fp64"] = out["fp32c"]["value"] / out["fp64"]["value"]
     prec = {"steps": w.steps, "against": "FP64 three-phase path (matches the reference CPU step to 1e-12)"}
@@ -455,8 +475,13 @@ def three_phase_leg(dev, steps: int = 200, warmup: int = 5) -> dict:
         prec[k] = {"max_abs": float(np.abs(a - b).max()),
                    "rel_l2": float(np.linalg.norm(a - b) / np.linalg.norm(b))}
     out["precision"] = prec
-    out["kernel"] = ("step3_fp64_kernel (FP64-bound: 13 pow per cell, 7 Newton iterations with Gauss-Jordan); "
-                     "step3_fp32c_kernel (FP32 stencil, two FP64 Newton iterations, Cramer's rule)")
+    for k in ("P_w", "S_w", "S_n"):
+        a, b = final["fp64_products"][k], final["fp64"][k]
+        out["fp64_products"][f"{k}_max_rel_vs_pow"] = float(np.abs(a - b).max() / np.abs(b).max())
+    out["speedup_products_vs_pow"] = out["fp64_products"]["value"] / out["fp64"]["value"]
+    out["kernel"] = ("step3_fp64_kernel (FP64: 13 pow per cell, or products and 4 sqrt with "
+                     "CAPAZ_FLAG_POW_PRODUCTS; 7 Newton iterations with Gauss-Jordan); step3_fp32c_tma_kernel + "
+                     "boundary3_kernel (TMA-staged FP32 stencil, one FP64 Newton step, Cramer's rule)")
     return out
 
 
@@ -557,7 +582,7 @@ def ensemble_leg(dev, steps: int = 300, warmup: int = 3) -> dict:
     """Batching form on the config-3 ensemble (64 two-phase instances, dims
     per axis from {32, 48, 64, 96, 128}, own lognormal K and dt each, 300
     steps): one persistent launch per step over all instances, the step
-    pair replayed as a CUDA graph, tile z-chunk and CTAs per SM autotuned;
+    pair replayed as a CUDA graph, tile shape, z-chunk and CTAs per SM autotuned;
     against the same 64 instances stepped one after another as separate
     contexts (precision form, and the plain FP64 path).  GPU time by CUDA
     events on one stream; aggregate cell-steps/s."""
@@ -691,11 +716,42 @@ def adjoint_leg(dev) -> dict:
             fd_out[key] = {"cells": len(cells), "step": h,
                            "rel_l2": float(np.linalg.norm(fd - ad) / np.linalg.norm(fd)),
                            "max_rel": float(np.max(np.abs(fd - ad) / np.abs(fd))), "pool_cells": int(len(pool))}
+    # Forward mode at the full size: the oracle's FP64 tangent-linear run (the
+    # restated reference step on dual numbers, through every Newton
+    # iteration) along two of the central-difference directions, the cells
+    # of the largest ln K and porosity gradients among the ones drawn, and
+    # along one dense seeded direction in both fields.
+    fwd = {}
+    try:
+        from oracle import oracle as O
+        t0 = time.perf_counter()
+        dirs = []
+        for which, g in (("lnK", gK), ("porosity", gm)):
+            flat = np.abs(g).ravel()
+            l = int(np.argmax(flat))
+            d = np.zeros(w.m.shape)
+            d.reshape(-1)[l] = 1.0
+            dirs.append((f"{which}_cell_{l}", d if which == "lnK" else None, d if which == "porosity" else None))
+        rng_d = np.random.default_rng(44)
+        dirs.append(("dense_both_fields", rng_d.standard_normal(w.m.shape), 0.01 * rng_d.standard_normal(w.m.shape)))
+        for name, dl, dm in dirs:
+            J_o, dJ = O.tangent(p, steps, w.m, w.K, obs, every, data, dlnK=dl, dm=dm)
+            fwd["misfit_oracle"] = J_o
+            fwd["misfit_rel_diff"] = abs(J - J_o) / abs(J_o)
+            terms = np.concatenate([(gK * dl).ravel() if dl is not None else np.zeros(0),
+                                    (gm * dm).ravel() if dm is not None else np.zeros(0)])
+            ad = float(np.sum(terms))
+            fwd[name] = {"adjoint": ad, "forward_mode": dJ, "rel_diff": abs(ad - dJ) / abs(dJ) if dJ else None}
+        fwd["rel_diff_max"] = max(v["rel_diff"] for v in fwd.values() if isinstance(v, dict) and v["rel_diff"] is not None)
+        fwd["cpu_seconds"] = time.perf_counter() - t0
+        fwd["threads"] = O.max_threads()
+    except Exception as e:  # reported, never fatal
+        fwd = {"failed": str(e)}
     h = steps_fd[0]
     return {"workload": f"cfg4 two-phase inverse problem {w.notes['workload_grid']}, FP64, {steps} steps, "
                         f"{len(obs)} observed cells every {every} steps, checkpoints every {cp}",
             "forward_ms": t_fwd * 1e3, "gradient_ms": t_grad * 1e3, "adjoint_over_forward": t_grad / t_fwd,
-            "misfit": J, "fd_step": h, "fd": fd_out,
+            "misfit": J, "fd_step": h, "fd": fd_out, "forward_mode": fwd,
             "timing": "wall clock around synchronised calls, best of 3; forward = data_initialization + "
                       "500 steps; gradient = checkpointed forward (misfit) + backward (recompute + reverse sweep)"}
 
@@ -795,6 +851,19 @@ def run_capaz(args) -> None:
         sim.close()
     t = timing[head]
     value = ncell * K * ws / (t["total_ms"] * 1e-3)
+    # The plain FP64 path with the lambda = 2 relative permeabilities as
+    # products (CAPAZ_FLAG_POW_PRODUCTS), timed the same way.
+    prod = None
+    if "fp64" in forms:
+        simq = make_sim(w, form_id["fp64"], dev, flags=native.FLAG_POW_PRODUCTS)
+        tq = time_form(simq, K, W, stream, ws, local)
+        simq.close()
+        prod = {"value": ncell * K * ws / (tq["total_ms"] * 1e-3), "ms_per_step": tq["total_ms"] / K,
+                "launches": tq["launches"]}
+        fl = fp64_flops_per_cell("step2_fp64_kernel")
+        if fl:
+            prod["fp64_flops_per_cell"] = fl["products"]
+            prod["fp64_gflops"] = fl["products"] * ncell / (tq["kern_ms"] * 1e-3) / 1e9
 
     # ---- precision of the precision form (1000 steps of the workload) -------
     prec = None
@@ -948,6 +1017,12 @@ def run_capaz(args) -> None:
             forms_out[f] = {"value": ncell * K * ws / (tt["total_ms"] * 1e-3), "ms_per_step": tt["total_ms"] / K,
                             "kernel_ms": tt["kern_ms"], "hbm_frac": ab / (tt["kern_ms"] * 1e-3) / 1e9 / peak,
                             "launches": tt["launches"]}
+            fl = fp64_flops_per_cell("step2_fp64_kernel") if f == "fp64" else None
+            if fl:
+                rate = ncell / (tt["kern_ms"] * 1e-3)
+                forms_out[f]["fp64_gflops"] = fl["pow"] * rate / 1e9
+                forms_out[f]["fp64_flops_per_cell"] = fl["pow"]
+                forms_out[f]["fp64_flops_source"] = "ncu DADD + DMUL + 2 DFMA per launch / cells (profiles/fp64_ops.json)"
         line = {
             "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": K,
             "warmup": W, "ms_per_step": t["total_ms"] / K, "higher_is_better": True, "scaling": "weak",
@@ -968,6 +1043,7 @@ def run_capaz(args) -> None:
             "forms": forms_out,
             "speedup_fp32c_vs_fp64": (forms_out["fp32c"]["value"] / forms_out["fp64"]["value"]
                                       if "fp32c" in forms_out and "fp64" in forms_out else None),
+            "fp64_products": prod,
             "precision": prec,
             "adjoint": adj,
             "three_phase": three,

@@ -36,6 +36,7 @@ CUDA_SOURCES = [
     ("step2_fp32c_tma.cu", []),
     ("step3_fp64.cu", ["-fmad=false"]),
     ("step3_fp32c.cu", []),
+    ("step3_fp32c_tma.cu", []),
     ("step_bl.cu", ["-fmad=false"]),
     ("step3e.cu", ["-fmad=false"]),
     ("fields.cu", []),
@@ -48,7 +49,7 @@ CUDA_SOURCES = [
     ("media.cu", []),
     ("slab.cu", []),
 ]
-HEADERS = ["capaz_internal.h", "capaz_ctx.h", "phys3.cuh", "diag_reduce.cuh"]
+HEADERS = ["capaz_internal.h", "capaz_ctx.h", "phys3.cuh", "phys3f.cuh", "diag_reduce.cuh"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

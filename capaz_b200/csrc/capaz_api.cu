@@ -129,6 +129,7 @@ Step2Const make_step2_const(const capaz_params& p) {
   // rounded quotient is >= t: the Newton iterations skip the division.
   c.se_fast_num = 2. * c.se_fast_min * (1. - p.S_wr);
   c.vol = p.hx * p.hy * p.hz;
+  c.lam2 = (p.flags & CAPAZ_FLAG_POW_PRODUCTS) && p.lambda == 2.0;
   return c;
 }
 
@@ -342,6 +343,7 @@ Step3Const make_step3_const(const capaz_params& p) {
   c.S_w_gr = p.S_w_gr;
   c.S_n_gr = p.S_n_gr;
   c.vol = p.hx * p.hy * p.hz;
+  c.a2 = (p.flags & CAPAZ_FLAG_POW_PRODUCTS) && p.lambda == 2.0;
   return c;
 }
 
@@ -755,6 +757,7 @@ void capaz_ctx::release() {
   if (m) cudaFree(m);
   if (K) cudaFree(K);
   if (err_flag) cudaFree(err_flag);
+  if (t3_counter) cudaFree(t3_counter);
   if (diag_out) cudaFree(diag_out);
   if (diag_host) cudaFreeHost(diag_host);
   for (int q = 0; q <= CAPAZ_DIAG_SLOTS; q++)

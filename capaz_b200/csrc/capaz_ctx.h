@@ -55,6 +55,11 @@ struct capaz_ctx {
   float4* rowF = nullptr;              // per-row tables (precision form)
   bool tma_applies() const;
   int tma_grid = 0;
+  // TMA path of the three-phase precision form: arguments per state parity.
+  capaz::Step3TArgs t3a[2];
+  bool t3_ready = false;
+  unsigned int* t3_counter = nullptr;
+  int t3_grid = 0;
   int tma_tile_y = capaz::TMA_TILE_Y;  // rows of a sweep tile (16 or 32)
   int tma_built_tile_y = 0;            // the tile the descriptor and item list were built for
   bool tma_ready = false;

@@ -47,6 +47,7 @@ struct Step2Const {
   double se_fast_min; // S_e at or above which P_d*pow(S_e, e) == +0 exactly
   double se_fast_num; // 1 - S_n - S_wr above which S_e >= se_fast_min without dividing
   double vol;         // hx*hy*hz (diagnostics)
+  int lam2;           // CAPAZ_FLAG_POW_PRODUCTS with lambda == 2: relperms by products
 };
 
 // Constants of the two-phase precision-form step (step2_fp32c.cu).
@@ -86,6 +87,7 @@ struct Step3Const {
   double hx, hy, hz, dt, g, P_atm;
   double ro0_w, ro0_n, ro0_g, beta_w, beta_n, mu_w, mu_n, mu_g;
   double S_wr, S_nr, S_gr, A, K0, S_w_gr, S_n_gr, vol;
+  int a2;  // CAPAZ_FLAG_POW_PRODUCTS with A == 2: relperms by products and sqrt
 };
 struct Step3Buffers {
   double *Pw, *Sw, *Sn, *Pn, *Pg;
@@ -117,6 +119,24 @@ struct Step3FArgs {
   unsigned int* err;
 };
 cudaError_t launch_step3_fp32c(const Step3FConst& c, const Step3FArgs& a, cudaStream_t s);
+// The same step with TMA-staged planes (step3_fp32c_tma.cu), for nx a
+// multiple of 4 (nx >= 4): a persistent sweep over the interior cells
+// (32 x 16 tiles, c.tiles_y from step3_fp32c_tma_tiles_y) and a kernel over
+// the boundary shell, which rearms the work counter.
+struct Step3TArgs {
+  CUtensorMap map_pw, map_sw, map_sn, map_K, map_m;  // input P_w, S_w, S_n deviations, K, m (36 x 18 boxes)
+  const float *p_n, *p_g;                            // input P_n, P_g deviations (read on the top and bottom rows)
+  float *o_pw, *o_sw, *o_sn, *o_pn, *o_pg;
+  const float* K;                                    // nullptr: uniform K0
+  const float4* rowF;                                // as in Step3FArgs
+  const double* Pref;
+  double* diag;                                      // per-CTA partials or nullptr
+  unsigned int* err;
+  unsigned int* counter;                             // work counter, zero between launches
+};
+int step3_fp32c_tma_tiles_y(int ny);
+int step3_fp32c_tma_grid(int device);
+cudaError_t launch_step3_fp32c_tma(const Step3FConst& c, const Step3TArgs& a, int grid, int nbound, cudaStream_t s);
 cudaError_t launch_row_tables3(const double* Pref, int ny, const Step3FConst& c, float4* rowF, cudaStream_t s);
 
 // Batched (ensemble) steps: one persistent launch over (instance, tile,

@@ -155,6 +155,74 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
     }
     return CAPAZ_OK;
   }
+  if (p.phases == 3 && p.form == CAPAZ_FORM_FP32C && p.nx % 4 == 0 && p.nx >= 4 && !(p.flags & CAPAZ_FLAG_NO_TMA)) {
+    Step3FConst c = make_step3f_const(p, S_ref_w, S_ref);
+    c.tiles_y = step3_fp32c_tma_tiles_y(p.ny);
+    if (p.nz > 1) {
+      c.zchunk = std::min(16, p.nz - 2);
+      c.nzchunks = (p.nz - 2 + c.zchunk - 1) / c.zchunk;
+    }
+    if (!t3_ready) {
+      const int ty = 16;
+      for (int b = 0; b < 2; b++) {
+        Step3TArgs& a = t3a[b];
+        memset(&a, 0, sizeof a);
+        if (encode_field_map(&a.map_pw, (const float*)state[b][0], p.nx, p.ny, p.nz, ty) ||
+            encode_field_map(&a.map_sw, (const float*)state[b][2], p.nx, p.ny, p.nz, ty) ||
+            encode_field_map(&a.map_sn, (const float*)state[b][1], p.nx, p.ny, p.nz, ty) ||
+            encode_field_map(&a.map_m, (const float*)m, p.nx, p.ny, p.nz, ty))
+          return fail_msg(CAPAZ_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+        if (p.flags & CAPAZ_FLAG_PERCELL_K) {
+          if (encode_field_map(&a.map_K, (const float*)K, p.nx, p.ny, p.nz, ty))
+            return fail_msg(CAPAZ_ERR_CUDA, "cuTensorMapEncodeTiled failed (K)");
+          a.K = (const float*)K;
+        } else {
+          a.map_K = a.map_m;  // unused (uniform K)
+          a.K = nullptr;
+        }
+        a.p_n = (const float*)state[b][3];
+        a.p_g = (const float*)state[b][4];
+        a.o_pw = (float*)state[b ^ 1][0];
+        a.o_sn = (float*)state[b ^ 1][1];
+        a.o_sw = (float*)state[b ^ 1][2];
+        a.o_pn = (float*)state[b ^ 1][3];
+        a.o_pg = (float*)state[b ^ 1][4];
+        a.rowF = rowF;
+        a.Pref = Pref;
+        a.err = err_flag;
+      }
+      if (!t3_counter) {
+        e = cudaMalloc(&t3_counter, sizeof(unsigned int));
+        if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(counter)");
+        e = cudaMemset(t3_counter, 0, sizeof(unsigned int));
+        if (e != cudaSuccess) return fail_cuda(e, "cudaMemset(counter)");
+      }
+      t3a[0].counter = t3a[1].counter = t3_counter;
+      t3_grid = std::min(c.tiles_x * c.tiles_y * c.nzchunks, step3_fp32c_tma_grid(device));
+      t3_ready = true;
+    }
+    if (diag && !diag_partials) {
+      diag_blocks = t3_grid;
+      e = cudaMalloc(&diag_partials, sizeof(double) * DIAG_STRIDE * diag_blocks);
+      if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(diag)");
+    }
+    const int nbound = boundary_cells(p.nx, p.ny, p.nz);
+    for (int t = 0; t < nsteps; t++) {
+      Step3TArgs a = t3a[cur];
+      a.diag = (diag && t == nsteps - 1) ? diag_partials : nullptr;
+      e = launch_step3_fp32c_tma(c, a, t3_grid, nbound, s);
+      launches += 2;
+      if (e != cudaSuccess) return fail_cuda(e, "step3_fp32c_tma launch");
+      cur ^= 1;
+      steps_done++;
+    }
+    if (diag) {
+      e = launch_diag_finalize(diag_partials, t3_grid, diag_out, s);
+      launches++;
+      if (e != cudaSuccess) return fail_cuda(e, "diag finalize launch");
+    }
+    return CAPAZ_OK;
+  }
   if (p.phases == 3 && p.form == CAPAZ_FORM_FP32C) {
     const Step3FConst c = make_step3f_const(p, S_ref_w, S_ref);
     if (diag && !diag_partials) {

@@ -7,23 +7,46 @@
 namespace capaz {
 namespace phys3 {
 
-// Relative permeabilities, three-phase.cpp:146-186.
-__device__ __forceinline__ double k_w3(double S_w_e, double A) {
+// Relative permeabilities, three-phase.cpp:146-186.  With a2 (A == 2 and
+// CAPAZ_FLAG_POW_PRODUCTS) the exponents A/(A-1) = 2, (A-1)/A = 1/2 and
+// 2(A-1)/A = 1 are taken as products and square roots.
+__device__ __forceinline__ double k_w3(double S_w_e, double A, bool a2 = false) {
   double k_w = 0;
-  if (S_w_e >= 1e-3) k_w = pow(S_w_e, 0.5) * pow(1. - pow(1. - pow(S_w_e, A / (A - 1.)), (A - 1.) / A), 2.);
+  if (S_w_e >= 1e-3) {
+    if (a2) {
+      const double t = 1. - sqrt(1. - S_w_e * S_w_e);
+      k_w = sqrt(S_w_e) * (t * t);
+    } else {
+      k_w = pow(S_w_e, 0.5) * pow(1. - pow(1. - pow(S_w_e, A / (A - 1.)), (A - 1.) / A), 2.);
+    }
+  }
   return k_w;
 }
-__device__ __forceinline__ double k_g3(double S_g_e, double A) {
+__device__ __forceinline__ double k_g3(double S_g_e, double A, bool a2 = false) {
   double k_g = 0;
-  if (S_g_e >= 1e-3) k_g = pow(S_g_e, 0.5) * pow(1. - pow(1. - S_g_e, A / (A - 1.)), 2. * (A - 1.) / A);
+  if (S_g_e >= 1e-3) {
+    if (a2) {
+      const double u = 1. - S_g_e;
+      k_g = sqrt(S_g_e) * (1. - u * u);
+    } else {
+      k_g = pow(S_g_e, 0.5) * pow(1. - pow(1. - S_g_e, A / (A - 1.)), 2. * (A - 1.) / A);
+    }
+  }
   return k_g;
 }
-__device__ __forceinline__ double k_n3(double S_w_e, double S_n_e, double A) {
+__device__ __forceinline__ double k_n3(double S_w_e, double S_n_e, double A, bool a2 = false) {
   double k_n = 0;
   double S_g_e = 1. - S_w_e - S_n_e;
   if (S_n_e >= 1e-3) {
-    double k_n_w = pow(1. - S_w_e, 0.5) * pow(1. - pow(S_w_e, A / (A - 1.)), 2. * (A - 1.) / A);
-    double k_n_g = pow(S_n_e, 0.5) * pow(1. - pow(1. - pow(S_n_e, A / (A - 1.)), (A - 1.) / A), 2.);
+    double k_n_w, k_n_g;
+    if (a2) {
+      k_n_w = sqrt(1. - S_w_e) * (1. - S_w_e * S_w_e);
+      const double t = 1. - sqrt(1. - S_n_e * S_n_e);
+      k_n_g = sqrt(S_n_e) * (t * t);
+    } else {
+      k_n_w = pow(1. - S_w_e, 0.5) * pow(1. - pow(S_w_e, A / (A - 1.)), 2. * (A - 1.) / A);
+      k_n_g = pow(S_n_e, 0.5) * pow(1. - pow(1. - pow(S_n_e, A / (A - 1.)), (A - 1.) / A), 2.);
+    }
     k_n = S_n_e * k_n_w * k_n_g / (1 - S_w_e) / (1 - S_g_e);
   }
   return k_n;

@@ -44,8 +44,16 @@ template <bool PD0>
 __device__ __forceinline__ void derive2(const Step2Const& c, double Pw, double Sn, double K, double& Pn,
                                         double& ro_w, double& ro_n, double& Xi_w, double& Xi_n) {
   double S_e = (1. - Sn - c.S_wr) / (1. - c.S_wr);
-  double k_w = pow(S_e, c.e_kw);
-  double k_n = (1. - S_e) * (1. - S_e) * (1 - pow(S_e, c.e_kn));
+  double k_w, k_n;
+  if (c.lam2) {
+    // lambda == 2: S_e^4 and S_e^2 as products (CAPAZ_FLAG_POW_PRODUCTS).
+    const double e2 = S_e * S_e;
+    k_w = e2 * e2;
+    k_n = (1. - S_e) * (1. - S_e) * (1 - e2);
+  } else {
+    k_w = pow(S_e, c.e_kw);
+    k_n = (1. - S_e) * (1. - S_e) * (1 - pow(S_e, c.e_kn));
+  }
   double P_k;
   if (PD0 && S_e >= c.se_fast_min) {
     P_k = 0.;  // P_d == 0 and pow finite: P_d*pow(...) is +0 exactly

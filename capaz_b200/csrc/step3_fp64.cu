@@ -51,7 +51,7 @@ __device__ __forceinline__ D3 derive3(const Step3Const& c, double Pw, double Sw,
   double S_w_e = (Sw - c.S_wr) / den;
   double S_n_e = (Sn - c.S_nr) / den;
   double S_g_e = 1. - S_w_e - S_n_e;
-  double k_w = k_w3(S_w_e, c.A), k_g = k_g3(S_g_e, c.A), k_n = k_n3(S_w_e, S_n_e, c.A);
+  double k_w = k_w3(S_w_e, c.A, c.a2), k_g = k_g3(S_g_e, c.A, c.a2), k_n = k_n3(S_w_e, S_n_e, c.A, c.a2);
   o.Xi_w = (-1.) * K * k_w / c.mu_w;
   o.Xi_n = (-1.) * K * k_n / c.mu_n;
   o.Xi_g = (-1.) * K * k_g / c.mu_g;

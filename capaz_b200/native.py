@@ -41,6 +41,7 @@ FLAG_DIAGNOSTICS = 0x2
 FLAG_SOURCE_WINDOW = 0x4
 FLAG_NO_TMA = 0x8
 FLAG_TEST_WAIT_TIMEOUT = 0x10
+FLAG_POW_PRODUCTS = 0x20
 
 ADJ_INIT_FROM_M = 0x1
 

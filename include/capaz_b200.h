@@ -77,6 +77,13 @@ enum capaz_form {
  * in flight and exits, and the step reports CAPAZ_ERR_CUDA.  Exercises the
  * timeout path without a fault or a hang. */
 #define CAPAZ_FLAG_TEST_WAIT_TIMEOUT 0x10u
+/* FP64 forms with Brooks-Corey index lambda == 2 (two-phase: k_w = S_e^4,
+ * k_n = (1-S_e)^2 (1-S_e^2); three-phase with A == 2: the square roots and
+ * squares of three-phase.cpp:146-186): the relative permeabilities by
+ * products and sqrt instead of pow.  Each value is within a few ulps of the
+ * pow form; P and S stay within 1e-12 of the reference (measured).  Ignored
+ * for other lambda and in the precision form (which always uses products). */
+#define CAPAZ_FLAG_POW_PRODUCTS 0x20u
 
 /*
  * Physical and numerical parameters: the subset of the reference's `consts`

@@ -50,11 +50,20 @@ def case(shape, seed):
     return p, m, K
 
 
-@pytest.mark.parametrize("shape,nsteps", [((48, 24, 40), 300), ((33, 20, 1), 300), ((1, 40, 1), 300)])
-def test_fp32c3_tracks_fp64(shape, nsteps):
+@pytest.mark.parametrize("shape,nsteps,no_tma", [
+    ((48, 24, 40), 300, False),  # TMA-staged sweep (nx a multiple of 4)
+    ((48, 24, 40), 300, True),   # the plain-load sweep on the same grid
+    ((44, 37, 19), 200, False),  # TMA, ragged tiles in x and y (the bottom row inside a tile)
+    ((32, 20, 1), 300, False),   # TMA, planar
+    ((33, 20, 1), 300, False),   # plain-load sweep (nx not a multiple of 4), planar
+    ((1, 40, 1), 300, False),    # column
+])
+def test_fp32c3_tracks_fp64(shape, nsteps, no_tma):
     """Config-2 physics (3x3 top NAPL source, lognormal K) from the
     reference's initial state; planar and column grids as well."""
     p, m, K = case(shape, sum(shape))
+    if no_tma:
+        p.flags |= native.FLAG_NO_TMA
     ref = run(p, native.FORM_FP64, m, K, nsteps)
     got = run(p, native.FORM_FP32C, m, K, nsteps)
     for k in ("P_w", "S_w", "S_n"):
