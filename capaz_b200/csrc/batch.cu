@@ -121,7 +121,17 @@ int build(capaz_batch* b) {
   for (int zc = 0; zc < maxc; zc++)
     for (int q = 0; q < n; q++)
       if (zc < nz_chunks[q])
-        for (int t = 0; t < ntiles[q]; t++) items.push_back(make_int4(q, t, zc, 0));
+        for (int t = 0; t < ntiles[q]; t++) {
+          if (b->fp32) {
+            // The precision sweep takes explicit z ranges: centres kb .. ke-1.
+            const capaz_params& pq = b->ctx[q]->p;
+            const int zq = std::min(b->zchunk, std::max(pq.nz - 2, 1));
+            const int kb = pq.nz == 1 ? 0 : 1 + zc * zq, ke = pq.nz == 1 ? 0 : std::min(kb + zq, pq.nz - 1);
+            items.push_back(make_int4(q, t, kb, ke));
+          } else {
+            items.push_back(make_int4(q, t, zc, 0));
+          }
+        }
   b->nitems = (int)items.size();
   if (items.size() > b->items_cap) {
     if (b->d_items) cudaFree(b->d_items);
@@ -172,9 +182,11 @@ bool stale(const capaz_batch* b) {
 int kernels_per_step(const capaz_batch* b) { return b->fp32 ? 2 : 1; }
 
 cudaError_t launch_one(capaz_batch* b, int parity, cudaStream_t s) {
-  if (b->fp32)
-    return launch_step2_fp32c_tma(b->phys, b->d_instT, b->d_items, b->nitems, b->d_bitems, b->nbitems, parity,
-                                  b->unik, b->planar, b->counter, nullptr, b->grid, s, nullptr, b->tile_y);
+  if (b->fp32) {
+    cudaError_t e = launch_step2_fp32c_tma(b->phys, b->d_instT, b->d_items, b->nitems, parity, b->unik, b->planar,
+                                           b->counter, nullptr, b->grid, s, nullptr, b->tile_y);
+    return e != cudaSuccess ? e : launch_boundary_fp32c(b->phys, b->d_instT, b->d_bitems, b->nbitems, parity, s);
+  }
   return launch_step2_fp64_batch(b->d_inst64, b->d_items, b->nitems, parity, b->unik, b->pd0, b->counter, b->grid, s);
 }
 
@@ -261,11 +273,12 @@ capaz_batch* capaz_batch_create(const capaz_params* params, int count, int devic
     // lambda = 2, and one set of physics constants for all instances.
     PhysF a = make_physf(p), z = make_physf(p0);
     const bool tma_ok = p.form != CAPAZ_FORM_FP32C ||
-                        (p.nx % 4 == 0 && p.P_d == 0. && p.lambda == 2.0 && memcmp(&a, &z, sizeof a) == 0 &&
-                         (p.nz == 1) == (p0.nz == 1));
+                        (p.nx % 4 == 0 && p.ny >= 4 && (p.nz == 1 || p.nz >= 4) && p.P_d == 0. && p.lambda == 2.0 &&
+                         memcmp(&a, &z, sizeof a) == 0 && (p.nz == 1) == (p0.nz == 1));
     if (!same || !tma_ok) {
       g_batch_error = "batch instances must be two-phase with the same form, flags and model class; "
-                      "precision-form batches need nx % 4 == 0, P_d = 0, lambda = 2, identical physics and "
+                      "precision-form batches need nx % 4 == 0, ny >= 4, nz == 1 or >= 4, P_d = 0, lambda = 2, "
+                      "identical physics and "
                       "all instances planar (nz == 1) or all three-dimensional";
       if (status) *status = CAPAZ_ERR_INVALID_ARGUMENT;
       return nullptr;
@@ -291,8 +304,8 @@ capaz_batch* capaz_batch_create(const capaz_params* params, int count, int devic
   }
   // The work counter starts at zero; the precision form's boundary kernel
   // rearms it after every sweep.
-  if (cudaMalloc(&b->counter, sizeof(unsigned int)) != cudaSuccess ||
-      cudaMemset(b->counter, 0, sizeof(unsigned int)) != cudaSuccess) {
+  if (cudaMalloc(&b->counter, sizeof(unsigned int) * SWEEP_COUNTERS) != cudaSuccess ||
+      cudaMemset(b->counter, 0, sizeof(unsigned int) * SWEEP_COUNTERS) != cudaSuccess) {
     capaz_batch_destroy(b);
     if (status) *status = CAPAZ_ERR_OUT_OF_MEMORY;
     return nullptr;

@@ -667,6 +667,10 @@ int capaz_step(capaz_ctx* ctx, int nsteps, void* stream) {
   if (!ctx || nsteps < 0) return CAPAZ_ERR_INVALID_ARGUMENT;
   return ctx->step(nsteps, (cudaStream_t)stream);
 }
+int capaz_step_split(capaz_ctx* ctx, void* edge_stream, void* interior_stream) {
+  if (!ctx || edge_stream == interior_stream) return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->step_split((cudaStream_t)edge_stream, (cudaStream_t)interior_stream);
+}
 int capaz_read_diag(capaz_ctx* ctx, capaz_diag* out, void* stream) {
   if (!ctx || !out) return CAPAZ_ERR_INVALID_ARGUMENT;
   return ctx->read_diag(out, (cudaStream_t)stream);
@@ -758,6 +762,10 @@ void capaz_ctx::release() {
   if (K) cudaFree(K);
   if (err_flag) cudaFree(err_flag);
   if (t3_counter) cudaFree(t3_counter);
+  if (split_items) cudaFree(split_items);
+  if (split_counters) cudaFree(split_counters);
+  for (auto& ev : split_ev)
+    if (ev) cudaEventDestroy(ev);
   if (diag_out) cudaFree(diag_out);
   if (diag_host) cudaFreeHost(diag_host);
   for (int q = 0; q <= CAPAZ_DIAG_SLOTS; q++)
@@ -769,8 +777,8 @@ void capaz_ctx::release() {
   if (stage) cudaFree(stage);
   if (tma_inst) cudaFree(tma_inst);
   if (tma_items) cudaFree(tma_items);
-  if (tma_bitems) cudaFree(tma_bitems);
   if (tma_counter) cudaFree(tma_counter);
+  if (tma_bitems) cudaFree(tma_bitems);
   if (first_bad) cudaFree(first_bad);
   if (sum_parts) cudaFree(sum_parts);
   if (S_ref_dev) cudaFree(S_ref_dev);
@@ -835,8 +843,13 @@ int capaz_ctx::set_field(int field, const void* src, bool on_device, cudaStream_
       CUDA_TRY(this, launch_decode_pressure((const float*)state[cur][4], Pref, p.nx, p.ny, n, wide[6], s));
       launches += 2;
     }
-    CUDA_TRY(this, launch_encode_pressure(d, p.nx, p.ny, p.nz, p.P_atm, Pref, PrelF, dPrefF, (float*)dst, s));
-    launches += 3;
+    if (ref_locked) {
+      CUDA_TRY(this, launch_encode_pressure_rel(d, Pref, p.nx, p.ny, n, (float*)dst, s));
+      launches++;
+    } else {
+      CUDA_TRY(this, launch_encode_pressure(d, p.nx, p.ny, p.nz, p.P_atm, Pref, PrelF, dPrefF, (float*)dst, s));
+      launches += 3;
+    }
     if (p.phases == 3) {
       CUDA_TRY(this, launch_encode_pressure_rel(wide[5], Pref, p.nx, p.ny, n, (float*)state[cur][3], s));
       CUDA_TRY(this, launch_encode_pressure_rel(wide[6], Pref, p.nx, p.ny, n, (float*)state[cur][4], s));
@@ -853,6 +866,9 @@ int capaz_ctx::set_field(int field, const void* src, bool on_device, cudaStream_
     CUDA_TRY(this, launch_encode_saturation(d, n, sum_parts, S_ref_dev, (float*)dst, s));
     launches += 3;
     CUDA_TRY(this, cudaMemcpyAsync(&S_ref_w, S_ref_dev, sizeof(double), cudaMemcpyDeviceToHost, s));
+  } else if (field == CAPAZ_FIELD_S_N && ref_locked) {
+    CUDA_TRY(this, launch_encode_saturation_ref(d, n, S_ref_dev, (float*)dst, s));
+    launches++;
   } else if (field == CAPAZ_FIELD_S_N) {
     CUDA_TRY(this, launch_encode_saturation(d, n, sum_parts, S_ref_dev, (float*)dst, s));
     launches += 3;

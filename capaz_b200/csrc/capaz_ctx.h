@@ -48,14 +48,25 @@ struct capaz_ctx {
   capaz::InstT* tma_inst = nullptr;  // device descriptor
   int4* tma_items = nullptr;
   int tma_nitems = 0;
+  unsigned int* tma_counter = nullptr;  // SWEEP_COUNTERS words
   int2* tma_bitems = nullptr;  // boundary-kernel blocks
   int tma_nbitems = 0;
-  unsigned int* tma_counter = nullptr;
   double tma_dt = 0., tma_S_ref = 0.;  // values baked into the descriptor
   float4* rowF = nullptr;              // per-row tables (precision form)
   bool tma_applies() const;
   int tma_grid = 0;
   // TMA path of the three-phase precision form: arguments per state parity.
+  // A reference state fixed by capaz_set_reference: P_w and S_n are then
+  // encoded against it instead of their own means.
+  bool ref_locked = false;
+  // capaz_step_split: work items of the edge planes (1, nz-2) then of the
+  // interior planes, their counters (SWEEP_COUNTERS words each), events.
+  int4* split_items = nullptr;
+  int split_nedge = 0, split_nint = 0, split_tile_y = 0, split_grid_e = 0, split_grid_i = 0;
+  unsigned int* split_counters = nullptr;
+  cudaEvent_t split_ev[2] = {nullptr, nullptr};
+  bool counters_dirty = false;  // a split step ran: rezero the single-launch counters
+  int step_split(cudaStream_t edge, cudaStream_t interior);
   capaz::Step3TArgs t3a[2];
   bool t3_ready = false;
   unsigned int* t3_counter = nullptr;

@@ -180,6 +180,7 @@ struct alignas(128) InstT {
   float dt_f;
   float sgr_dev_f;  // S_n_gr - S_ref (stored deviation of the source saturation)
   int nbound;       // boundary cells (written by the boundary kernel after the sweep)
+  int halo_lo, halo_hi;  // planes 0 / nz-1 are z-slab halo planes: the boundary kernel leaves them
   int tile_y;       // rows of a tile (the tensor maps' box is 36 x (tile_y + 2))
   // Bytes each raw stage announces beyond what its copies bring: 0, except
   // under CAPAZ_FLAG_TEST_WAIT_TIMEOUT, where it makes the first bounded
@@ -196,15 +197,20 @@ struct alignas(128) InstT {
 constexpr int TMA_TILE_Y = 16;
 bool tma_tile_supported(int tile_y);
 // All instances of one launch are planar (nz == 1) or all three-dimensional.
-// Launches the sweep over the interior cells and then the boundary kernel
-// (bitems: (instance, first boundary cell) blocks of BOUND_BLOCK cells).
+// A step is the sweep over the interior cells (work items: instance, tile,
+// first centre plane, last plane loaded) and then the boundary kernel over
+// every instance's boundary shell (bitems: (instance, first boundary cell)
+// blocks of BOUND_BLOCK).  counters: four zeroed words (work items and
+// finished CTAs per state parity) that the sweeps rearm themselves.  With
+// diag_partials, the sweep writes per-CTA diagnostics partials (grid of
+// them) and its last CTA reduces them into diag_out.
 constexpr int BOUND_BLOCK = 256;
-// With diag_partials, the sweep writes per-CTA diagnostics partials (grid
-// of them) and the boundary kernel reduces them into diag_out.
-cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems,
-                                   const int2* bitems, int nbitems, int parity, bool unik, bool planar,
-                                   unsigned int* counter, double* diag_partials, int grid, cudaStream_t s,
-                                   double* diag_out, int tile_y);
+constexpr int SWEEP_COUNTERS = 4;
+cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
+                                   bool unik, bool planar, unsigned int* counters, double* diag_partials, int grid,
+                                   cudaStream_t s, double* diag_out, int tile_y);
+cudaError_t launch_boundary_fp32c(const PhysF& f, const InstT* insts, const int2* bitems, int nbitems, int parity,
+                                  cudaStream_t s);
 // Boundary cells of an nx x ny x nz grid (faces, edges, corners; nz == 1: the
 // four sides of the plane).
 inline int boundary_cells(int nx, int ny, int nz) {
@@ -226,6 +232,11 @@ cudaError_t launch_encode_pressure_rel(const double* P, const double* Pref, int 
                                        cudaStream_t s);
 cudaError_t launch_decode_pressure(const float* p, const double* Pref, int nx, int ny, long long n, double* out,
                                    cudaStream_t s);
+// Tables of a given per-row reference (P_ref - P_atm, P_ref(j+1) - P_ref(j))
+// and saturation deviations from a given reference value.
+cudaError_t launch_pref_tables(const double* Pref, int ny, double P_atm, float* PrelF, float* dPrefF, cudaStream_t s);
+cudaError_t launch_encode_saturation_ref(const double* S, long long n, const double* S_ref, float* out,
+                                         cudaStream_t s);
 
 // Per-block partial diagnostics: mass[3], max residual, non-finite count.
 constexpr int DIAG_STRIDE = 5;

@@ -72,6 +72,13 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
   if (tma_applies()) {
     int st = tma_prepare();
     if (st) return st;
+    if (counters_dirty) {
+      // Split steps advanced the state without this path's launches: its
+      // per-parity counters are rezeroed instead of rearmed.
+      e = cudaMemsetAsync(tma_counter, 0, sizeof(unsigned int) * SWEEP_COUNTERS, s);
+      if (e != cudaSuccess) return fail_cuda(e, "cudaMemsetAsync(counters)");
+      counters_dirty = false;
+    }
     const PhysF f = make_physf(p);
     const bool unik = !(p.flags & CAPAZ_FLAG_PERCELL_K);
     if (diag && !diag_partials) {
@@ -83,9 +90,9 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
       const bool last = t == nsteps - 1;
       // With diagnostics, the last step's boundary kernel also reduces the
       // sweep's partials into diag_out.
-      e = launch_step2_fp32c_tma(f, tma_inst, tma_items, tma_nitems, tma_bitems, tma_nbitems, cur, unik, p.nz == 1,
-                                 tma_counter, (diag && last) ? diag_partials : nullptr, tma_grid, s, diag_out,
-                                 tma_tile_y);
+      e = launch_step2_fp32c_tma(f, tma_inst, tma_items, tma_nitems, cur, unik, p.nz == 1, tma_counter,
+                                 (diag && last) ? diag_partials : nullptr, tma_grid, s, diag_out, tma_tile_y);
+      if (e == cudaSuccess) e = launch_boundary_fp32c(f, tma_inst, tma_bitems, tma_nbitems, cur, s);
       launches += 2;
       if (e != cudaSuccess) return fail_cuda(e, "step2_fp32c_tma launch");
       cur ^= 1;
@@ -400,9 +407,94 @@ int capaz_ctx::derived(int field, cudaStream_t s, bool from_current) {
   return fail_msg(CAPAZ_ERR_UNSUPPORTED, "derived fields for this phase/form are not built yet");
 }
 
+// One time step as two sweeps: the edge planes (1 and nz - 2, with their
+// boundary cells) on `edge`, the interior planes (2 .. nz - 3) on
+// `interior`.  Each stream first waits for everything queued on the other,
+// so the caller's exchange of the previous step's planes on `edge` is done
+// before this step reads them.  The new state becomes current at once; its
+// edge planes are complete in `edge` order and can be sent while the
+// interior sweep runs.
+int capaz_ctx::step_split(cudaStream_t edge, cudaStream_t interior) {
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail_cuda(e, "cudaSetDevice");
+  if (!tma_applies() || p.nz < 4 || (p.flags & CAPAZ_FLAG_DIAGNOSTICS))
+    return fail_msg(CAPAZ_ERR_UNSUPPORTED,
+                    "split steps need the two-phase precision form with the TMA sweep (nx a multiple of 4, ny and "
+                    "nz at least 4) and no diagnostics");
+  int st = tma_prepare();
+  if (st) return st;
+  const bool unik = !(p.flags & CAPAZ_FLAG_PERCELL_K);
+  if (!split_items || split_tile_y != tma_tile_y) {
+    const int ty = tma_tile_y;
+    const int ntiles = ((p.nx - 2 + TX - 1) / TX) * ((p.ny - 2 + ty - 1) / ty);
+    std::vector<int4> items;
+    for (int t = 0; t < ntiles; t++) items.push_back(make_int4(0, t, 1, 2));
+    if (p.nz - 2 > 1)
+      for (int t = 0; t < ntiles; t++) items.push_back(make_int4(0, t, p.nz - 2, p.nz - 1));
+    split_nedge = (int)items.size();
+    for (int kb = 2; kb < p.nz - 2; kb += 16)
+      for (int t = 0; t < ntiles; t++) items.push_back(make_int4(0, t, kb, std::min(kb + 16, p.nz - 2)));
+    split_nint = (int)items.size() - split_nedge;
+    if (split_items) cudaFree(split_items);
+    split_items = nullptr;
+    e = cudaMalloc(&split_items, sizeof(int4) * items.size());
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(split items)");
+    e = cudaMemcpy(split_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy(split items)");
+    const int full = step2_fp32c_tma_grid(device, unik, ty);
+    split_grid_e = std::min(split_nedge, full);
+    split_grid_i = std::min(std::max(split_nint, 1), full);
+    split_tile_y = ty;
+    if (!split_counters) {
+      e = cudaMalloc(&split_counters, sizeof(unsigned int) * 2 * SWEEP_COUNTERS);
+      if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(split counters)");
+    }
+    for (auto& ev : split_ev)
+      if (!ev && (e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
+        return fail_cuda(e, "cudaEventCreate");
+  }
+  // Join the two streams.
+  if ((e = cudaEventRecord(split_ev[0], edge)) != cudaSuccess ||
+      (e = cudaEventRecord(split_ev[1], interior)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(edge, split_ev[1], 0)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(interior, split_ev[0], 0)) != cudaSuccess)
+    return fail_cuda(e, "stream join");
+  // Counters are rezeroed every split step (the two sweeps do not alternate
+  // with each other the way consecutive single launches do).
+  if ((e = cudaMemsetAsync(split_counters, 0, sizeof(unsigned int) * SWEEP_COUNTERS, edge)) != cudaSuccess ||
+      (e = cudaMemsetAsync(split_counters + SWEEP_COUNTERS, 0, sizeof(unsigned int) * SWEEP_COUNTERS, interior)) !=
+          cudaSuccess)
+    return fail_cuda(e, "cudaMemsetAsync(split counters)");
+  const PhysF f = make_physf(p);
+  e = launch_step2_fp32c_tma(f, tma_inst, split_items, split_nedge, cur, unik, false, split_counters, nullptr,
+                             split_grid_e, edge, nullptr, tma_tile_y);
+  if (e != cudaSuccess) return fail_cuda(e, "edge sweep launch");
+  launches++;
+  if (split_nint > 0) {
+    e = launch_step2_fp32c_tma(f, tma_inst, split_items + split_nedge, split_nint, cur, unik, false,
+                               split_counters + SWEEP_COUNTERS, nullptr, split_grid_i, interior, nullptr, tma_tile_y);
+    if (e != cudaSuccess) return fail_cuda(e, "interior sweep launch");
+    launches++;
+  }
+  // The boundary cells (of every plane but the halo planes) after both
+  // sweeps, on the interior stream.
+  if ((e = cudaEventRecord(split_ev[0], edge)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(interior, split_ev[0], 0)) != cudaSuccess)
+    return fail_cuda(e, "stream join");
+  e = launch_boundary_fp32c(f, tma_inst, tma_bitems, tma_nbitems, cur, interior);
+  if (e != cudaSuccess) return fail_cuda(e, "boundary launch");
+  launches++;
+  cur ^= 1;
+  steps_done++;
+  counters_dirty = true;
+  return CAPAZ_OK;
+}
+
 bool capaz_ctx::tma_applies() const {
+  // The sweep writes each boundary cell from its basic cell with at most one
+  // face per axis: grids at least four cells thick (or planar in z).
   return p.phases == 2 && p.form == CAPAZ_FORM_FP32C && p.nx % 4 == 0 && p.P_d == 0. && p.lambda == 2.0 &&
-         !(p.flags & CAPAZ_FLAG_NO_TMA);
+         p.ny >= 4 && (p.nz == 1 || p.nz >= 4) && !(p.flags & CAPAZ_FLAG_NO_TMA);
 }
 
 // Builds (or refreshes) the device descriptor of the TMA-staged precision
@@ -438,6 +530,8 @@ int capaz_ctx::tma_prepare() {
   h.dt_f = (float)p.dt;
   h.sgr_dev_f = (float)(p.S_n_gr - S_ref);
   h.nbound = boundary_cells(p.nx, p.ny, p.nz);
+  h.halo_lo = p.z_offset > 0;
+  h.halo_hi = p.nz_global > 0 && p.z_offset + p.nz < p.nz_global;
   h.test_tx_extra = (p.flags & CAPAZ_FLAG_TEST_WAIT_TIMEOUT) ? 16u : 0u;
   h.S_ref = S_ref;
   h.dt = p.dt;
@@ -476,9 +570,9 @@ int capaz_ctx::tma_prepare() {
   if (!tma_inst) {
     e = cudaMalloc(&tma_inst, sizeof(InstT));
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(tma)");
-    e = cudaMalloc(&tma_counter, sizeof(unsigned int));
+    e = cudaMalloc(&tma_counter, sizeof(unsigned int) * SWEEP_COUNTERS);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(tma)");
-    e = cudaMemset(tma_counter, 0, sizeof(unsigned int));
+    e = cudaMemset(tma_counter, 0, sizeof(unsigned int) * SWEEP_COUNTERS);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemset(tma)");
   }
   e = cudaMemcpy(tma_inst, &h, sizeof h, cudaMemcpyHostToDevice);
@@ -489,7 +583,10 @@ int capaz_ctx::tma_prepare() {
     const int ntiles = h.tiles_x * h.tiles_y;
     std::vector<int4> items;
     for (int zc = 0; zc < h.nzchunks; zc++)
-      for (int t = 0; t < ntiles; t++) items.push_back(make_int4(0, t, zc, 0));
+      for (int t = 0; t < ntiles; t++) {
+        const int kb = p.nz == 1 ? 0 : 1 + zc * h.zchunk, ke = p.nz == 1 ? 0 : std::min(kb + h.zchunk, p.nz - 1);
+        items.push_back(make_int4(0, t, kb, ke));
+      }
     if (tma_items && (int)items.size() > tma_nitems) {
       cudaFree(tma_items);
       tma_items = nullptr;

@@ -144,6 +144,17 @@ cudaError_t launch_decode_pressure(const float* p, const double* Pref, int nx, i
   return cudaGetLastError();
 }
 
+cudaError_t launch_pref_tables(const double* Pref, int ny, double P_atm, float* PrelF, float* dPrefF, cudaStream_t s) {
+  pref_tables_kernel<<<(ny + 127) / 128, 128, 0, s>>>(Pref, ny, P_atm, PrelF, dPrefF);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_encode_saturation_ref(const double* S, long long n, const double* S_ref, float* out,
+                                         cudaStream_t s) {
+  encode_s_kernel<<<grid_for(n, 256), 256, 0, s>>>(S, S_ref, n, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_row_tables(const double* Pref, int ny, const PhysF& f, float4* rowF, cudaStream_t s) {
   row_tables_kernel<<<(ny + 127) / 128, 128, 0, s>>>(Pref, ny, f, rowF);
   return cudaGetLastError();

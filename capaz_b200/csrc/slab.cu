@@ -10,6 +10,8 @@
 #include "capaz_ctx.h"
 #include "capaz_internal.h"
 
+using namespace capaz;
+
 namespace {
 
 __global__ void plane_decode_kernel(const float* __restrict__ a, const double* __restrict__ Pref, double S_ref,
@@ -83,6 +85,85 @@ int capaz_set_plane(capaz_ctx* ctx, int field, int k, const double* src, void* s
     e = cudaGetLastError();
   }
   return e == cudaSuccess ? CAPAZ_OK : ctx->fail_cuda(e, "capaz_set_plane");
+}
+
+// Plane k of a state field in its stored representation (float64 in the
+// FP64 form, the float32 deviation in the precision form), device to device:
+// the halo exchange of slabs that share one reference state moves these
+// bytes unchanged.
+int capaz_get_plane_raw(capaz_ctx* ctx, int field, int k, void* dst, void* stream) {
+  int slot = 0;
+  int st = plane_args(ctx, field, k, &slot);
+  if (st || !dst) return st ? st : CAPAZ_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return ctx->fail_cuda(e, "cudaSetDevice");
+  const capaz_params& p = ctx->p;
+  const size_t es = p.form == CAPAZ_FORM_FP64 ? sizeof(double) : sizeof(float), n = (size_t)p.nx * p.ny;
+  const char* src = (const char*)ctx->state[ctx->cur][slot] + (size_t)k * n * es;
+  e = cudaMemcpyAsync(dst, src, n * es, cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+  return e == cudaSuccess ? CAPAZ_OK : ctx->fail_cuda(e, "capaz_get_plane_raw");
+}
+
+int capaz_set_plane_raw(capaz_ctx* ctx, int field, int k, const void* src, void* stream) {
+  int slot = 0;
+  int st = plane_args(ctx, field, k, &slot);
+  if (st || !src) return st ? st : CAPAZ_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return ctx->fail_cuda(e, "cudaSetDevice");
+  const capaz_params& p = ctx->p;
+  const size_t es = p.form == CAPAZ_FORM_FP64 ? sizeof(double) : sizeof(float), n = (size_t)p.nx * p.ny;
+  char* dst = (char*)ctx->state[ctx->cur][slot] + (size_t)k * n * es;
+  e = cudaMemcpyAsync(dst, src, n * es, cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+  return e == cudaSuccess ? CAPAZ_OK : ctx->fail_cuda(e, "capaz_set_plane_raw");
+}
+
+// The precision form's reference state: per-row reference pressure (ny
+// values) and reference saturation S_n.
+int capaz_get_reference(capaz_ctx* ctx, double* Pref, double* S_ref) {
+  if (!ctx || !Pref || !S_ref) return CAPAZ_ERR_INVALID_ARGUMENT;
+  const capaz_params& p = ctx->p;
+  if (p.form != CAPAZ_FORM_FP32C || p.phases != 2)
+    return ctx->fail_msg(CAPAZ_ERR_UNSUPPORTED, "a reference state belongs to the two-phase precision form");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(Pref, ctx->Pref, sizeof(double) * p.ny, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return ctx->fail_cuda(e, "capaz_get_reference");
+  *S_ref = ctx->S_ref;
+  return CAPAZ_OK;
+}
+
+// Fixes the reference state: the current state is decoded with the old
+// reference and encoded with the new one, and later P_w / S_n (set_field,
+// init_state) are encoded against it instead of their own means.
+int capaz_set_reference(capaz_ctx* ctx, const double* Pref, double S_ref) {
+  if (!ctx || !Pref || !(S_ref == S_ref)) return CAPAZ_ERR_INVALID_ARGUMENT;
+  const capaz_params& p = ctx->p;
+  if (p.form != CAPAZ_FORM_FP32C || p.phases != 2)
+    return ctx->fail_msg(CAPAZ_ERR_UNSUPPORTED, "a reference state belongs to the two-phase precision form");
+  for (int j = 0; j < p.ny; j++)
+    if (!(Pref[j] == Pref[j]) || Pref[j] - Pref[j] != 0.)
+      return ctx->fail_msg(CAPAZ_ERR_INVALID_ARGUMENT, "reference pressures must be finite");
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return ctx->fail_cuda(e, "cudaSetDevice");
+  e = cudaDeviceSynchronize();  // steps in flight read the old reference
+  if (e != cudaSuccess) return ctx->fail_cuda(e, "cudaDeviceSynchronize");
+  int st = ctx->decode_all(ctx->cur, nullptr);
+  if (st) return st;
+  const long long n = ctx->n;
+  e = cudaMemcpy(ctx->Pref, Pref, sizeof(double) * p.ny, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(ctx->S_ref_dev, &S_ref, sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = launch_pref_tables(ctx->Pref, p.ny, p.P_atm, ctx->PrelF, ctx->dPrefF, nullptr);
+  if (e == cudaSuccess) e = launch_row_tables(ctx->Pref, p.ny, make_physf(p), ctx->rowF, nullptr);
+  if (e == cudaSuccess)
+    e = launch_encode_pressure_rel(ctx->wide[0], ctx->Pref, p.nx, p.ny, n, (float*)ctx->state[ctx->cur][0], nullptr);
+  if (e == cudaSuccess) e = launch_encode_saturation_ref(ctx->wide[1], n, ctx->S_ref_dev, (float*)ctx->state[ctx->cur][1], nullptr);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return ctx->fail_cuda(e, "capaz_set_reference");
+  ctx->launches += 4;
+  ctx->S_ref = S_ref;
+  ctx->ref_locked = true;
+  ctx->tma_ready = false;  // S_ref is part of the sweep's descriptor
+  return CAPAZ_OK;
 }
 
 }  // extern "C"

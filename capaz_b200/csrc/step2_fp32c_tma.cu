@@ -216,15 +216,15 @@ struct SmemRC {
   float4 rowF[TL::WY];
   double2 rowR[TL::WY];
   double rowPrel[TL::WY];
-  double red[TL::NW][4];
+  double red[TL::NW][DIAG_STRIDE];
   int w_sh;
 };
 
 template <int TYT, bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
 __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
     step2_fp32c_tma_kernel(const __grid_constant__ PhysF f, const InstT* __restrict__ insts,
-                          const int4* __restrict__ items, int nitems, int parity, unsigned int* __restrict__ counter,
-                          double* __restrict__ diag_partials) {
+                          const int4* __restrict__ items, int nitems, int parity, unsigned int* __restrict__ counters,
+                          double* __restrict__ diag_partials, double* __restrict__ diag_out) {
   using TL = Tile<TYT>;
   constexpr int WY = TL::WY, NHALO = TL::NHALO, BYW = TL::BYW, RC_R = TL::R, RC_TY = TL::NW, RC_NT = TL::NT;
   static_assert(NHALO <= RC_NT - 32, "a warp without halo work issues the copies");
@@ -267,7 +267,16 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
   float rmax = 0.f;
   const float iro0w_f = DIAG ? (float)(1. / f.ro0_w) : 0.f, iro0n_f = DIAG ? (float)(1. / f.ro0_n) : 0.f;
   const float aw_ro0w_f = DIAG ? (float)(f.aw / f.ro0_w) : 0.f, bn_ro0n_f = DIAG ? (float)(f.bn / f.ro0_n) : 0.f;
+  // counters[parity]: this launch's work items; counters[2 + parity]: its
+  // CTAs that have finished.  The launch before this one used the other
+  // parity's pair and has completed once griddepcontrol.wait returns, so
+  // this launch rearms them for the next.
+  unsigned int* counter = counters + parity;
   grid_dependency_wait();
+  if (blockIdx.x == 0 && tid == 0) {
+    counters[parity ^ 1] = 0u;
+    counters[2 + (parity ^ 1)] = 0u;
+  }
 
   for (;;) {
     if (tid == 0) sm.w_sh = (int)atomicAdd(counter, 1u);
@@ -288,7 +297,7 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
     float* __restrict__ p_out = A.p_out;
     float* __restrict__ s_out = A.s_out;
     unsigned int* __restrict__ err = A.err;
-    const int tile = it.y, zc = it.z;
+    const int tile = it.y;  // it.z, it.w: first centre plane, last plane loaded (centres it.z .. it.w - 1)
     const int ti = tile % I->tiles_x, tj = tile / I->tiles_x;
     const int i0 = 1 + ti * TX, j0 = 1 + tj * TYT;
     const int x0 = i0 - 1;
@@ -300,8 +309,8 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
     const int l0 = i + jS * sy32;
     bool bad = false;
     float chk = 0.f;  // sum of |p| + |s| of the written cells (non-diagnostic steps)
-    const int kb = PLANAR ? 0 : 1 + zc * I->zchunk;
-    const int ke = PLANAR ? 0 : min(kb + I->zchunk, nz - 1);
+    const int kb = PLANAR ? 0 : it.z;
+    const int ke = PLANAR ? 0 : it.w;
     const int pb = PLANAR ? 0 : kb - 1;
     const uint32_t stage_bytes = (UNIK ? 3u : 4u) * (uint32_t)(BXW * BYW * sizeof(float)) + I->test_tx_extra;
 
@@ -536,7 +545,9 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
   }
 
   if (DIAG) {
-    double(*red)[4] = sm.red;
+    // Per-CTA partials, then the last CTA to finish reduces them in index
+    // order (deterministic) into diag_out.
+    double(*red)[DIAG_STRIDE] = sm.red;
     const int lane = tid & 31, wid = tid >> 5;
     const double s0 = warp_sum(acc_w), s1 = warp_sum(acc_n), rr = warp_max((double)rmax), nf = warp_sum(nonfinite);
     if (lane == 0) {
@@ -560,6 +571,50 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
       out[2] = 0.;
       out[3] = t2;
       out[4] = t3;
+      __threadfence();
+      sm.w_sh = (atomicAdd(counters + 2 + parity, 1u) == gridDim.x - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    if (sm.w_sh) {
+      __threadfence();
+      const int nparts = gridDim.x;
+      const int per = (nparts + RC_NT - 1) / RC_NT;
+      const int b0 = tid * per, b1 = min(nparts, b0 + per);
+      double v[DIAG_STRIDE] = {0., 0., 0., 0., 0.};
+      for (int b = b0; b < b1; b++) {
+        const volatile double* q = diag_partials + (size_t)DIAG_STRIDE * b;
+        v[0] += q[0];
+        v[1] += q[1];
+        v[2] += q[2];
+        v[3] = fmax(v[3], q[3]);
+        v[4] += q[4];
+      }
+      for (int o = 1; o < 32; o <<= 1) {
+        double t[DIAG_STRIDE];
+#pragma unroll
+        for (int e = 0; e < DIAG_STRIDE; e++) t[e] = __shfl_down_sync(0xffffffffu, v[e], o);
+        if ((lane & (2 * o - 1)) == 0) {
+          v[0] += t[0];
+          v[1] += t[1];
+          v[2] += t[2];
+          v[3] = fmax(v[3], t[3]);
+          v[4] += t[4];
+        }
+      }
+      if (lane == 0)
+        for (int e = 0; e < DIAG_STRIDE; e++) red[wid][e] = v[e];
+      __syncthreads();
+      if (tid == 0) {
+        double t[DIAG_STRIDE] = {0., 0., 0., 0., 0.};
+        for (int qq = 0; qq < RC_TY; qq++) {
+          t[0] += red[qq][0];
+          t[1] += red[qq][1];
+          t[2] += red[qq][2];
+          t[3] = fmax(t[3], red[qq][3]);
+          t[4] += red[qq][4];
+        }
+        for (int e = 0; e < DIAG_STRIDE; e++) diag_out[e] = t[e];
+      }
     }
   }
 }
@@ -570,22 +625,13 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
 // the injection window, S_n_gr; the bottom row adds the weight
 // (rho_n S_n + rho_w (1 - S_n)) m g hy of the basic cell with its new S_n and
 // start-of-step densities (Border_P, main.cpp:255-267).  One thread per
-// boundary cell; items are (instance, first cell) blocks of BOUND_BLOCK.
-// With diagnostics, block 0 also reduces the sweep's per-CTA partials into
-// diag_out (they are complete once the sweep is), so the step needs no
-// separate reduction launch.
+// boundary cell; items are (instance, first cell) blocks of BOUND_BLOCK.  A
+// z-slab's halo planes (its planes 0 and nz - 1 when a neighbour owns them)
+// are left to the halo exchange.
 __global__ void __launch_bounds__(BOUND_BLOCK)
     boundary_fp32c_kernel(const __grid_constant__ PhysF f, const InstT* __restrict__ insts,
-                          const int2* __restrict__ bitems, int parity, unsigned int* __restrict__ counter,
-                          const double* __restrict__ diag_partials, int nparts, double* __restrict__ diag_out) {
-  grid_dependency_wait();  // the sweep's interior values and its use of the counter
-  // The sweep before this launch has taken all its work items: rearm its
-  // work counter for the next step.
-  if (blockIdx.x == 0 && threadIdx.x == 0) *counter = 0u;
-  if (diag_out != nullptr && blockIdx.x == 0) {
-    __shared__ double red[BOUND_BLOCK / 32][DIAG_STRIDE];
-    diag_reduce_block<BOUND_BLOCK / 32>(diag_partials, nparts, diag_out, red);
-  }
+                          const int2* __restrict__ bitems, int parity) {
+  grid_dependency_wait();  // the sweep's interior values
   const int2 it = bitems[blockIdx.x];
   const InstT* __restrict__ I = insts + it.x;
   const int q0 = it.y + (int)threadIdx.x;
@@ -622,6 +668,7 @@ __global__ void __launch_bounds__(BOUND_BLOCK)
       j = 1 + q / (nx - 2);
     }
   }
+  if ((k == 0 && I->halo_lo) || (k == nz - 1 && I->halo_hi)) return;
   const int i1 = min(max(i, 1), nx - 2), j1 = min(max(j, 1), ny - 2);
   const int k1 = nz == 1 ? 0 : min(max(k, 1), nz - 2);
   const long long sy = I->sy, sz = I->sz;
@@ -684,43 +731,39 @@ cudaError_t prepare_t() {
 
 template <int TYT, bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
 cudaError_t launch_t(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
-                     unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
+                     unsigned int* counter, double* diag_partials, int grid, cudaStream_t s, double* diag_out) {
   cudaError_t e = prepare_t<TYT, UNIK, DIAG, PLANAR, UNITH>();
   if (e != cudaSuccess) return e;
   return launch_dependent(step2_fp32c_tma_kernel<TYT, UNIK, DIAG, PLANAR, UNITH>, dim3(grid),
                           dim3(TX, Tile<TYT>::NW), sizeof(SmemRC<TYT>), s, f, insts, items, nitems, parity, counter,
-                          diag_partials);
+                          diag_partials, diag_out);
 }
 
 template <int TYT, bool UNIK, bool DIAG, bool PLANAR>
 cudaError_t launch_h(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
-                     unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
+                     unsigned int* counter, double* diag_partials, int grid, cudaStream_t s, double* diag_out) {
   // Unit spacing (the workloads' h = 1 m): forces are plain differences.
   const bool unith = f.inv_hx2 == 1.f && f.inv_hy2 == 1.f && f.inv_hz2 == 1.f;
-  return unith
-             ? launch_t<TYT, UNIK, DIAG, PLANAR, true>(f, insts, items, nitems, parity, counter, diag_partials, grid, s)
-             : launch_t<TYT, UNIK, DIAG, PLANAR, false>(f, insts, items, nitems, parity, counter, diag_partials, grid,
-                                                        s);
+  return unith ? launch_t<TYT, UNIK, DIAG, PLANAR, true>(f, insts, items, nitems, parity, counter, diag_partials,
+                                                          grid, s, diag_out)
+               : launch_t<TYT, UNIK, DIAG, PLANAR, false>(f, insts, items, nitems, parity, counter, diag_partials,
+                                                           grid, s, diag_out);
 }
 
 template <int TYT>
 cudaError_t launch_shape(bool unik, bool planar, const PhysF& f, const InstT* insts, const int4* items, int nitems,
-                         int parity, unsigned int* counter, double* diag_partials, int grid, cudaStream_t s) {
+                         int parity, unsigned int* counter, double* diag_partials, int grid, cudaStream_t s,
+                         double* diag_out) {
   const bool d = diag_partials != nullptr;
+#define CAPAZ_LH(U, D, P) launch_h<TYT, U, D, P>(f, insts, items, nitems, parity, counter, d ? diag_partials : nullptr, \
+                                                 grid, s, d ? diag_out : nullptr)
   if (unik) {
-    if (d) return planar ? launch_h<TYT, true, true, true>(f, insts, items, nitems, parity, counter, diag_partials,
-                                                           grid, s)
-                         : launch_h<TYT, true, true, false>(f, insts, items, nitems, parity, counter, diag_partials,
-                                                            grid, s);
-    return planar ? launch_h<TYT, true, false, true>(f, insts, items, nitems, parity, counter, nullptr, grid, s)
-                  : launch_h<TYT, true, false, false>(f, insts, items, nitems, parity, counter, nullptr, grid, s);
+    if (d) return planar ? CAPAZ_LH(true, true, true) : CAPAZ_LH(true, true, false);
+    return planar ? CAPAZ_LH(true, false, true) : CAPAZ_LH(true, false, false);
   }
-  if (d) return planar ? launch_h<TYT, false, true, true>(f, insts, items, nitems, parity, counter, diag_partials,
-                                                          grid, s)
-                       : launch_h<TYT, false, true, false>(f, insts, items, nitems, parity, counter, diag_partials,
-                                                           grid, s);
-  return planar ? launch_h<TYT, false, false, true>(f, insts, items, nitems, parity, counter, nullptr, grid, s)
-                : launch_h<TYT, false, false, false>(f, insts, items, nitems, parity, counter, nullptr, grid, s);
+  if (d) return planar ? CAPAZ_LH(false, true, true) : CAPAZ_LH(false, true, false);
+  return planar ? CAPAZ_LH(false, false, true) : CAPAZ_LH(false, false, false);
+#undef CAPAZ_LH
 }
 
 template <int TYT>
@@ -745,22 +788,21 @@ int grid_shape(int device, bool unik) {
 
 bool tma_tile_supported(int tile_y) { return tile_y == 16 || tile_y == 32; }
 
-cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems,
-                                   const int2* bitems, int nbitems, int parity, bool unik, bool planar,
-                                   unsigned int* counter, double* diag_partials, int grid, cudaStream_t s,
-                                   double* diag_out, int tile_y) {
-  // `counter` is zero on entry: zeroed at allocation and rearmed by every
-  // boundary launch.
-  cudaError_t e;
+cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
+                                   bool unik, bool planar, unsigned int* counters, double* diag_partials, int grid,
+                                   cudaStream_t s, double* diag_out, int tile_y) {
+  // counters[0..3] are zero at allocation; every launch rearms the pair of
+  // the other parity (see the kernel).
   if (tile_y == 32)
-    e = launch_shape<32>(unik, planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s);
-  else if (tile_y == 16)
-    e = launch_shape<16>(unik, planar, f, insts, items, nitems, parity, counter, diag_partials, grid, s);
-  else
-    return cudaErrorInvalidValue;
-  if (e != cudaSuccess) return e;
-  return launch_dependent(boundary_fp32c_kernel, dim3(nbitems), dim3(BOUND_BLOCK), 0, s, f, insts, bitems, parity,
-                          counter, (const double*)diag_partials, grid, diag_partials ? diag_out : nullptr);
+    return launch_shape<32>(unik, planar, f, insts, items, nitems, parity, counters, diag_partials, grid, s, diag_out);
+  if (tile_y == 16)
+    return launch_shape<16>(unik, planar, f, insts, items, nitems, parity, counters, diag_partials, grid, s, diag_out);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_boundary_fp32c(const PhysF& f, const InstT* insts, const int2* bitems, int nbitems, int parity,
+                                  cudaStream_t s) {
+  return launch_dependent(boundary_fp32c_kernel, dim3(nbitems), dim3(BOUND_BLOCK), 0, s, f, insts, bitems, parity);
 }
 
 int step2_fp32c_tma_grid(int device, bool unik, int tile_y) {

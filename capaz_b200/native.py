@@ -136,6 +136,11 @@ PROTOTYPES = {
     "capaz_sync": (C.c_int, [_VP]),
     "capaz_get_plane": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),
     "capaz_set_plane": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),
+    "capaz_get_plane_raw": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),
+    "capaz_set_plane_raw": (C.c_int, [_VP, C.c_int, C.c_int, _VP, _VP]),
+    "capaz_get_reference": (C.c_int, [_VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "capaz_set_reference": (C.c_int, [_VP, C.POINTER(C.c_double), C.c_double]),
+    "capaz_step_split": (C.c_int, [_VP, _VP, _VP]),
     "capaz_read_permeability_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _VP]),
     "capaz_load_permeability": (C.c_int, [_VP, C.c_char_p]),
     "capaz_generate_media": (C.c_int, [_VP, C.c_ulonglong, C.c_double, C.c_double, C.c_double, C.c_double,

@@ -167,6 +167,27 @@ class Simulation:
     def get_plane(self, name: str, k: int, dev_ptr: int, stream: int = 0) -> None:
         check(self.lib.capaz_get_plane(self.ctx, FIELDS[name], int(k), dev_ptr, stream or None), self.ctx)
 
+    def get_plane_raw(self, name: str, k: int, dev_ptr: int, stream: int = 0) -> None:
+        check(self.lib.capaz_get_plane_raw(self.ctx, FIELDS[name], int(k), dev_ptr, stream or None), self.ctx)
+
+    def set_plane_raw(self, name: str, k: int, dev_ptr: int, stream: int = 0) -> None:
+        check(self.lib.capaz_set_plane_raw(self.ctx, FIELDS[name], int(k), dev_ptr, stream or None), self.ctx)
+
+    def get_reference(self):
+        Pref = np.empty(self.params.ny, dtype=np.float64)
+        S = C.c_double(0.0)
+        check(self.lib.capaz_get_reference(self.ctx, Pref.ctypes.data_as(C.POINTER(C.c_double)), C.byref(S)),
+              self.ctx)
+        return Pref, S.value
+
+    def set_reference(self, Pref, S_ref: float) -> None:
+        Pref = np.ascontiguousarray(Pref, dtype=np.float64)
+        check(self.lib.capaz_set_reference(self.ctx, Pref.ctypes.data_as(C.POINTER(C.c_double)), float(S_ref)),
+              self.ctx)
+
+    def step_split(self, edge_stream: int, interior_stream: int) -> None:
+        check(self.lib.capaz_step_split(self.ctx, edge_stream, interior_stream), self.ctx)
+
     def set_plane(self, name: str, k: int, dev_ptr: int, stream: int = 0) -> None:
         check(self.lib.capaz_set_plane(self.ctx, FIELDS[name], int(k), dev_ptr, stream or None), self.ctx)
 

@@ -130,11 +130,42 @@ def state_fields(p: Params) -> list[str]:
     return ["P_w", "S_n"] + (["S_w", "P_n", "P_g"] if p.phases == 3 else [])
 
 
+def overlap_applies(p: Params) -> bool:
+    """Whether a slab of `p` steps with capaz_step_split and exchanges its
+    halo while the interior sweep runs (the two-phase precision form with
+    the TMA-staged sweep, no diagnostics)."""
+    from . import native
+    return (p.phases == 2 and p.form == native.FORM_FP32C and p.nx % 4 == 0 and p.P_d == 0.0 and
+            p.lambda_ == 2.0 and not (p.flags & (native.FLAG_NO_TMA | native.FLAG_DIAGNOSTICS)))
+
+
+def shared_reference(P_owned: np.ndarray, S_owned: np.ndarray, device, group=None):
+    """The precision form's reference state of the whole grid from every
+    rank's owned planes (nz_own, ny, nx): per-row means of P_w and the mean of
+    S_n, by all-reduces of sums and counts, so every rank holds the same."""
+    import torch
+    import torch.distributed as dist
+    rows = torch.from_numpy(np.ascontiguousarray(P_owned.sum(axis=(0, 2)))).to(device)
+    tot = torch.tensor([float(S_owned.sum()), float(S_owned.size), float(P_owned.shape[0] * P_owned.shape[2])],
+                       dtype=torch.float64, device=device)
+    dist.all_reduce(rows, op=dist.ReduceOp.SUM, group=group)
+    dist.all_reduce(tot, op=dist.ReduceOp.SUM, group=group)
+    t = tot.cpu().tolist()
+    return rows.cpu().numpy() / t[2], t[0] / t[1]
+
+
 class SlabSimulation:
     """One rank's slab of a decomposed grid on its GPU (torch.distributed
-    initialised with the NCCL backend, one process per GPU)."""
+    initialised with the NCCL backend, one process per GPU).
 
-    def __init__(self, params: Params, device: int, group=None):
+    In the two-phase precision form every step is capaz_step_split: the
+    slab's edge planes are swept on one stream and sent to the neighbours
+    (float32 deviations, grouped NCCL send/recv) while the interior planes
+    are swept on another; the received planes land in the halo planes before
+    the next step reads them.  All ranks share one reference state, so the
+    planes cross unchanged.  Other forms step, then exchange float64 planes."""
+
+    def __init__(self, params: Params, device: int, group=None, overlap=None):
         import torch
         import torch.distributed as dist
 
@@ -147,8 +178,17 @@ class SlabSimulation:
         self.device = torch.device("cuda", device)
         self.stream = torch.cuda.current_stream(self.device).cuda_stream
         self.fields = state_fields(params)
-        self.halo = HaloExchange(self.layout, params.nx * params.ny, self.fields, self.device, group)
         self.group = group
+        self.overlap = overlap_applies(params) if overlap is None else bool(overlap)
+        if self.overlap:
+            n = params.nx * params.ny
+            self.edge = torch.cuda.Stream(self.device)
+            self.interior = torch.cuda.Stream(self.device)
+            mk = lambda: torch.empty(n, dtype=torch.float32, device=self.device)  # noqa: E731
+            self.send = {(f, side): mk() for f in self.fields for side in ("lo", "hi")}
+            self.recv = {(f, side): mk() for f in self.fields for side in ("lo", "hi")}
+        else:
+            self.halo = HaloExchange(self.layout, params.nx * params.ny, self.fields, self.device, group)
 
     def _get(self, f, k, t):
         self.sim.get_plane(f, k, t.data_ptr(), self.stream)
@@ -161,11 +201,51 @@ class SlabSimulation:
 
     def init_state(self) -> None:
         self.sim.init_state()
+        if self.overlap:
+            self.share_reference()
+
+    def share_reference(self) -> None:
+        """Gives every rank the whole grid's reference state (collective)."""
+        Pref, S_ref = shared_reference(self.owned_field("P_w"), self.owned_field("S_n"), self.device, self.group)
+        self.sim.set_reference(Pref, S_ref)
+
+    def _exchange_raw(self) -> None:
+        """The halo exchange of one split step, queued on the edge stream."""
+        import torch
+        import torch.distributed as dist
+        L, es = self.layout, self.edge.cuda_stream
+        with torch.cuda.stream(self.edge):
+            ops = []
+            for f in self.fields:
+                if L.lo:
+                    self.sim.get_plane_raw(f, L.own_lo, self.send[(f, "lo")].data_ptr(), es)
+                    ops.append(dist.P2POp(dist.isend, self.send[(f, "lo")], L.rank - 1, self.group))
+                    ops.append(dist.P2POp(dist.irecv, self.recv[(f, "lo")], L.rank - 1, self.group))
+                if L.hi:
+                    self.sim.get_plane_raw(f, L.own_hi, self.send[(f, "hi")].data_ptr(), es)
+                    ops.append(dist.P2POp(dist.isend, self.send[(f, "hi")], L.rank + 1, self.group))
+                    ops.append(dist.P2POp(dist.irecv, self.recv[(f, "hi")], L.rank + 1, self.group))
+            if ops:
+                for req in dist.batch_isend_irecv(ops):
+                    req.wait()  # the edge stream waits; the host does not
+            for f in self.fields:
+                if L.lo:
+                    self.sim.set_plane_raw(f, 0, self.recv[(f, "lo")].data_ptr(), es)
+                if L.hi:
+                    self.sim.set_plane_raw(f, L.nz_local - 1, self.recv[(f, "hi")].data_ptr(), es)
 
     def step(self, nsteps: int = 1) -> None:
         for _ in range(nsteps):
-            self.sim.step(1, self.stream)
-            self.halo.exchange(self._get, self._set)
+            if self.overlap:
+                self.sim.step_split(self.edge.cuda_stream, self.interior.cuda_stream)
+                self._exchange_raw()
+            else:
+                self.sim.step(1, self.stream)
+                self.halo.exchange(self._get, self._set)
+
+    def synchronize(self) -> None:
+        import torch
+        torch.cuda.synchronize(self.device)
 
     def diag(self) -> dict:
         """Diagnostics of the last step over the whole grid (needs
@@ -173,6 +253,8 @@ class SlabSimulation:
         return reduce_diag(self.sim.diag(self.stream), self.device, self.group)
 
     def owned_field(self, name: str) -> np.ndarray:
+        if self.overlap:
+            self.synchronize()
         return self.layout.owned(self.sim.get_field(name))
 
     def gather(self, name: str):

@@ -330,6 +330,36 @@ int capaz_sync(capaz_ctx* ctx);
  * halo planes (P_S_exchange, mpi.cpp:113-294, once per step). */
 int capaz_get_plane(capaz_ctx* ctx, int field, int k, double* dst_device, void* stream);
 int capaz_set_plane(capaz_ctx* ctx, int field, int k, const double* src_device, void* stream);
+/* The same plane in its stored representation, device to device: float64 in
+ * the FP64 form, the float32 deviation from the reference state in the
+ * precision form (nx*ny values either way).  Slabs whose contexts share one
+ * reference state (capaz_set_reference) exchange these bytes unchanged:
+ * half the bytes of the float64 planes, and the slabs then step exactly like
+ * the undivided grid. */
+int capaz_get_plane_raw(capaz_ctx* ctx, int field, int k, void* dst_device, void* stream);
+int capaz_set_plane_raw(capaz_ctx* ctx, int field, int k, const void* src_device, void* stream);
+/* Two-phase precision form: the reference state (per-row reference pressure,
+ * ny values, and reference S_n) against which P_w and S_n are stored.
+ * capaz_set_reference fixes it: the current state is re-encoded, and later
+ * P_w and S_n (capaz_set_field, capaz_init_state) are encoded against it
+ * instead of their own means.  CAPAZ_ERR_UNSUPPORTED for other forms. */
+int capaz_get_reference(capaz_ctx* ctx, double* Pref_host, double* S_ref);
+int capaz_set_reference(capaz_ctx* ctx, const double* Pref_host, double S_ref);
+/* One time step as two sweeps so that a slab's halo exchange overlaps the
+ * interior: the edge planes (1 and nz-2, with their boundary cells) on
+ * edge_stream, the interior planes on interior_stream.  Each stream first
+ * waits for the work queued on the other, so an exchange queued on
+ * edge_stream after the previous call has landed before this step reads it.
+ * On return the new state is current: its edge planes are final in
+ * edge_stream order (read them with capaz_get_plane_raw there and write the
+ * received halo planes with capaz_set_plane_raw there), the interior in
+ * interior_stream order.  Synchronise both streams (or capaz_sync) before
+ * reading whole fields.  Two-phase precision form with the TMA-staged sweep
+ * (nx a multiple of 4), nz >= 3, no diagnostics (CAPAZ_ERR_UNSUPPORTED
+ * otherwise).  The exchange the reference does with MPI after its stages
+ * (mpi.cpp:113-241) becomes one exchange per step that the interior sweep
+ * hides. */
+int capaz_step_split(capaz_ctx* ctx, void* edge_stream, void* interior_stream);
 
 /* ---- heterogeneous media -------------------------------------------------
  * capaz_read_permeability_file: the permeability file of load_permeability

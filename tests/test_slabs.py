@@ -162,3 +162,128 @@ def test_decomposed_gpu_slabs_equal_whole_grid(form, world):
             assert np.array_equal(got[f], want[f]), f
         else:
             assert np.linalg.norm(got[f] - want[f]) <= 1e-7 * np.linalg.norm(want[f]), f
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world", [2, 3])
+def test_split_step_slabs_equal_whole_grid(world):
+    """The overlapped slab step (capaz_step_split: edge planes and interior
+    planes on two streams, float32 planes exchanged on the edge side while
+    the interior sweep runs) with every slab holding the whole grid's
+    reference state: bit-identical to one context stepping the whole grid."""
+    import torch
+    from capaz_b200 import Simulation
+    nz, nsteps = 29, 17
+    p = _params(nz)
+    p.nx, p.form = 12, FORM_FP32C
+    p.lambda_, p.P_d = 2.0, 0.0  # the TMA-staged sweep's model
+    m = _porosity(p, 6)
+    with Simulation(p) as whole:
+        whole.set_field("m", m)
+        whole.init_state()
+        Pref, S_ref = whole.get_reference()
+        whole.step(nsteps)
+        want = {f: whole.get_field(f) for f in ("P_w", "S_n")}
+    layouts = [SlabLayout(nz, r, world) for r in range(world)]
+    sims = [Simulation(L.local_params(p)) for L in layouts]
+    edge = [torch.cuda.Stream() for _ in sims]
+    inner = [torch.cuda.Stream() for _ in sims]
+    xchg = torch.cuda.Stream()
+    n = p.nx * p.ny
+    buf = {(r, f, side): torch.empty(n, dtype=torch.float32, device="cuda:0")
+           for r in range(world) for f in ("P_w", "S_n") for side in ("lo", "hi")}
+    try:
+        for L, s in zip(layouts, sims):
+            s.set_field("m", L.local(m))
+            s.set_reference(Pref, S_ref)  # fixed before the state is encoded
+            s.init_state()
+        torch.cuda.synchronize()
+        for _ in range(nsteps):
+            for s, e, i in zip(sims, edge, inner):
+                s.step_split(e.cuda_stream, i.cuda_stream)
+            # the exchange: after every slab's edge sweep, before its next step
+            for e in edge:
+                xchg.wait_stream(e)
+            xs = xchg.cuda_stream
+            for r in range(world):
+                L, s = layouts[r], sims[r]
+                for f in ("P_w", "S_n"):
+                    if L.lo:
+                        s.get_plane_raw(f, L.own_lo, buf[(r, f, "lo")].data_ptr(), xs)
+                    if L.hi:
+                        s.get_plane_raw(f, L.own_hi, buf[(r, f, "hi")].data_ptr(), xs)
+            for r in range(world):
+                L, s = layouts[r], sims[r]
+                for f in ("P_w", "S_n"):
+                    if L.lo:
+                        s.set_plane_raw(f, 0, buf[(r - 1, f, "hi")].data_ptr(), xs)
+                    if L.hi:
+                        s.set_plane_raw(f, L.nz_local - 1, buf[(r + 1, f, "lo")].data_ptr(), xs)
+            for e in edge:
+                e.wait_stream(xchg)
+        torch.cuda.synchronize()
+        got = {f: np.concatenate([L.owned(s.get_field(f)) for L, s in zip(layouts, sims)]) for f in ("P_w", "S_n")}
+    finally:
+        for s in sims:
+            s.close()
+    for f in ("P_w", "S_n"):
+        assert np.array_equal(got[f], want[f]), f
+
+
+@pytest.mark.gpu
+def test_split_step_of_one_grid_matches_single_launch_steps():
+    """capaz_step_split on an undivided grid (nothing to exchange), mixed
+    with ordinary steps, reproduces ordinary steps bit for bit."""
+    import torch
+    from capaz_b200 import Simulation
+    p = _params(21)
+    p.nx, p.form = 16, FORM_FP32C
+    p.lambda_, p.P_d = 2.0, 0.0
+    m = _porosity(p, 7)
+    out = []
+    for plan in ("ssssss", "pppppp", "psspps"):
+        with Simulation(p) as s:
+            s.set_field("m", m)
+            s.init_state()
+            e, i = torch.cuda.Stream(), torch.cuda.Stream()
+            for c in plan:
+                if c == "s":
+                    s.step(1)
+                else:
+                    torch.cuda.synchronize()
+                    s.step_split(e.cuda_stream, i.cuda_stream)
+                    torch.cuda.synchronize()
+            out.append((s.get_field("P_w"), s.get_field("S_n")))
+    for P, S in out[1:]:
+        assert np.array_equal(P, out[0][0]) and np.array_equal(S, out[0][1])
+
+
+def _reference_worker(rank, world, port, tmp):
+    import torch.distributed as dist
+    from capaz_b200.slabs import SlabLayout, shared_reference
+    os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    rng = np.random.default_rng(5)
+    P = 1e5 + 1e3 * rng.standard_normal((19, 7, 8))
+    S = rng.uniform(0.1, 0.9, (19, 7, 8))
+    L = SlabLayout(19, rank, world)
+    k0, k1 = L.k0, L.k1
+    Pref, S_ref = shared_reference(P[k0:k1], S[k0:k1], "cpu")
+    np.savez(os.path.join(tmp, f"ref{rank}.npz"), Pref=Pref, S_ref=S_ref, want=P.mean(axis=(0, 2)), wantS=S.mean())
+    dist.destroy_process_group()
+
+
+def test_shared_reference_is_the_whole_grids_on_every_rank(tmp_path):
+    """The overlapped slabs' common reference state: every rank gets the
+    same per-row mean pressure and mean saturation of the whole grid."""
+    import torch.multiprocessing as mp
+    world = 3
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    mp.start_processes(_reference_worker, args=(world, port, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    parts = [np.load(os.path.join(tmp_path, f"ref{r}.npz")) for r in range(world)]
+    for q in parts:
+        assert np.array_equal(q["Pref"], parts[0]["Pref"]) and float(q["S_ref"]) == float(parts[0]["S_ref"])
+        assert np.allclose(q["Pref"], q["want"], rtol=1e-13) and abs(float(q["S_ref"]) - float(q["wantS"])) < 1e-13
