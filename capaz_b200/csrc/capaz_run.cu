@@ -9,6 +9,24 @@
 
 using namespace capaz;
 
+// The number of z-chunks of the interior planes for a persistent sweep over
+// ntiles tiles with gmax resident CTAs: the one that minimises the estimated
+// span, the rounds of items per CTA (rounded up) times the planes an item
+// loads (its chunk and two halo planes).  Chunks shorter than four planes
+// derive more halo planes than they update and are not considered.  Chunk zc
+// covers the centre planes 1 + zc*interior/n .. 1 + (zc+1)*interior/n - 1.
+static int balanced_zchunks(long long ntiles, int interior, int gmax) {
+  int best = 1;
+  long long best_cost = -1;
+  for (int nc = 1; nc <= interior; nc++) {
+    const int len = (interior + nc - 1) / nc;
+    if (nc > 1 && len < 4) break;
+    const long long cost = ((ntiles * nc + gmax - 1) / gmax) * (len + 2);
+    if (best_cost < 0 || cost < best_cost) best_cost = cost, best = nc;
+  }
+  return best;
+}
+
 int capaz_ctx::step(int nsteps, cudaStream_t s) {
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return fail_cuda(e, "cudaSetDevice");
@@ -165,9 +183,11 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
   if (p.phases == 3 && p.form == CAPAZ_FORM_FP32C && p.nx % 4 == 0 && p.nx >= 4 && !(p.flags & CAPAZ_FLAG_NO_TMA)) {
     Step3FConst c = make_step3f_const(p, S_ref_w, S_ref);
     c.tiles_y = step3_fp32c_tma_tiles_y(p.ny);
+    const int g3 = step3_fp32c_tma_grid(device);
+    if (g3 <= 0) return fail_msg(CAPAZ_ERR_CUDA, "no resident CTA for the three-phase sweep");
     if (p.nz > 1) {
-      c.zchunk = std::min(16, p.nz - 2);
-      c.nzchunks = (p.nz - 2 + c.zchunk - 1) / c.zchunk;
+      c.nzchunks = balanced_zchunks((long long)c.tiles_x * c.tiles_y, p.nz - 2, g3);
+      c.zchunk = (p.nz - 2 + c.nzchunks - 1) / c.nzchunks;
     }
     if (!t3_ready) {
       const int ty = 16;
@@ -205,7 +225,7 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
         if (e != cudaSuccess) return fail_cuda(e, "cudaMemset(counter)");
       }
       t3a[0].counter = t3a[1].counter = t3_counter;
-      t3_grid = std::min(c.tiles_x * c.tiles_y * c.nzchunks, step3_fp32c_tma_grid(device));
+      t3_grid = std::min(c.tiles_x * c.tiles_y * c.nzchunks, g3);
       t3_ready = true;
     }
     if (diag && !diag_partials) {
@@ -516,12 +536,12 @@ int capaz_ctx::tma_prepare() {
   window_k(p, &h.win_k0, &h.win_k1);
   h.sy = d.sy;
   h.sz = d.sz;
-  // 16-plane z-chunks: the dynamic schedule balances the work, and the
-  // chunk count gives every SM several items.
+  // z-chunks that fill the persistent grid (balanced_zchunks).
+  const int gmax = step2_fp32c_tma_grid(device, !(p.flags & CAPAZ_FLAG_PERCELL_K), ty);
+  if (gmax <= 0) return fail_msg(CAPAZ_ERR_CUDA, "no resident CTA for the precision sweep");
   if (p.nz > 1) {
-    const int interior = p.nz - 2;
-    h.zchunk = std::min(16, interior);
-    h.nzchunks = (interior + h.zchunk - 1) / h.zchunk;
+    h.nzchunks = balanced_zchunks((long long)h.tiles_x * h.tiles_y, p.nz - 2, gmax);
+    h.zchunk = (p.nz - 2 + h.nzchunks - 1) / h.nzchunks;
   } else {
     h.zchunk = 1;
     h.nzchunks = 1;
@@ -582,9 +602,11 @@ int capaz_ctx::tma_prepare() {
     // z range, so the halos of neighbouring tiles meet in L2.
     const int ntiles = h.tiles_x * h.tiles_y;
     std::vector<int4> items;
+    const long long interior = std::max(p.nz - 2, 1);
     for (int zc = 0; zc < h.nzchunks; zc++)
       for (int t = 0; t < ntiles; t++) {
-        const int kb = p.nz == 1 ? 0 : 1 + zc * h.zchunk, ke = p.nz == 1 ? 0 : std::min(kb + h.zchunk, p.nz - 1);
+        const int kb = p.nz == 1 ? 0 : 1 + (int)(zc * interior / h.nzchunks);
+        const int ke = p.nz == 1 ? 0 : 1 + (int)((zc + 1) * interior / h.nzchunks);
         items.push_back(make_int4(0, t, kb, ke));
       }
     if (tma_items && (int)items.size() > tma_nitems) {
@@ -598,7 +620,7 @@ int capaz_ctx::tma_prepare() {
     }
     e = cudaMemcpy(tma_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy(items)");
-    tma_grid = std::min(tma_nitems, step2_fp32c_tma_grid(device, !(p.flags & CAPAZ_FLAG_PERCELL_K), ty));
+    tma_grid = std::min(tma_nitems, gmax);
     if (diag_partials && diag_blocks < tma_grid) {
       // The diagnostics partials are sized for the previous grid.
       cudaFree(diag_partials);

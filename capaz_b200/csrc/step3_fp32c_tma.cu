@@ -150,8 +150,8 @@ __global__ void __launch_bounds__(NT3, 2)
     const int i0 = 1 + ti * TX, j0 = 1 + tj * T3, x0 = i0 - 1;
     const int i = i0 + tx, jA = j0 + ty, jB = jA + Y3;
     const bool actA = (i <= c.nx - 2) && (jA <= c.ny - 2), actB = (i <= c.nx - 2) && (jB <= c.ny - 2);
-    const int kb = PLANAR ? 0 : 1 + zc * c.zchunk;
-    const int ke = PLANAR ? 0 : min(kb + c.zchunk, c.nz - 1);
+    const int kb = PLANAR ? 0 : 1 + (int)((long long)zc * (c.nz - 2) / c.nzchunks);
+    const int ke = PLANAR ? 0 : 1 + (int)((long long)(zc + 1) * (c.nz - 2) / c.nzchunks);
     const int pb = PLANAR ? 0 : kb - 1;
     bool bad = false;
     if (tid < WY3) {
