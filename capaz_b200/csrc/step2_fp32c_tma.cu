@@ -13,10 +13,11 @@
 //     across planes, so only the x neighbours and the segment ends go
 //     through shared memory (the sweep kernel's comment has the details);
 //   - the raw planes (p, s, K, m) of the tile's window (a 36 x 18 box at
-//     x = 32*ti, a 128-byte-aligned start) stream into a two-stage ring with
-//     cp.async.bulk.tensor (TMA, 3-D tensor maps, no multicast) completing on
-//     mbarriers, issued by a thread of the warp that derives no halo cells;
-//   - 124 registers and 51 KB of shared memory: four CTAs per SM;
+//     x = 32*ti, a 128-byte-aligned start) stream into a three-stage ring
+//     with cp.async.bulk.tensor (TMA, 3-D tensor maps, no multicast)
+//     completing on mbarriers, issued by a thread of the warp that derives no
+//     halo cells;
+//   - 128 registers and 52 KB of shared memory: four CTAs per SM;
 //   - physics constants are kernel parameters (constant-bank operands);
 //     per-row quantities (rho at the row's reference pressure, the scaled
 //     reference-pressure step) come from small per-instance tables.
@@ -185,16 +186,21 @@ __device__ __forceinline__ double warp_max(double v) {
 // (a 34 x 18 window with its halo); thread (tx, ty) owns the column segment of
 // four cells at x = tx, rows 4 ty .. 4 ty + 3.  Per z-plane, one elected
 // thread of the warp without halo work streams the raw window (p, s, K, m)
-// into a two-stage ring with cp.async.bulk.tensor (3-D tensor maps, no
+// into a three-stage ring with cp.async.bulk.tensor (3-D tensor maps, no
 // multicast) completing on mbarriers; every thread derives its four cells
 // (three warps also one halo cell each) into registers and into the plane's
 // shared derived slot, as the pair (p, p) and the pair (M_w, M_n) with
-// M = K k_r rho / mu.  After one barrier per plane the thread updates its
-// cells of the plane below: the x neighbours and the segment's two end
-// neighbours come from the shared slot, the vertical neighbours inside the
-// segment and both z neighbours from registers, and the -z inflow of each
-// cell is the +z outflow it computed on the plane below (the same product),
-// carried in registers.  Both phases run in packed f32x2 arithmetic: a face's
+// M = K k_r rho / mu.  In the same barrier interval it updates its cells of
+// the plane below: the x neighbours and the segment's two end neighbours
+// come from that plane's slot (complete since the previous barrier), the
+// vertical neighbours inside the segment and both z neighbours from
+// registers, and s and m from that plane's raw stage, which is refilled only
+// after the barrier that ends the update.  The -z inflow of each cell is the
+// +z outflow it computed on the plane below (the same product), carried in
+// registers.  One barrier per plane separates a slot's update reads from its
+// next writes (two derived slots alternate) and a raw stage's last reads from
+// its refill (three stages: the centre plane's, this plane's, and the next
+// one in flight).  Both phases run in packed f32x2 arithmetic: a face's
 // pressure difference is a (dp, dp) pair, the selected upwind mobilities a
 // (M_w, M_n) pair, the out - in term of an axis one multiply and one fused
 // multiply-add; on the vertical axis the phases' gravity terms are one pair
@@ -204,9 +210,10 @@ __device__ __forceinline__ double warp_max(double v) {
 // deviation, and its reciprocal from the hardware double-precision estimate
 // refined by one Newton-Raphson step (two with diagnostics).  The plane loop
 // is unrolled by two so the register roles of consecutive planes swap
-// without copies; the three derived slots (planes k - 1, k, k + 1) rotate.
-constexpr int RC_NRAW = 2;               // raw planes in flight
-constexpr int RC_NDER = 3;               // derived planes: read (k-1), written (k), next (k+1)
+// without copies.  The rows' constant pairs are read from shared memory where
+// they are used, which leaves the registers to the four cells.
+constexpr int RC_NRAW = 3;  // raw planes: the centre (k - 1, its s and m), k (derived), k + 1 (in flight)
+constexpr int RC_NDER = 2;  // derived planes: k - 1 (read), k (written)
 template <int TYT>
 struct SmemRC {
   using TL = Tile<TYT>;
@@ -214,6 +221,8 @@ struct SmemRC {
   ulonglong2 der[RC_NDER][TL::WCELLS];
   uint64_t bar[RC_NRAW];
   float4 rowF[TL::WY];
+  float2 rowAR[TL::WY];
+  float4 rowG[TL::WY];
   double2 rowR[TL::WY];
   double rowPrel[TL::WY];
   double red[TL::NW][DIAG_STRIDE];
@@ -271,24 +280,32 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
   // CTAs that have finished.  The launch before this one used the other
   // parity's pair and has completed once griddepcontrol.wait returns, so
   // this launch rearms them for the next.
+  // The first item of a CTA is its own index, the others come from the
+  // counter.  The work list and the instance records are written by the host
+  // only, so the first item's are read before waiting for the previous
+  // kernel; everything a kernel writes (state, media, row tables, counters)
+  // is touched after the wait.
   unsigned int* counter = counters + parity;
-  grid_dependency_wait();
-  if (blockIdx.x == 0 && tid == 0) {
-    counters[parity ^ 1] = 0u;
-    counters[2 + (parity ^ 1)] = 0u;
-  }
+  bool waited = false;
+  auto wait_previous = [&]() {
+    grid_dependency_wait();
+    waited = true;
+    if (blockIdx.x == 0 && tid == 0) {
+      counters[parity ^ 1] = 0u;
+      counters[2 + (parity ^ 1)] = 0u;
+    }
+  };
+  int w = blockIdx.x;
 
   for (;;) {
-    if (tid == 0) sm.w_sh = (int)atomicAdd(counter, 1u);
-    __syncthreads();
-    const int w = sm.w_sh;
     if (w >= nitems) {
+      if (!waited) wait_previous();
       asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
       break;
     }
     const int4 it = items[w];
     const InstT* __restrict__ I = insts + it.x;
-    const int nx = I->nx, ny = I->ny, nz = I->nz;
+    const int nx = I->nx, ny = I->ny;
     const int sy32 = (int)I->sy, sz32 = (int)I->sz;
     const float c1 = I->c1_f;
     const float dt_f = I->dt_f;
@@ -297,6 +314,7 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
     float* __restrict__ p_out = A.p_out;
     float* __restrict__ s_out = A.s_out;
     unsigned int* __restrict__ err = A.err;
+    if (!waited) wait_previous();
     const int tile = it.y;  // it.z, it.w: first centre plane, last plane loaded (centres it.z .. it.w - 1)
     const int ti = tile % I->tiles_x, tj = tile / I->tiles_x;
     const int i0 = 1 + ti * TX, j0 = 1 + tj * TYT;
@@ -331,19 +349,22 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
     };
     if (tid == ISS)
       for (int q = 0; q < RC_NRAW && pb + q <= ke; q++) issue(q, pb + q);
+    int qs = 0;  // raw stage of the plane being derived
     __syncthreads();
-    // Row pairs of the segment's rows (see the packed sweep).
-    f32x2 AR[RC_R], G1[RC_R], G2[RC_R];
-#pragma unroll
-    for (int r = 0; r < RC_R; r++) {
-      const int wr = RC_R * ty + 1 + r;
-      const float4 rw = sm.rowF[wr];
-      const float dn = sm.rowF[wr - 1].z;
+    // Row pairs of the window's rows (the own rows 1 .. TYT are used): the
+    // reference densities over mu, and the vertical gravity terms of the
+    // faces below and above.
+    if (tid >= 1 && tid < WY) {
+      const float4 rw = sm.rowF[tid];
+      const float dn = sm.rowF[tid - 1].z;
       const float gw = f.g_mu_w * rw.x, gn = f.g_mu_n * rw.y;
-      AR[r] = pack2(rw.x, rw.y);
-      G1[r] = pack2(gw - dn, gn - dn);
-      G2[r] = pack2(gw - rw.z, gn - rw.z);
+      sm.rowAR[tid] = make_float2(rw.x, rw.y);
+      sm.rowG[tid] = make_float4(gw - dn, gn - dn, gw - rw.z, gn - rw.z);
     }
+    __syncthreads();
+    auto AR = [&](int r) { const float2 v = sm.rowAR[RC_R * ty + 1 + r]; return pack2(v.x, v.y); };
+    auto G1 = [&](int r) { const float4 v = sm.rowG[RC_R * ty + 1 + r]; return pack2(v.x, v.y); };
+    auto G2 = [&](int r) { const float4 v = sm.rowG[RC_R * ty + 1 + r]; return pack2(v.z, v.w); };
 
     auto derive_cell = [&](f32x2 ARr, float p, float sv, float K) -> ulonglong2 {
       const float S_e = (c1 - sv) * f.inv_one_m_swr;
@@ -445,41 +466,61 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
 
     // Derived cells of two consecutive planes in registers: planes pb, pb + 2,
     // ... in X0, the others in X1 (the loop is unrolled by two, so the
-    // centre and next-plane roles swap without copies); likewise s and m.
-    static_assert(RC_NRAW == 2, "the unrolled plane loop alternates two raw stages");
+    // centre and next-plane roles swap without copies).
     ulonglong2 X0[RC_R], X1[RC_R];
     f32x2 Zin[RC_R];                     // -z inflow pairs of the centre cells
-    float s0[RC_R], m0[RC_R], s1[RC_R], m1[RC_R];
-    // Derived slots of planes pl - 1, pl and pl + 1, rotated every plane.
-    ulonglong2* Dr = sm.der[RC_NDER - 1];
-    ulonglong2* Dw = sm.der[0];
-    ulonglong2* Dn = sm.der[1];
     auto plane = [&](auto T, int pl) -> bool {
-      constexpr int t = decltype(T)::value;  // (pl - pb) mod 2, also plane pl's raw stage
+      constexpr int t = decltype(T)::value;  // (pl - pb) mod 2: plane pl's derived slot
       ulonglong2(&N)[RC_R] = t ? X1 : X0;
       ulonglong2(&C)[RC_R] = t ? X0 : X1;
-      float(&sN)[RC_R] = t ? s1 : s0;
-      float(&mN)[RC_R] = t ? m1 : m0;
-      float(&sC)[RC_R] = t ? s0 : s1;
-      float(&mC)[RC_R] = t ? m0 : m1;
-      const bool landed = mbar_wait_bounded(&sm.bar[t], (phase >> t) & 1u);
+      ulonglong2* const Dw = sm.der[t];      // plane pl
+      ulonglong2* const Dr = sm.der[t ^ 1];  // plane pl - 1
+      const int qc = qs == 0 ? RC_NRAW - 1 : qs - 1;  // raw stage of plane pl - 1
+      const bool landed = mbar_wait_bounded(&sm.bar[qs], (phase >> qs) & 1u);
       if (landed) {
-        phase ^= (1u << t);
-        armed &= ~(1u << t);
+        phase ^= (1u << qs);
+        armed &= ~(1u << qs);
       }
+      const auto& R = sm.raw[qs];
+      const auto& RC = sm.raw[qc];
       {
-        const auto& R = sm.raw[t];
 #pragma unroll
         for (int r = 0; r < RC_R; r++) {
           const int ri = raw0 + r * BXW;
-          sN[r] = R.s[ri];
-          mN[r] = R.m[ri];
-          N[r] = derive_cell(AR[r], R.p[ri], sN[r], UNIK ? f.K0 : R.K[ri]);
+          N[r] = derive_cell(AR(r), R.p[ri], R.s[ri], UNIK ? f.K0 : R.K[ri]);
           Dw[own0 + r * WX] = N[r];
         }
         if (halo_slot >= 0) {
           const float4 rh = sm.rowF[halo_row];
           Dw[halo_slot] = derive_cell(pack2(rh.x, rh.y), R.p[halo_raw], R.s[halo_raw], UNIK ? f.K0 : R.K[halo_raw]);
+        }
+      }
+      // The update of the centre plane pl - 1 before the barrier: its slot
+      // was written before the previous barrier, this plane's own cells are
+      // in registers, so the derive and the update overlap.  A thread whose
+      // wait ran out stores nothing.
+      if (!PLANAR) {
+        if (pl == pb + 1) {
+#pragma unroll
+          for (int r = 0; r < RC_R; r++) Zin[r] = zflux(C[r], N[r]);  // inflow of plane kb through its -z face
+        } else if (pl >= pb + 2) {
+          // x and segment-end neighbours from the centre plane's slot, the
+          // rest from registers, s and m from its raw stage.
+          const int lk = l0 + (pl - 1) * sz32;
+#pragma unroll
+          for (int r = 0; r < RC_R; r++) {
+            const int o = own0 + r * WX;
+            const ulonglong2 c = C[r];
+            const ulonglong2 ya = r == 0 ? Dr[o - WX] : C[r - 1];
+            const ulonglong2 yb = r == RC_R - 1 ? Dr[o + WX] : C[r + 1];
+            Kahan2 k(xaxis(c, Dr[o - 1], Dr[o + 1]));
+            k.add(yaxis(c, ya, yb, G1(r), G2(r)));
+            const f32x2 out = zflux(c, N[r]);
+            k.add(sub2(out, Zin[r]));
+            Zin[r] = out;
+            finish(c, k.sum(), r, RC.s[raw0 + r * BXW], RC.m[raw0 + r * BXW], lk + r * sy32,
+                   landed && ((active >> r) & 1u));
+          }
         }
       }
       if (__syncthreads_or(!landed)) {
@@ -491,9 +532,10 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
         __syncthreads();
         return true;
       }
-      if (tid == ISS && pl + RC_NRAW <= ke) {
+      // Plane pl - 1's stage is free once every thread has updated it.
+      if (tid == ISS && pl > pb && pl + RC_NRAW - 1 <= ke) {
         fence_proxy_async();
-        issue(t, pl + RC_NRAW);
+        issue(qc, pl + RC_NRAW - 1);
       }
       if (PLANAR) {
 #pragma unroll
@@ -503,34 +545,11 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
           const ulonglong2 ya = r == 0 ? Dw[o - WX] : N[r - 1];
           const ulonglong2 yb = r == RC_R - 1 ? Dw[o + WX] : N[r + 1];
           Kahan2 k(xaxis(c, Dw[o - 1], Dw[o + 1]));
-          k.add(yaxis(c, ya, yb, G1[r], G2[r]));
-          finish(c, k.sum(), r, sN[r], mN[r], l0 + r * sy32, (active >> r) & 1u);
-        }
-      } else if (pl == pb + 1) {
-#pragma unroll
-        for (int r = 0; r < RC_R; r++) Zin[r] = zflux(C[r], N[r]);  // inflow of plane kb through its -z face
-      } else if (pl >= pb + 2) {
-        // Centre plane pl - 1: x and segment-end neighbours from its shared
-        // slot, the rest from registers.
-        const int lk = l0 + (pl - 1) * sz32;
-#pragma unroll
-        for (int r = 0; r < RC_R; r++) {
-          const int o = own0 + r * WX;
-          const ulonglong2 c = C[r];
-          const ulonglong2 ya = r == 0 ? Dr[o - WX] : C[r - 1];
-          const ulonglong2 yb = r == RC_R - 1 ? Dr[o + WX] : C[r + 1];
-          Kahan2 k(xaxis(c, Dr[o - 1], Dr[o + 1]));
-          k.add(yaxis(c, ya, yb, G1[r], G2[r]));
-          const f32x2 out = zflux(c, N[r]);
-          k.add(sub2(out, Zin[r]));
-          Zin[r] = out;
-          finish(c, k.sum(), r, sC[r], mC[r], lk + r * sy32, (active >> r) & 1u);
+          k.add(yaxis(c, ya, yb, G1(r), G2(r)));
+          finish(c, k.sum(), r, R.s[raw0 + r * BXW], R.m[raw0 + r * BXW], l0 + r * sy32, (active >> r) & 1u);
         }
       }
-      ulonglong2* const old = Dr;
-      Dr = Dw;
-      Dw = Dn;
-      Dn = old;
+      qs = qs == RC_NRAW - 1 ? 0 : qs + 1;
       return false;
     };
     for (int base = pb; base <= ke; base += 2) {
@@ -541,7 +560,9 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
     if (stopped) break;
     if (!DIAG) bad = !(chk <= 3.0e38f);
     if (__any_sync(0xffffffffu, bad) && (tid & 31) == 0) atomicOr(err, 1u);
+    if (tid == 0) sm.w_sh = (int)gridDim.x + (int)atomicAdd(counter, 1u);
     __syncthreads();  // the next item's loads reuse the stages, slots and rows
+    w = sm.w_sh;
   }
 
   if (DIAG) {
@@ -631,7 +652,11 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
 __global__ void __launch_bounds__(BOUND_BLOCK)
     boundary_fp32c_kernel(const __grid_constant__ PhysF f, const InstT* __restrict__ insts,
                           const int2* __restrict__ bitems, int parity) {
-  grid_dependency_wait();  // the sweep's interior values
+  // The work lists and instance records are not written by the sweep: the
+  // cell's position is worked out before waiting for the sweep's values, and
+  // the next step's sweep may be scheduled as soon as every block is here
+  // (it waits for this kernel's completion before reading the state).
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int2 it = bitems[blockIdx.x];
   const InstT* __restrict__ I = insts + it.x;
   const int q0 = it.y + (int)threadIdx.x;
@@ -674,12 +699,15 @@ __global__ void __launch_bounds__(BOUND_BLOCK)
   const long long sy = I->sy, sz = I->sz;
   const long long lb = i + j * sy + (long long)k * sz, l1 = i1 + j1 * sy + (long long)k1 * sz;
   const Step2FArgs& A = I->a[parity];
-  const float s1 = A.s_out[l1];
+  float* __restrict__ const s_out = A.s_out;
+  float* __restrict__ const p_out = A.p_out;
+  grid_dependency_wait();  // the sweep's interior values
+  const float s1 = s_out[l1];
   float sb = s1;
   if ((j == 0) && (I->source > 0) && in_window(I, i, k)) sb = I->sgr_dev_f;
   float pb;
   if ((j != 0) && (j != ny - 1)) {
-    pb = A.p_out[l1];
+    pb = p_out[l1];
   } else if (j == 0) {
     pb = (float)((f.P_atm + f.P_top) - I->Pref[0]);
   } else {
@@ -687,12 +715,12 @@ __global__ void __launch_bounds__(BOUND_BLOCK)
     const double pr = prel + (double)A.p_in[l1];  // start-of-step pressure of the basic cell
     const double rw = fma(f.aw, pr, f.ro0_w), rn = fma(f.bn, pr, f.ro0_n);
     const double Snew = I->S_ref + (double)s1;
-    const double Pnew = (prel + f.P_atm) + (double)A.p_out[l1];
+    const double Pnew = (prel + f.P_atm) + (double)p_out[l1];
     const double ro_g_dy = (rn * Snew + rw * (1 - Snew)) * (double)A.m[l1] * f.g * f.hy;
     pb = (float)(Pnew + ro_g_dy - I->Pref[ny - 1]);
   }
-  A.s_out[lb] = sb;
-  A.p_out[lb] = pb;
+  s_out[lb] = sb;
+  p_out[lb] = pb;
 }
 
 // Launches with programmatic stream serialisation: the kernel may start

@@ -18,8 +18,12 @@
 //     (p_n, p_g), which differ from p_w only on the grid's top and bottom
 //     rows (three-phase.cpp:345-427 with zero capillary pressures) and are
 //     read there from the stored state;
-//   - the update of the plane below reads the centre and its six
-//     neighbours from the ring: one barrier per plane;
+//   - the update of the plane below, in the same barrier interval as the
+//     derive: it reads the centre and its x and y neighbours from the centre
+//     plane's slot (complete since the previous barrier), its z neighbours'
+//     own cells from the slots of the planes around it, and the centre's
+//     s and m from its raw stage, which is refilled (with the plane two ahead)
+//     only after the barrier that ends the update: one barrier per plane;
 //   - boundary cells are written after the sweep by a kernel over the
 //     boundary shell (Border_S, Border_P), from the new state of each cell's
 //     basic-coordinate cell; that kernel also rearms the work counter.
@@ -288,9 +292,12 @@ __global__ void __launch_bounds__(NT3, 2)
       }
     };
 
-    float swA0 = 0.f, snA0 = 0.f, mA0 = 0.f, swB0 = 0.f, snB0 = 0.f, mB0 = 0.f;
+    // Plane pl: derive into slot u, then update the centre plane pl - 1
+    // (slot and raw stage uc, its s and m read there) before the barrier; the
+    // stage of plane pl - 1 is refilled with plane pl + 2 after it.
     auto plane = [&](auto U, int pl) -> bool {
       constexpr int u = decltype(U)::value;
+      constexpr int uc = (u + 2) % NST3, um = (u + 1) % NST3;  // planes pl - 1 and pl - 2
       const bool landed = bar_wait(&sm.bar[u], (phase >> u) & 1u);
       if (landed) {
         phase ^= 1u << u;
@@ -299,11 +306,17 @@ __global__ void __launch_bounds__(NT3, 2)
       const Raw3T& R = sm.raw[u];
       float4* D = sm.der[u];
       float2* G = sm.png[u];
-      const float swA1 = R.sw[rawA], snA1 = R.sn[rawA], mA1 = R.m[rawA];
-      const float swB1 = R.sw[rawB], snB1 = R.sn[rawB], mB1 = R.m[rawB];
       derive(R, D, G, rawA, ownA, ty + 1, bA, i, jA, pl);
       derive(R, D, G, rawB, ownB, ty + Y3 + 1, bB, i, jB, pl);
       if (hslot >= 0) derive(R, D, G, hraw, hslot, hy, bH, gh_i, gh_j, pl);
+      if (!PLANAR && pl >= pb + 2) {
+        const Raw3T& RC = sm.raw[uc];
+        const long long lk = i + (long long)(pl - 1) * c.sz;
+        update(sm.der[uc], sm.png[uc], sm.der[um], D, ownA, ty + 1, RC.sw[rawA], RC.sn[rawA], RC.m[rawA],
+               lk + (long long)jA * c.sy, landed && actA, jA);
+        update(sm.der[uc], sm.png[uc], sm.der[um], D, ownB, ty + Y3 + 1, RC.sw[rawB], RC.sn[rawB], RC.m[rawB],
+               lk + (long long)jB * c.sy, landed && actB, jB);
+      }
       if (__syncthreads_or(!landed)) {
         if (tid == ISS3) {
           atomicOr(a.err, 2u);
@@ -313,27 +326,14 @@ __global__ void __launch_bounds__(NT3, 2)
         __syncthreads();
         return true;
       }
-      if (tid == ISS3 && pl + NST3 <= ke) {
+      if (tid == ISS3 && pl > pb && pl + NST3 - 1 <= ke) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        issue(u, pl + NST3);
+        issue(uc, pl + NST3 - 1);
       }
       if (PLANAR) {
-        update(D, G, D, D, ownA, ty + 1, swA1, snA1, mA1, i + (long long)jA * c.sy, actA, jA);
-        update(D, G, D, D, ownB, ty + Y3 + 1, swB1, snB1, mB1, i + (long long)jB * c.sy, actB, jB);
-      } else if (pl >= pb + 2) {
-        constexpr int uc = (u + 2) % NST3, um = (u + 1) % NST3;
-        const long long lk = i + (long long)(pl - 1) * c.sz;
-        update(sm.der[uc], sm.png[uc], sm.der[um], D, ownA, ty + 1, swA0, snA0, mA0, lk + (long long)jA * c.sy, actA,
-               jA);
-        update(sm.der[uc], sm.png[uc], sm.der[um], D, ownB, ty + Y3 + 1, swB0, snB0, mB0, lk + (long long)jB * c.sy,
-               actB, jB);
+        update(D, G, D, D, ownA, ty + 1, R.sw[rawA], R.sn[rawA], R.m[rawA], i + (long long)jA * c.sy, actA, jA);
+        update(D, G, D, D, ownB, ty + Y3 + 1, R.sw[rawB], R.sn[rawB], R.m[rawB], i + (long long)jB * c.sy, actB, jB);
       }
-      swA0 = swA1;
-      snA0 = snA1;
-      mA0 = mA1;
-      swB0 = swB1;
-      snB0 = snB1;
-      mB0 = mB1;
       return false;
     };
     for (int base = pb; base <= ke; base += NST3) {
