@@ -143,12 +143,19 @@ __global__ void __launch_bounds__(NT3, 2)
   const int nitems = ntiles * c.nzchunks;
   const uint32_t stage_bytes = (UNIK ? 4u : 5u) * (uint32_t)(BX3 * WY3 * sizeof(float));
   double acc[3] = {0., 0., 0.}, rmax = 0., nonfinite = 0.;
+  // Launched with programmatic stream serialisation: the previous kernel
+  // (the boundary kernel, which rearms the counter) has completed and its
+  // writes are visible once this returns.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 
   for (;;) {
     if (tid == 0) sm.w_sh = (int)atomicAdd(a.counter, 1u);
     __syncthreads();
     const int w = sm.w_sh;
-    if (w >= nitems) break;
+    if (w >= nitems) {
+      asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+      break;
+    }
     const int tile = w % ntiles, zc = w / ntiles;
     const int ti = tile % c.tiles_x, tj = tile / c.tiles_x;
     const int i0 = 1 + ti * TX, j0 = 1 + tj * T3, x0 = i0 - 1;
@@ -378,7 +385,10 @@ __global__ void __launch_bounds__(NT3, 2)
 // step's expressions).  Block 0 rearms the sweep's work counter.
 __global__ void __launch_bounds__(256) boundary3_kernel(const __grid_constant__ Step3FConst c,
                                                          const __grid_constant__ Step3TArgs a, int nbound) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) *a.counter = 0u;
+  // The next sweep may be scheduled once every block is here (it waits for
+  // this kernel's completion); the cell's position is worked out before
+  // waiting for the sweep's values.
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int q0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (q0 >= nbound) return;
   const int nx = c.nx, ny = c.ny, nz = c.nz;
@@ -416,6 +426,8 @@ __global__ void __launch_bounds__(256) boundary3_kernel(const __grid_constant__ 
   const int i1 = min(max(i, 1), nx - 2), j1 = min(max(j, 1), ny - 2);
   const int k1 = nz == 1 ? 0 : min(max(k, 1), nz - 2);
   const long long lb = i + j * c.sy + (long long)k * c.sz, l1 = i1 + j1 * c.sy + (long long)k1 * c.sz;
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // the sweep's interior values
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.counter = 0u;
   const double Pn1 = a.Pref[j1] + (double)a.o_pw[l1];
   double sw = c.S_ref_w + (double)a.o_sw[l1], sn = c.S_ref_n + (double)a.o_sn[l1];
   if ((j == 0) && (c.source > 0) &&
@@ -448,6 +460,25 @@ __global__ void __launch_bounds__(256) boundary3_kernel(const __grid_constant__ 
   a.o_pg[lb] = (float)(pg - pr);
 }
 
+// Launches with programmatic stream serialisation: the kernel may start
+// while the previous kernel in the stream finishes, and waits for it with
+// griddepcontrol.wait before touching what that kernel writes.
+template <typename... Params, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 template <bool UNIK, bool DIAG, bool PLANAR, bool A2>
 cudaError_t launch_t3(const Step3FConst& c, const Step3TArgs& a, int grid, cudaStream_t s) {
   auto kern = step3_fp32c_tma_kernel<UNIK, DIAG, PLANAR, A2>;
@@ -461,8 +492,7 @@ cudaError_t launch_t3(const Step3FConst& c, const Step3TArgs& a, int grid, cudaS
     if (e != cudaSuccess) return e;
     __atomic_fetch_or(&done, bit, __ATOMIC_ACQ_REL);
   }
-  kern<<<grid, dim3(TX, Y3), kSmem3T, s>>>(c, a);
-  return cudaGetLastError();
+  return launch_pdl(kern, dim3(grid), dim3(TX, Y3), kSmem3T, s, c, a);
 }
 
 template <bool UNIK, bool DIAG>
@@ -496,8 +526,7 @@ cudaError_t launch_step3_fp32c_tma(const Step3FConst& c, const Step3TArgs& a, in
                        : (diag ? launch_pa<false, true>(planar, a2, c, a, grid, s)
                                : launch_pa<false, false>(planar, a2, c, a, grid, s));
   if (e != cudaSuccess) return e;
-  boundary3_kernel<<<(nbound + 255) / 256, 256, 0, s>>>(c, a, nbound);
-  return cudaGetLastError();
+  return launch_pdl(boundary3_kernel, dim3((nbound + 255) / 256), dim3(256), 0, s, c, a, nbound);
 }
 
 }  // namespace capaz
