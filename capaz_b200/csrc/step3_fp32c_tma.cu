@@ -165,6 +165,7 @@ __global__ void __launch_bounds__(NT3, 2)
     const int ke = PLANAR ? 0 : 1 + (int)((long long)(zc + 1) * (c.nz - 2) / c.nzchunks);
     const int pb = PLANAR ? 0 : kb - 1;
     bool bad = false;
+    float chk = 0.f;  // sum of |p_w| + |s_w| + |s_n| of the written cells (non-diagnostic steps)
     if (tid < WY3) {
       const int gj = min(j0 - 1 + tid, c.ny - 1);
       sm.rowF[tid] = a.rowF[gj];
@@ -274,13 +275,19 @@ __global__ void __launch_bounds__(NT3, 2)
       const double dSw = (a11 * (dAn * a32 - a23 * dAg) + dAw * c12) * inv;
       const double dSn = (a12 * (dAn * a31 - a21 * dAg) + dAw * c13 - a11 * dAn * a32) * inv;
       const double Pn1 = P + dP, Swn = Sw + dSw, Snn = Sn + dSn;
+      const float pwf = (float)(pw0 + dP), swf = (float)((double)sw0 + dSw), snf = (float)((double)sn0 + dSn);
       if (act) {
-        a.o_pw[l] = (float)(pw0 + dP);
-        a.o_sw[l] = (float)((double)sw0 + dSw);
-        a.o_sn[l] = (float)((double)sn0 + dSn);
+        a.o_pw[l] = pwf;
+        a.o_sw[l] = swf;
+        a.o_sn[l] = snf;
       }
-      const bool finite = isfinite(Pn1) && isfinite(Swn) && isfinite(Snn);
-      bad |= act && !finite;
+      bool finite = true;
+      if (DIAG) {
+        finite = isfinite(Pn1) && isfinite(Swn) && isfinite(Snn);
+        bad |= act && !finite;
+      } else if (act) {
+        chk += fabsf(pwf) + fabsf(swf) + fabsf(snf);  // not finite (or beyond FLT_MAX) once any term is
+      }
       if (DIAG && act) {
         const double Sgn = 1. - Swn - Snn;
         const double rw1 = c.ro0_w * (1. + (c.beta_w) * (Pn1 - c.P_atm));
@@ -351,6 +358,7 @@ __global__ void __launch_bounds__(NT3, 2)
       if (plane(std::integral_constant<int, 2>{}, base + 2)) { stopped = true; break; }
     }
     if (stopped) break;
+    if (!DIAG) bad = !(chk <= 3.0e38f);
     if (__any_sync(0xffffffffu, bad) && (tid & 31) == 0) atomicOr(a.err, 1u);
     __syncthreads();  // the next item reuses the stages, slots and rows
   }
