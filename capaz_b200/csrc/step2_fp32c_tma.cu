@@ -208,7 +208,8 @@ __device__ __forceinline__ double warp_max(double v) {
 // The three axis terms are Kahan-summed per phase.  The FP64 Newton takes the
 // densities from the row's reference densities plus the stored pressure
 // deviation, and its reciprocal from the hardware double-precision estimate
-// refined by one Newton-Raphson step (two with diagnostics).  The plane loop
+// refined by one Newton-Raphson step, with or without diagnostics, so a step
+// with diagnostics gives the same state as one without.  The plane loop
 // is unrolled by two so the register roles of consecutive planes swap
 // without copies.  The rows' constant pairs are read from shared memory where
 // they are used, which leaves the registers to the four cells.
@@ -224,7 +225,6 @@ struct SmemRC {
   float2 rowAR[TL::WY];
   float4 rowG[TL::WY];
   double2 rowR[TL::WY];
-  double rowPrel[TL::WY];
   double red[TL::NW][DIAG_STRIDE];
   int w_sh;
 };
@@ -337,7 +337,6 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
       const double prel = I->Pref[gj] - f.P_atm;
       sm.rowF[tid] = I->rowF[gj];
       sm.rowR[tid] = make_double2(fma(f.aw, prel, f.ro0_w), fma(f.bn, prel, f.ro0_n));
-      sm.rowPrel[tid] = prel;
     }
     auto issue = [&](int q, int pl) {
       mbar_expect_tx(&sm.bar[q], stage_bytes);
@@ -432,7 +431,6 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
       double inv;
       asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(inv) : "d"(det));
       inv = fma(inv, fma(-det, inv, 1.), inv);
-      if (DIAG) inv = fma(inv, fma(-det, inv, 1.), inv);
       const double dP = fma(rn, Aw, rw * An) * inv;
       const double dS = fma(J11, An, -(J21 * Aw)) * inv;
       const float pn = (float)(pd + dP);
@@ -441,26 +439,28 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
         st_global(p_out + l, pn);
         st_global(s_out + l, snew);
       }
-      bool finite = true;
-      if (DIAG) {
-        finite = isfinite(pn) && isfinite(snew);
-        bad |= act && !finite;
-      } else if (act) {
-        chk += fabsf(pn) + fabsf(snew);  // not finite (or beyond FLT_MAX) once any term is
-      }
-      if (DIAG && act) {
-        const float e = (float)fma(det, inv, -1.);
-        const float q = (float)(dP * dS);
-        const float F1 = fmaf(Awf * iro0w_f, e, -aw_ro0w_f * q);
-        const float F2 = fmaf(Anf * iro0n_f, e, bn_ro0n_f * q);
-        const float rf = fmaxf(fabsf(F1), fabsf(F2));
-        const double md = (double)mc;
-        const double mS1 = md * (S_ref + (double)snew);
-        const double P1rel = sm.rowPrel[RC_R * ty + 1 + r] + (double)pn;
-        acc_w = fma(md - mS1, fma(f.aw, P1rel, f.ro0_w), acc_w);
-        acc_n = fma(mS1, fma(f.bn, P1rel, f.ro0_n), acc_n);
-        if (!(rf <= rmax)) rmax = rf;
-        if (!finite) nonfinite += 1.;
+      if (!DIAG) {
+        if (act) chk += fabsf(pn) + fabsf(snew);  // not finite (or beyond FLT_MAX) once any term is
+      } else {
+        // Diagnostics of the written cells: the phase masses of the new state
+        // in FP64, at the unrounded new (P, S), within an FP32 rounding of
+        // the stored values; the Newton residual; the non-finite count.
+        if (act) {
+          const bool fin = fabsf(pn) + fabsf(snew) <= 3.0e38f;
+          bad |= !fin;
+          const double md = (double)mc;
+          const double P1 = pd + dP;
+          const double mS1 = md * (S + dS);
+          acc_w = fma(md - mS1, fma(f.aw, P1, rr.x), acc_w);
+          acc_n = fma(mS1, fma(f.bn, P1, rr.y), acc_n);
+          const float e = (float)fma(det, inv, -1.);
+          const float q = (float)(dP * dS);
+          const float F1 = fmaf(Awf * iro0w_f, e, -aw_ro0w_f * q);
+          const float F2 = fmaf(Anf * iro0n_f, e, bn_ro0n_f * q);
+          const float rf = fmaxf(fabsf(F1), fabsf(F2));
+          if (!(rf <= rmax)) rmax = rf;
+          if (!fin) nonfinite += 1.;
+        }
       }
     };
 

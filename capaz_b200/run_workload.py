@@ -2,7 +2,7 @@
 command line to time or profile a single step kernel (ncu, nvidia-smi).
 
     python -m capaz_b200.run_workload WORKLOAD [--steps N] [--warmup W]
-                                      [--pow-products] [--no-tma] [--tile 16|32]
+                                      [--pow-products] [--no-tma] [--tile 16|32] [--diag]
 
 Workloads (gravity on z, the workloads of capaz_b200.configs):
   two-phase-fp32c    256x256x128 two-phase, precision form
@@ -11,7 +11,8 @@ Workloads (gravity on z, the workloads of capaz_b200.configs):
   three-phase-fp64   192x192x96 three-phase, plain FP64
 Each run sets the media, builds the initial state on the device, steps
 `warmup` steps, synchronises, steps `steps` steps and prints the time of the
-latter (CUDA events) and the kernel launches it made.
+latter (CUDA events) and the kernel launches it made.  With --diag every
+step reduces the step diagnostics (CAPAZ_FLAG_DIAGNOSTICS, one step per call).
 """
 from __future__ import annotations
 
@@ -38,6 +39,7 @@ def main(argv=None) -> dict:
     ap.add_argument("--pow-products", action="store_true", help="CAPAZ_FLAG_POW_PRODUCTS (FP64 forms)")
     ap.add_argument("--no-tma", action="store_true", help="CAPAZ_FLAG_NO_TMA (precision forms)")
     ap.add_argument("--tile", type=int, default=16, help="rows of the two-phase precision sweep's tile")
+    ap.add_argument("--diag", action="store_true", help="diagnostics reduced on every step")
     a = ap.parse_args(argv)
     import torch
 
@@ -49,6 +51,16 @@ def main(argv=None) -> dict:
         p.flags |= native.FLAG_POW_PRODUCTS
     if a.no_tma:
         p.flags |= native.FLAG_NO_TMA
+    if a.diag:
+        p.flags |= native.FLAG_DIAGNOSTICS
+
+    def run(n):
+        if a.diag:
+            for _ in range(n):
+                s.step(1)
+        else:
+            s.step(n)
+
     with Simulation(p) as s:
         s.set_field("m", w.m)
         if w.K is not None:
@@ -56,12 +68,12 @@ def main(argv=None) -> dict:
         if a.tile != 16:
             s.set_sweep_tile(a.tile)
         s.init_state()
-        s.step(a.warmup)
+        run(a.warmup)
         s.sync()
         l0 = s.launch_count
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        s.step(a.steps)
+        run(a.steps)
         e1.record()
         s.sync()
         out = {"workload": a.workload, "cells": p.ncell, "steps": a.steps, "ms_per_step": e0.elapsed_time(e1) / max(a.steps, 1),

@@ -94,6 +94,33 @@ def test_fp32c_full_workload_1000_steps_vs_fp64():
     assert out32["diag"]["max_residual"] < 1e-9
 
 
+def test_diagnostics_leave_the_state_unchanged():
+    """A precision-form step that reduces the diagnostics computes the same
+    state as one that does not (both refine the reciprocal of the Newton
+    determinant once), and the diagnostics of every step agree with those of
+    a run that reduces them only at its end."""
+    p = two_phase_params(64, 40, 48, form=native.FORM_FP32C)
+    m, K = heterogeneous_fields((p.nz, p.ny, p.nx), 1.0, 4.0, 11)
+    p.dt = stable_dt(p, m, K)
+    plain = run(p, m, K, 6)
+    q = p.copy()
+    q.flags |= native.FLAG_DIAGNOSTICS
+    with Simulation(q) as s:
+        s.set_field("m", m)
+        s.set_field("K", K)
+        s.init_state()
+        for _ in range(6):
+            s.step(1)
+        every = {"P_w": s.get_field("P_w"), "S_n": s.get_field("S_n"), "diag": s.diag()}
+    last = run(p, m, K, 6, diag=True)
+    for k in ("P_w", "S_n"):
+        assert np.array_equal(every[k], plain[k]), k
+        assert np.array_equal(last[k], plain[k]), k
+    assert every["diag"]["mass"] == last["diag"]["mass"]
+    assert every["diag"]["max_residual"] == last["diag"]["max_residual"]
+    assert every["diag"]["nonfinite_cells"] == 0
+
+
 def test_fp32c_planar_and_capillary():
     p = two_phase_params(70, 33, 1, form=native.FORM_FP32C)
     p.P_d, p.lambda_ = 755.0, 2.7
