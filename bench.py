@@ -938,18 +938,19 @@ def run_capaz(args) -> None:
 
         def e2e_pass(nsteps):
             """Upload, nsteps steps with their diagnostics, download.  Each
-            step's diagnostics are read one step behind: the copy is posted
-            after step i and waited for after step i + 1 has been queued, so
-            the device never idles while the host reads.  Events on the
-            stream split the pass into upload, steps and download."""
+            step's diagnostics are read one step behind: capaz_step_post_diag
+            steps and posts them into a pinned ring slot (the sweep writes the
+            slot itself), and the host waits for step i after step i + 1 has
+            been queued, so the device never idles while the host reads.
+            Events on the stream split the pass into upload, steps and
+            download."""
             ev[0].record(stream)
             for name in ("m", "K", "P_w", "S_n"):
                 native.check(sim2.lib.capaz_set_field(sim2.ctx, native.FIELDS[name], host[name].data_ptr(), sh),
                              sim2.ctx)
             ev[1].record(stream)
             for i in range(nsteps):
-                sim2.step(1, stream=sh)
-                sim2.post_diag(i % slots, stream=sh)
+                sim2.step_post_diag(1, i % slots, stream=sh)
                 if i > 0:
                     sim2.wait_diag((i - 1) % slots)
             ev[2].record(stream)

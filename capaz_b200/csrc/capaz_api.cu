@@ -679,6 +679,10 @@ int capaz_post_diag(capaz_ctx* ctx, int slot, void* stream) {
   if (!ctx || slot < 0 || slot >= CAPAZ_DIAG_SLOTS) return CAPAZ_ERR_INVALID_ARGUMENT;
   return ctx->post_diag(slot, (cudaStream_t)stream);
 }
+int capaz_step_post_diag(capaz_ctx* ctx, int nsteps, int slot, void* stream) {
+  if (!ctx || nsteps < 0 || slot < 0 || slot >= CAPAZ_DIAG_SLOTS) return CAPAZ_ERR_INVALID_ARGUMENT;
+  return ctx->step_post_diag(nsteps, slot, (cudaStream_t)stream);
+}
 int capaz_wait_diag(capaz_ctx* ctx, int slot, capaz_diag* out) {
   if (!ctx || !out || slot < 0 || slot >= CAPAZ_DIAG_SLOTS) return CAPAZ_ERR_INVALID_ARGUMENT;
   return ctx->wait_diag(slot, out);
@@ -1053,6 +1057,23 @@ int capaz_ctx::post_diag(int slot, cudaStream_t s) {
     return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "diagnostics need CAPAZ_FLAG_DIAGNOSTICS");
   CUDA_TRY(this, launch_diag_publish(diag_out, diag_host_dev + DIAG_STRIDE * slot, s));
   launches++;
+  CUDA_TRY(this, cudaEventRecord(diag_ev[slot], s));
+  diag_posted[slot] = true;
+  return CAPAZ_OK;
+}
+
+// A step whose last sweep writes the reduced diagnostics straight into the
+// mapped ring slot (the precision form's TMA sweep), followed by the event
+// the host waits for; other paths step and then publish with post_diag.
+int capaz_ctx::step_post_diag(int nsteps, int slot, cudaStream_t s) {
+  if (!(p.flags & CAPAZ_FLAG_DIAGNOSTICS))
+    return fail(this, CAPAZ_ERR_INVALID_ARGUMENT, "diagnostics need CAPAZ_FLAG_DIAGNOSTICS");
+  publish_to = diag_host_dev + DIAG_STRIDE * slot;
+  published = false;
+  const int r = step(nsteps, s);
+  publish_to = nullptr;
+  if (r != CAPAZ_OK) return r;
+  if (!published) return post_diag(slot, s);
   CUDA_TRY(this, cudaEventRecord(diag_ev[slot], s));
   diag_posted[slot] = true;
   return CAPAZ_OK;

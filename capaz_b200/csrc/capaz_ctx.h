@@ -34,6 +34,11 @@ struct capaz_ctx {
   double* diag_host_dev = nullptr;
   cudaEvent_t diag_ev[CAPAZ_DIAG_SLOTS + 1] = {};
   bool diag_posted[CAPAZ_DIAG_SLOTS + 1] = {};
+  // Set by step_post_diag for the next step() call: where the last step's
+  // sweep also writes its reduced diagnostics (mapped pinned memory), and
+  // whether it did.
+  double* publish_to = nullptr;
+  bool published = false;
   double* scratch = nullptr;         // one float64 field, derived fields
   void* host_stage = nullptr;
   // Precision form: state stored as FP32 deviations from P_ref(j) and S_ref.
@@ -109,6 +114,7 @@ struct capaz_ctx {
   int step(int nsteps, cudaStream_t s);
   int read_diag(capaz_diag* out, cudaStream_t s);
   int post_diag(int slot, cudaStream_t s);
+  int step_post_diag(int nsteps, int slot, cudaStream_t s);
   int wait_diag(int slot, capaz_diag* out);
   int check_flag();
   // Precision form: FP64 view of (P_w, S_n, m, K) of state buffer b.

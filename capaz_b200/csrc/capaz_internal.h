@@ -203,12 +203,13 @@ bool tma_tile_supported(int tile_y);
 // blocks of BOUND_BLOCK).  counters: four zeroed words (work items and
 // finished CTAs per state parity) that the sweeps rearm themselves.  With
 // diag_partials, the sweep writes per-CTA diagnostics partials (grid of
-// them) and its last CTA reduces them into diag_out.
+// them) and its last CTA reduces them into diag_out, and also into diag_host
+// (the device view of mapped pinned host memory) when that is not null.
 constexpr int BOUND_BLOCK = 256;
 constexpr int SWEEP_COUNTERS = 4;
 cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
                                    bool unik, bool planar, unsigned int* counters, double* diag_partials, int grid,
-                                   cudaStream_t s, double* diag_out, int tile_y);
+                                   cudaStream_t s, double* diag_out, int tile_y, double* diag_host = nullptr);
 cudaError_t launch_boundary_fp32c(const PhysF& f, const InstT* insts, const int2* bitems, int nbitems, int parity,
                                   cudaStream_t s);
 // Boundary cells of an nx x ny x nz grid (faces, edges, corners; nz == 1: the

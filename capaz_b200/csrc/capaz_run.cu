@@ -108,8 +108,10 @@ int capaz_ctx::step(int nsteps, cudaStream_t s) {
       const bool last = t == nsteps - 1;
       // With diagnostics, the last step's boundary kernel also reduces the
       // sweep's partials into diag_out.
+      double* const pub = (diag && last) ? publish_to : nullptr;
       e = launch_step2_fp32c_tma(f, tma_inst, tma_items, tma_nitems, cur, unik, p.nz == 1, tma_counter,
-                                 (diag && last) ? diag_partials : nullptr, tma_grid, s, diag_out, tma_tile_y);
+                                 (diag && last) ? diag_partials : nullptr, tma_grid, s, diag_out, tma_tile_y, pub);
+      if (pub) published = true;
       if (e == cudaSuccess) e = launch_boundary_fp32c(f, tma_inst, tma_bitems, tma_nbitems, cur, s);
       launches += 2;
       if (e != cudaSuccess) return fail_cuda(e, "step2_fp32c_tma launch");

@@ -233,7 +233,8 @@ template <int TYT, bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
 __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
     step2_fp32c_tma_kernel(const __grid_constant__ PhysF f, const InstT* __restrict__ insts,
                           const int4* __restrict__ items, int nitems, int parity, unsigned int* __restrict__ counters,
-                          double* __restrict__ diag_partials, double* __restrict__ diag_out) {
+                          double* __restrict__ diag_partials, double* __restrict__ diag_out,
+                          double* __restrict__ diag_host) {
   using TL = Tile<TYT>;
   constexpr int WY = TL::WY, NHALO = TL::NHALO, BYW = TL::BYW, RC_R = TL::R, RC_TY = TL::NW, RC_NT = TL::NT;
   static_assert(NHALO <= RC_NT - 32, "a warp without halo work issues the copies");
@@ -635,6 +636,12 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
           t[4] += red[qq][4];
         }
         for (int e = 0; e < DIAG_STRIDE; e++) diag_out[e] = t[e];
+        if (diag_host) {
+          // Published into mapped pinned host memory as well: the host reads
+          // it after an event recorded behind this step, with no further launch.
+          for (int e = 0; e < DIAG_STRIDE; e++) diag_host[e] = t[e];
+          __threadfence_system();
+        }
       }
     }
   }
@@ -759,32 +766,34 @@ cudaError_t prepare_t() {
 
 template <int TYT, bool UNIK, bool DIAG, bool PLANAR, bool UNITH>
 cudaError_t launch_t(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
-                     unsigned int* counter, double* diag_partials, int grid, cudaStream_t s, double* diag_out) {
+                     unsigned int* counter, double* diag_partials, int grid, cudaStream_t s, double* diag_out,
+                     double* diag_host) {
   cudaError_t e = prepare_t<TYT, UNIK, DIAG, PLANAR, UNITH>();
   if (e != cudaSuccess) return e;
   return launch_dependent(step2_fp32c_tma_kernel<TYT, UNIK, DIAG, PLANAR, UNITH>, dim3(grid),
                           dim3(TX, Tile<TYT>::NW), sizeof(SmemRC<TYT>), s, f, insts, items, nitems, parity, counter,
-                          diag_partials, diag_out);
+                          diag_partials, diag_out, diag_host);
 }
 
 template <int TYT, bool UNIK, bool DIAG, bool PLANAR>
 cudaError_t launch_h(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
-                     unsigned int* counter, double* diag_partials, int grid, cudaStream_t s, double* diag_out) {
+                     unsigned int* counter, double* diag_partials, int grid, cudaStream_t s, double* diag_out,
+                     double* diag_host) {
   // Unit spacing (the workloads' h = 1 m): forces are plain differences.
   const bool unith = f.inv_hx2 == 1.f && f.inv_hy2 == 1.f && f.inv_hz2 == 1.f;
   return unith ? launch_t<TYT, UNIK, DIAG, PLANAR, true>(f, insts, items, nitems, parity, counter, diag_partials,
-                                                          grid, s, diag_out)
+                                                          grid, s, diag_out, diag_host)
                : launch_t<TYT, UNIK, DIAG, PLANAR, false>(f, insts, items, nitems, parity, counter, diag_partials,
-                                                           grid, s, diag_out);
+                                                           grid, s, diag_out, diag_host);
 }
 
 template <int TYT>
 cudaError_t launch_shape(bool unik, bool planar, const PhysF& f, const InstT* insts, const int4* items, int nitems,
                          int parity, unsigned int* counter, double* diag_partials, int grid, cudaStream_t s,
-                         double* diag_out) {
+                         double* diag_out, double* diag_host) {
   const bool d = diag_partials != nullptr;
 #define CAPAZ_LH(U, D, P) launch_h<TYT, U, D, P>(f, insts, items, nitems, parity, counter, d ? diag_partials : nullptr, \
-                                                 grid, s, d ? diag_out : nullptr)
+                                                 grid, s, d ? diag_out : nullptr, d ? diag_host : nullptr)
   if (unik) {
     if (d) return planar ? CAPAZ_LH(true, true, true) : CAPAZ_LH(true, true, false);
     return planar ? CAPAZ_LH(true, false, true) : CAPAZ_LH(true, false, false);
@@ -818,13 +827,15 @@ bool tma_tile_supported(int tile_y) { return tile_y == 16 || tile_y == 32; }
 
 cudaError_t launch_step2_fp32c_tma(const PhysF& f, const InstT* insts, const int4* items, int nitems, int parity,
                                    bool unik, bool planar, unsigned int* counters, double* diag_partials, int grid,
-                                   cudaStream_t s, double* diag_out, int tile_y) {
+                                   cudaStream_t s, double* diag_out, int tile_y, double* diag_host) {
   // counters[0..3] are zero at allocation; every launch rearms the pair of
   // the other parity (see the kernel).
   if (tile_y == 32)
-    return launch_shape<32>(unik, planar, f, insts, items, nitems, parity, counters, diag_partials, grid, s, diag_out);
+    return launch_shape<32>(unik, planar, f, insts, items, nitems, parity, counters, diag_partials, grid, s, diag_out,
+                            diag_host);
   if (tile_y == 16)
-    return launch_shape<16>(unik, planar, f, insts, items, nitems, parity, counters, diag_partials, grid, s, diag_out);
+    return launch_shape<16>(unik, planar, f, insts, items, nitems, parity, counters, diag_partials, grid, s, diag_out,
+                            diag_host);
   return cudaErrorInvalidValue;
 }
 

@@ -121,6 +121,7 @@ PROTOTYPES = {
     "capaz_step": (C.c_int, [_VP, C.c_int, _VP]),
     "capaz_read_diag": (C.c_int, [_VP, C.POINTER(Diag), _VP]),
     "capaz_post_diag": (C.c_int, [_VP, C.c_int, _VP]),
+    "capaz_step_post_diag": (C.c_int, [_VP, C.c_int, C.c_int, _VP]),
     "capaz_wait_diag": (C.c_int, [_VP, C.c_int, C.POINTER(Diag)]),
     "capaz_set_dt": (C.c_int, [_VP, C.c_double]),
     "capaz_set_sweep_tile": (C.c_int, [_VP, C.c_int]),

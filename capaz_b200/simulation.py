@@ -154,6 +154,11 @@ class Simulation:
         `slot` (< native.DIAG_SLOTS) without waiting."""
         check(self.lib.capaz_post_diag(self.ctx, int(slot), stream or None), self.ctx)
 
+    def step_post_diag(self, nsteps: int, slot: int, stream: int = 0) -> None:
+        """step(nsteps) and post_diag(slot) in one call: the precision form's
+        sweep writes the last step's diagnostics into the slot itself."""
+        check(self.lib.capaz_step_post_diag(self.ctx, int(nsteps), int(slot), stream or None), self.ctx)
+
     def wait_diag(self, slot: int) -> dict:
         """Waits for the copy posted to `slot` and returns it (the form of diag())."""
         d = Diag()

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define CAPAZ_ABI_VERSION 5
+#define CAPAZ_ABI_VERSION 6
 
 /* ---- status codes ------------------------------------------------------ */
 enum capaz_status {
@@ -277,6 +277,12 @@ int capaz_read_diag(capaz_ctx* ctx, capaz_diag* out, void* stream);
 #define CAPAZ_DIAG_SLOTS 4
 int capaz_post_diag(capaz_ctx* ctx, int slot, void* stream);
 int capaz_wait_diag(capaz_ctx* ctx, int slot, capaz_diag* out);
+/* capaz_step followed by capaz_post_diag(slot) in one call (needs
+ * CAPAZ_FLAG_DIAGNOSTICS).  In the precision form's TMA-staged sweep the last
+ * step writes its reduced diagnostics straight into the ring slot, which saves
+ * the copy launch; elsewhere it is the two calls.  capaz_wait_diag(slot)
+ * returns them. */
+int capaz_step_post_diag(capaz_ctx* ctx, int nsteps, int slot, void* stream);
 /* Sets dt for the following steps (a per-step parameter in the reference:
  * consts.dt); host value, no device traffic beyond the kernel argument. */
 int capaz_set_dt(capaz_ctx* ctx, double dt);

@@ -32,7 +32,7 @@ def test_struct_layouts():
     lib = native.load()
     assert lib.capaz_params_size() == C.sizeof(native.Params)
     assert lib.capaz_diag_size() == C.sizeof(native.Diag)
-    assert lib.capaz_abi_version() == 5
+    assert lib.capaz_abi_version() == 6
 
 
 def test_defaults_are_reference_two_phase_ini():

@@ -175,16 +175,27 @@ def test_gpu_pipelined_diagnostics_equal_synchronous_reads(form):
         with pytest.raises(native.CapazError) as e:
             s.wait_diag(0)  # nothing posted since its last wait
         assert e.value.code == native.ERR_INVALID_ARGUMENT
-    if form == native.FORM_FP64:
-        assert got == want
-    else:
-        # The precision form's sweep hands out tiles from a work counter, so
-        # its per-CTA partial sums (and their FP64 rounding) vary from run
-        # to run; the state itself does not.
-        for a, b in zip(got, want):
-            for i in range(2):
-                assert abs(a["mass"][i] - b["mass"][i]) <= 1e-13 * abs(b["mass"][i])
-            assert a["max_residual"] == b["max_residual"] and a["nonfinite_cells"] == b["nonfinite_cells"]
+    # The step and the post in one call (the precision form's sweep writes
+    # the slot itself).
+    with Simulation(p) as s:
+        fresh(s)
+        fused = []
+        for i in range(nsteps):
+            s.step_post_diag(1, i % native.DIAG_SLOTS)
+            if i > 0:
+                fused.append(s.wait_diag((i - 1) % native.DIAG_SLOTS))
+        fused.append(s.wait_diag((nsteps - 1) % native.DIAG_SLOTS))
+    for seq in (got, fused):
+        if form == native.FORM_FP64:
+            assert seq == want
+        else:
+            # The precision form's sweep may hand out tiles from a work
+            # counter, so its per-CTA partial sums (and their FP64 rounding)
+            # may vary from run to run; the state itself does not.
+            for a, b in zip(seq, want):
+                for i in range(2):
+                    assert abs(a["mass"][i] - b["mass"][i]) <= 1e-13 * abs(b["mass"][i])
+                assert a["max_residual"] == b["max_residual"] and a["nonfinite_cells"] == b["nonfinite_cells"]
     assert len({d["mass"][0] for d in got}) > 1  # the steps differ
 
 
