@@ -454,8 +454,15 @@ int capaz_ctx::step_split(cudaStream_t edge, cudaStream_t interior) {
     if (p.nz - 2 > 1)
       for (int t = 0; t < ntiles; t++) items.push_back(make_int4(0, t, p.nz - 2, p.nz - 1));
     split_nedge = (int)items.size();
-    for (int kb = 2; kb < p.nz - 2; kb += 16)
-      for (int t = 0; t < ntiles; t++) items.push_back(make_int4(0, t, kb, std::min(kb + 16, p.nz - 2)));
+    const int full = step2_fp32c_tma_grid(device, unik, ty);
+    const int inner = p.nz - 4;  // centre planes 2 .. nz - 3
+    if (inner > 0) {
+      const int nc = balanced_zchunks(ntiles, inner, full);
+      for (int zc = 0; zc < nc; zc++)
+        for (int t = 0; t < ntiles; t++)
+          items.push_back(make_int4(0, t, 2 + (int)((long long)zc * inner / nc),
+                                    2 + (int)((long long)(zc + 1) * inner / nc)));
+    }
     split_nint = (int)items.size() - split_nedge;
     if (split_items) cudaFree(split_items);
     split_items = nullptr;
@@ -463,7 +470,6 @@ int capaz_ctx::step_split(cudaStream_t edge, cudaStream_t interior) {
     if (e != cudaSuccess) return fail_cuda(e, "cudaMalloc(split items)");
     e = cudaMemcpy(split_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail_cuda(e, "cudaMemcpy(split items)");
-    const int full = step2_fp32c_tma_grid(device, unik, ty);
     split_grid_e = std::min(split_nedge, full);
     split_grid_i = std::min(std::max(split_nint, 1), full);
     split_tile_y = ty;

@@ -5,9 +5,11 @@
 // configuration the workloads use (no capillary pressure, P_d = 0, so
 // P_n = P_w; Brooks-Corey index lambda = 2, so k_w = S_e^4 and
 // k_n = (1-S_e)^2 (1-S_e^2)), and laid out for Blackwell:
-//   - persistent CTAs take (instance, tile, z-chunk) work items from a global
-//     counter, so one launch covers one grid or a whole ensemble of uneven
-//     grids without tail waves;
+//   - persistent CTAs take (instance, tile, z-range) work items, the first
+//     one by their index and the rest from a global counter, so one launch
+//     covers one grid or a whole ensemble of uneven grids; a grid's z-ranges
+//     are sized so its items fill the grid of CTAs in as few rounds as
+//     possible;
 //   - a tile is 32 x 16 cells, a CTA four warps; each thread owns a column
 //     segment of four cells and keeps their derived values in registers
 //     across planes, so only the x neighbours and the segment ends go
