@@ -113,7 +113,7 @@ __device__ __forceinline__ double wmax3(double v) {
   return v;
 }
 
-template <bool UNIK, bool DIAG, bool PLANAR, bool A2>
+template <bool UNIK, bool DIAG, bool PLANAR, bool A2, bool UNITH>
 __global__ void __launch_bounds__(NT3, 2)
     step3_fp32c_tma_kernel(const __grid_constant__ Step3FConst c, const __grid_constant__ Step3TArgs a) {
   extern __shared__ __align__(128) unsigned char smem_bytes[];
@@ -218,15 +218,17 @@ __global__ void __launch_bounds__(NT3, 2)
       const float2 yaN = Gc[own - WX3], ybN = Gc[own + WX3];
       const float pc = cc.x;  // interior: p_n = p_g = p_w
       const float4 row = sm.rowF[wr];
-      const float dn = sm.rowF[wr - 1].w * c.inv_hy2_f, dp = row.w * c.inv_hy2_f;
-      const float x1 = (xa.x - pc) * c.inv_hx2_f, x2 = (pc - xb.x) * c.inv_hx2_f;
+      // Unit spacing (the workloads' h = 1 m): the 1/h^2 factors drop out.
+      const float ihx = UNITH ? 1.f : c.inv_hx2_f, ihy = UNITH ? 1.f : c.inv_hy2_f, ihz = UNITH ? 1.f : c.inv_hz2_f;
+      const float dn = sm.rowF[wr - 1].w * ihy, dp = row.w * ihy;
+      const float x1 = (xa.x - pc) * ihx, x2 = (pc - xb.x) * ihx;
       float z1 = 0.f, z2 = 0.f;
       float4 zm, zp;
       if (!PLANAR) {
         zm = Dm[own];
         zp = Dp[own];
-        z1 = (zm.x - pc) * c.inv_hz2_f;
-        z2 = (pc - zp.x) * c.inv_hz2_f;
+        z1 = (zm.x - pc) * ihz;
+        z2 = (pc - zp.x) * ihz;
       }
       const float pa[3] = {ya.x, yaN.x, yaN.y}, pbv[3] = {yb.x, ybN.x, ybN.y};
       const float Mc[3] = {cc.y, cc.z, cc.w}, Ma[3] = {xa.y, xa.z, xa.w}, Mb[3] = {xb.y, xb.z, xb.w};
@@ -237,8 +239,8 @@ __global__ void __launch_bounds__(NT3, 2)
       for (int ph = 0; ph < 3; ph++) {
         const float fx = face3(x1, x2, Mc[ph], Ma[ph], Mb[ph]);
         const float gr = c.g_inv_hy_f * fmaf(slope[ph], pc, rho[ph]);
-        const float y1 = fmaf(pa[ph] - pc, c.inv_hy2_f, -dn) + gr;
-        const float y2 = fmaf(pc - pbv[ph], c.inv_hy2_f, -dp) + gr;
+        const float y1 = fmaf(pa[ph] - pc, ihy, -dn) + gr;
+        const float y2 = fmaf(pc - pbv[ph], ihy, -dp) + gr;
         const float fy = face3(y1, y2, Mc[ph], My1[ph], My2[ph]);
         float s = fx + fy;
         float comp = (s - fx) - fy;
@@ -487,9 +489,9 @@ cudaError_t launch_pdl(void (*kernel)(Params...), dim3 grid, dim3 block, size_t 
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
-template <bool UNIK, bool DIAG, bool PLANAR, bool A2>
+template <bool UNIK, bool DIAG, bool PLANAR, bool A2, bool UNITH>
 cudaError_t launch_t3(const Step3FConst& c, const Step3TArgs& a, int grid, cudaStream_t s) {
-  auto kern = step3_fp32c_tma_kernel<UNIK, DIAG, PLANAR, A2>;
+  auto kern = step3_fp32c_tma_kernel<UNIK, DIAG, PLANAR, A2, UNITH>;
   static unsigned long long done = 0;  // bit d: shared memory opted in on device d
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -503,10 +505,17 @@ cudaError_t launch_t3(const Step3FConst& c, const Step3TArgs& a, int grid, cudaS
   return launch_pdl(kern, dim3(grid), dim3(TX, Y3), kSmem3T, s, c, a);
 }
 
+template <bool UNIK, bool DIAG, bool PLANAR, bool A2>
+cudaError_t launch_h3(const Step3FConst& c, const Step3TArgs& a, int grid, cudaStream_t s) {
+  const bool unith = c.inv_hx2_f == 1.f && c.inv_hy2_f == 1.f && c.inv_hz2_f == 1.f;
+  return unith ? launch_t3<UNIK, DIAG, PLANAR, A2, true>(c, a, grid, s)
+               : launch_t3<UNIK, DIAG, PLANAR, A2, false>(c, a, grid, s);
+}
+
 template <bool UNIK, bool DIAG>
 cudaError_t launch_pa(bool planar, bool a2, const Step3FConst& c, const Step3TArgs& a, int grid, cudaStream_t s) {
-  if (planar) return a2 ? launch_t3<UNIK, DIAG, true, true>(c, a, grid, s) : launch_t3<UNIK, DIAG, true, false>(c, a, grid, s);
-  return a2 ? launch_t3<UNIK, DIAG, false, true>(c, a, grid, s) : launch_t3<UNIK, DIAG, false, false>(c, a, grid, s);
+  if (planar) return a2 ? launch_h3<UNIK, DIAG, true, true>(c, a, grid, s) : launch_h3<UNIK, DIAG, true, false>(c, a, grid, s);
+  return a2 ? launch_h3<UNIK, DIAG, false, true>(c, a, grid, s) : launch_h3<UNIK, DIAG, false, false>(c, a, grid, s);
 }
 
 }  // namespace
@@ -516,7 +525,7 @@ int step3_fp32c_tma_tiles_y(int ny) { return (ny - 2 + T3 - 1) / T3; }
 int step3_fp32c_tma_grid(int device) {
   int sms = 148, per = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  auto kern = step3_fp32c_tma_kernel<false, true, false, true>;
+  auto kern = step3_fp32c_tma_kernel<false, true, false, true, false>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem3T) != cudaSuccess) {
     cudaGetLastError();
     return sms;
