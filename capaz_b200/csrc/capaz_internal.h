@@ -9,6 +9,15 @@
 
 namespace capaz {
 
+#ifdef __CUDACC__
+// True when a and b have the same bits.  A Newton iteration that returns its
+// input bit for bit has reached a fixed point: every later iteration repeats
+// it, so stopping there gives exactly the result of the full iteration count.
+__device__ __forceinline__ bool same_bits(double a, double b) {
+  return __double_as_longlong(a) == __double_as_longlong(b);
+}
+#endif
+
 // Message returned by capaz_last_error(NULL) (calls without a context).
 void set_create_error(const char* msg);
 

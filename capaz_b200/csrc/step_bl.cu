@@ -160,8 +160,10 @@ __global__ void __launch_bounds__(256, 4) step_bl_interior_kernel(const BLConst 
     const double det = F1P * F2S - F1S * F2P;
     const double nP = P - (1. / det) * (F2S * F1 - F1S * F2);
     const double nS = S - (1. / det) * (F1P * F2 - F2P * F1);
+    const bool fixed = same_bits(nP, P) && same_bits(nS, S);
     P = nP;
     S = nS;
+    if (fixed) break;  // the remaining iterations would repeat this one
   }
   Pw_out[l] = P;
   Sn_out[l] = S;
@@ -246,8 +248,10 @@ __global__ void __launch_bounds__(NTHREADS, 4)
     const double det = F1P * F2S - F1S * F2P;
     const double nP = P - (1. / det) * (F2S * F1 - F1S * F2);
     const double nS = S - (1. / det) * (F1P * F2 - F2P * F1);
+    const bool fixed = same_bits(nP, P) && same_bits(nS, S);
     P = nP;
     S = nS;
+    if (fixed) break;  // the remaining iterations would repeat this one
   }
   Pw_out[l] = P;
   Sn_out[l] = S;
