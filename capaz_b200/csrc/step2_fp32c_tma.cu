@@ -162,6 +162,8 @@ __device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
 struct Kahan2 {
   f32x2 s, c;
   __device__ __forceinline__ explicit Kahan2(f32x2 a) : s(a), c(0ull) {}
+  // The first two terms: the compensation starts at the rounding of a + b.
+  __device__ __forceinline__ Kahan2(f32x2 a, f32x2 b) : s(add2(a, b)), c(sub2(sub2(s, a), b)) {}
   __device__ __forceinline__ void add(f32x2 x) {
     const f32x2 y = sub2(x, c);
     const f32x2 t = add2(s, y);
@@ -516,8 +518,7 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
             const ulonglong2 c = C[r];
             const ulonglong2 ya = r == 0 ? Dr[o - WX] : C[r - 1];
             const ulonglong2 yb = r == RC_R - 1 ? Dr[o + WX] : C[r + 1];
-            Kahan2 k(xaxis(c, Dr[o - 1], Dr[o + 1]));
-            k.add(yaxis(c, ya, yb, G1(r), G2(r)));
+            Kahan2 k(xaxis(c, Dr[o - 1], Dr[o + 1]), yaxis(c, ya, yb, G1(r), G2(r)));
             const f32x2 out = zflux(c, N[r]);
             k.add(sub2(out, Zin[r]));
             Zin[r] = out;
@@ -547,8 +548,7 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
           const ulonglong2 c = N[r];
           const ulonglong2 ya = r == 0 ? Dw[o - WX] : N[r - 1];
           const ulonglong2 yb = r == RC_R - 1 ? Dw[o + WX] : N[r + 1];
-          Kahan2 k(xaxis(c, Dw[o - 1], Dw[o + 1]));
-          k.add(yaxis(c, ya, yb, G1(r), G2(r)));
+          Kahan2 k(xaxis(c, Dw[o - 1], Dw[o + 1]), yaxis(c, ya, yb, G1(r), G2(r)));
           finish(c, k.sum(), r, R.s[raw0 + r * BXW], R.m[raw0 + r * BXW], l0 + r * sy32, (active >> r) & 1u);
         }
       }
