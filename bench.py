@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--forward-mode-fd-cells", type=int, default=0,
+                    help="also run the FP64 forward mode along the first N central-difference cells of each field "
+                         "(about 50 s of host time per cell)")
     ap.add_argument("--no-three-phase", action="store_true")
     ap.add_argument("--no-physics", action="store_true", help="skip the Buckley-Leverett and energy legs")
     ap.add_argument("--no-ensemble", action="store_true")
@@ -640,12 +643,14 @@ def ensemble_leg(dev, steps: int = 300, warmup: int = 3) -> dict:
             "speedup_vs_sequential_fp32c": seq32 / batch_ms, "speedup_vs_sequential_fp64": seq64 / batch_ms}
 
 
-def adjoint_leg(dev) -> dict:
+def adjoint_leg(dev, fm_cells: int = 0) -> dict:
     """Differentiation form on the config-4 inverse problem (128x128x64,
     FP64, 500 steps, checkpoints every 50): time of one forward solve vs. one
     gradient (checkpointed forward + backward), and central differences of
     the misfit (steps 1e-6 and 1e-4 in ln K and in porosity) at 32 seeded
-    random cells among those whose gradient is at least 1% of the largest."""
+    random cells among those whose gradient is at least 1% of the largest.
+    With fm_cells > 0 the FP64 forward mode also runs along the first fm_cells
+    of those cells in each field, beside their central differences."""
     import torch
 
     from capaz_b200 import Adjoint, Simulation
@@ -693,6 +698,7 @@ def adjoint_leg(dev) -> dict:
     steps_fd = (1e-6, 1e-4)
     rng = np.random.default_rng(32)
     fd_out = {}
+    fd_cells = {}
     for which, g in (("lnK", gK), ("porosity", gm)):
         flat = np.abs(g).ravel()
         pool = np.flatnonzero(flat >= 1e-2 * flat.max())
@@ -712,6 +718,8 @@ def adjoint_leg(dev) -> dict:
                 fd.append((misfit(mp.reshape(w.m.shape), Kp.reshape(w.K.shape)) -
                            misfit(mq.reshape(w.m.shape), Kq.reshape(w.K.shape))) / (2 * h))
             fd = np.array(fd)
+            for l, v in zip(cells[:fm_cells], fd[:fm_cells]):
+                fd_cells.setdefault(which, {}).setdefault(int(l), {})[f"fd_h{h:g}"] = float(v)
             key = which if h == steps_fd[0] else f"{which}_h{h:g}"
             fd_out[key] = {"cells": len(cells), "step": h,
                            "rel_l2": float(np.linalg.norm(fd - ad) / np.linalg.norm(fd)),
@@ -743,6 +751,20 @@ def adjoint_leg(dev) -> dict:
             ad = float(np.sum(terms))
             fwd[name] = {"adjoint": ad, "forward_mode": dJ, "rel_diff": abs(ad - dJ) / abs(dJ) if dJ else None}
         fwd["rel_diff_max"] = max(v["rel_diff"] for v in fwd.values() if isinstance(v, dict) and v["rel_diff"] is not None)
+        # The central-difference cells themselves, each a unit direction.
+        if fd_cells:
+            per = {}
+            for which, g in (("lnK", gK), ("porosity", gm)):
+                for l, row in fd_cells.get(which, {}).items():
+                    d = np.zeros(w.m.shape)
+                    d.reshape(-1)[l] = 1.0
+                    _, dJ = O.tangent(p, steps, w.m, w.K, obs, every, data, dlnK=d if which == "lnK" else None,
+                                      dm=d if which == "porosity" else None)
+                    ad = float(g.ravel()[l])
+                    row.update({"adjoint": ad, "forward_mode": dJ, "rel_diff": abs(ad - dJ) / abs(dJ) if dJ else None})
+                    per[f"{which}_cell_{l}"] = row
+            fwd["fd_cells"] = per
+            fwd["fd_cells_rel_diff_max"] = max(v["rel_diff"] for v in per.values() if v["rel_diff"] is not None)
         fwd["cpu_seconds"] = time.perf_counter() - t0
         fwd["threads"] = O.max_threads()
     except Exception as e:  # reported, never fatal
@@ -912,7 +934,7 @@ def run_capaz(args) -> None:
     adj = None
     if not args.no_adjoint and ws == 1:
         try:
-            adj = adjoint_leg(dev)
+            adj = adjoint_leg(dev, args.forward_mode_fd_cells)
         except Exception as e:  # reported, never fatal to the headline line
             adj = {"failed": str(e)}
 
