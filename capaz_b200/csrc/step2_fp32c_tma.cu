@@ -312,9 +312,10 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
     const InstT* __restrict__ I = insts + it.x;
     const int nx = I->nx, ny = I->ny;
     const int sy32 = (int)I->sy, sz32 = (int)I->sz;
-    const float c1 = I->c1_f;
+    const float c1s = I->c1_f * f.inv_one_m_swr;  // S_e = c1s - s / (1 - S_wr)
     const float dt_f = I->dt_f;
     const double S_ref = I->S_ref;
+    const double aw1 = f.aw * (1. - S_ref), bnS = f.bn * S_ref;  // J11, J21 at s = 0
     const Step2FArgs& A = I->a[parity];
     float* __restrict__ p_out = A.p_out;
     float* __restrict__ s_out = A.s_out;
@@ -371,7 +372,7 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
     auto G2 = [&](int r) { const float4 v = sm.rowG[RC_R * ty + 1 + r]; return pack2(v.z, v.w); };
 
     auto derive_cell = [&](f32x2 ARr, float p, float sv, float K) -> ulonglong2 {
-      const float S_e = (c1 - sv) * f.inv_one_m_swr;
+      const float S_e = fmaf(-sv, f.inv_one_m_swr, c1s);
       const float e2 = S_e * S_e;
       const float om = 1.f - S_e;
       const float kw = e2 * e2;
@@ -430,8 +431,7 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
       const double2 rr = sm.rowR[RC_R * ty + 1 + r];
       const double rw = fma(f.aw, pd, rr.x);
       const double rn = fma(f.bn, pd, rr.y);
-      const double S = S_ref + sd;
-      const double J11 = fma(-f.aw, S, f.aw), J21 = f.bn * S;
+      const double J11 = fma(-f.aw, sd, aw1), J21 = fma(f.bn, sd, bnS);
       const double det = fma(J11, rn, rw * J21);
       double inv;
       asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(inv) : "d"(det));
@@ -455,7 +455,7 @@ __global__ void __launch_bounds__(Tile<TYT>::NT, Tile<TYT>::MINB)
           bad |= !fin;
           const double md = (double)mc;
           const double P1 = pd + dP;
-          const double mS1 = md * (S + dS);
+          const double mS1 = md * ((S_ref + sd) + dS);
           acc_w = fma(md - mS1, fma(f.aw, P1, rr.x), acc_w);
           acc_n = fma(mS1, fma(f.bn, P1, rr.y), acc_n);
           const float e = (float)fma(det, inv, -1.);
