@@ -19,7 +19,8 @@
 //     with cp.async.bulk.tensor (TMA, 3-D tensor maps, no multicast)
 //     completing on mbarriers, issued by a thread of the warp that derives no
 //     halo cells;
-//   - 128 registers and 52 KB of shared memory: four CTAs per SM;
+//   - at most 128 registers (the launch bound) and 52 KB of shared memory:
+//     four CTAs per SM;
 //   - physics constants are kernel parameters (constant-bank operands);
 //     per-row quantities (rho at the row's reference pressure, the scaled
 //     reference-pressure step) come from small per-instance tables.
